@@ -1,0 +1,383 @@
+#!/usr/bin/env python
+"""Throughput of the fused D3Q19 step on B200 (MLUPS and HBM roofline).
+
+Default workload: 256^3 lid-driven cavity, MRT + Smagorinsky LES (Cs=0.1),
+Re=5000 (tau = 3*u*N/Re + 0.5 = 0.51536), FP32 populations, seeded density
+noise 1e-6, synthetic.  A "step" is one lattice time step over the whole
+domain (one fused kernel launch).  Both lattices (2 x 1.27 GB) are far larger
+than the 126 MB L2, so no L2 flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun) every rank steps its own 256^3 domain (independent
+replicas, no collective on the data path): weak scaling, value = all
+lattice updates / max-over-ranks time.
+
+--impl reference times the reference's own CPU implementation of the step
+(its lbm_codelets.cpp bodies, built as OpenMP C++ in oracle/_ref) on the host
+cores, on rank 0 only.
+"""
+import argparse
+import importlib.util
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+BYTES = {"f32": 4, "f16_shift": 2, "bf16_shift": 2, "f64": 8}
+
+
+def load_package():
+    name = "nflow_red_poplar_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(
+        name, os.path.join(ROOT, "nflow-red-poplar_b200", "__init__.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+WORKLOADS = {
+    # the headline metric's configuration
+    "cavity256_mrt_les": dict(nx=256, ny=256, nz=256, case="cavity", re=5000.0, u=0.1, cs=0.1,
+                              mrt=True, les=True, init=1, amp=1e-6),
+    # the reference's CPU-runnable case
+    "cavity64_srt": dict(nx=64, ny=64, nz=64, case="cavity", tau=0.6, u=0.1, cs=0.0, mrt=False,
+                         les=False, init=1, amp=1e-6),
+    # channel, Re = u_max*ny/nu = 1000
+    "channel512x128x128_mrt_les": dict(nx=512, ny=128, nz=128, case="channel", re_ch=1000.0,
+                                       u=0.05, cs=0.1, mrt=True, les=True, init=2, amp=0.01),
+}
+
+
+def make_case(pkg, w, size=None):
+    nx, ny, nz = w["nx"], w["ny"], w["nz"]
+    if size:
+        f = size / nx
+        nx, ny, nz = size, max(3, int(ny * f)), max(3, int(nz * f))
+    if w["case"] == "cavity":
+        if "tau" in w:
+            iv = pkg.make_inputval(nx, ny, nz, casetype=pkg.CAVITY, tau=w["tau"], u=w["u"],
+                                   mrt=w["mrt"], les=w["les"], cs=w["cs"], h=nx)
+        else:
+            iv = pkg.make_inputval(nx, ny, nz, casetype=pkg.CAVITY, re=w["re"], u=w["u"],
+                                   mrt=w["mrt"], les=w["les"], cs=w["cs"], h=nx)
+    else:
+        nu = w["u"] * ny / w["re_ch"]
+        iv = pkg.make_inputval(nx, ny, nz, casetype=pkg.CHANNEL, tau=3.0 * nu + 0.5, u=w["u"],
+                               mrt=w["mrt"], les=w["les"], cs=w["cs"])
+    return iv
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_from_profile(workload, storage):
+    """dram bytes per launch of k_step from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", f"k_step_{storage}_{workload}.txt")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_launch:"):
+                return int(float(line.split(":", 1)[1].split()[0]))
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, local_rank):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        ident = str(local_rank)
+        if vis:
+            ids = [v.strip() for v in vis.split(",") if v.strip()]
+            if local_rank < len(ids):
+                ident = ids[local_rank]
+        q = ("clocks.sm,clocks.max.sm,power.draw,utilization.gpu,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", f"--id={ident}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            out, _ = self.p.communicate(timeout=5)
+        except Exception:
+            self.p.kill()
+            out = ""
+        rows = []
+        for ln in out.splitlines():
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                rows.append(dict(sm=float(parts[0]), smax=float(parts[1]), util=float(parts[3]),
+                                 hw=parts[4], hwt=parts[5], swt=parts[6], pc=parts[7]))
+            except ValueError:
+                continue
+        if not rows:
+            return None
+        load = [r for r in rows if r["util"] > 0] or rows
+        reasons = set()
+        for r in load:
+            for k, name in (("hw", "hw_slowdown"), ("hwt", "hw_thermal_slowdown"),
+                            ("swt", "sw_thermal_slowdown"), ("pc", "sw_power_cap")):
+                if r[k].lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(r["sm"] for r in load),
+                "sm_max_mhz": max(r["smax"] for r in load), "reasons": sorted(reasons),
+                "samples": len(load)}
+
+
+def cpu_baseline(pkg, w, budget_s=20.0):
+    """The reference's own codelets (oracle/_ref) on the host cores, or the
+    oracle port if the reference build is absent: one warm-up step, then as
+    many full-size steps as fit in the budget."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+
+    cores = os.cpu_count() or 1
+    which = "ref" if O.poplar_ref_lib() is not None and w["case"] == "cavity" and w["mrt"] else "orc"
+    iv = make_case(pkg, w)
+    split = max(1, math.ceil(2 * cores / 27))
+    r = O.Run(iv, init_kind=w["init"], amp=w["amp"], split=split, threads=cores, which=which)
+    t0 = time.perf_counter()
+    r.step(1)
+    t1 = time.perf_counter()
+    per = t1 - t0
+    n = max(1, min(50, int(budget_s / max(per, 1e-3))))
+    t0 = time.perf_counter()
+    r.step(n)
+    dt = time.perf_counter() - t0
+    r.close()
+    cells = iv.nx * iv.ny * iv.nz
+    return dict(value=cells * n / dt / 1e6, unit="MLUPS", cores=cores,
+                kind="reference" if which == "ref" else "port",
+                sample=f"{n} full steps of {iv.nx}x{iv.ny}x{iv.nz} after 1 warm-up step, "
+                       f"{27 * split} tiles, {cores} OpenMP threads, {dt:.1f} s")
+
+
+def run_reference_arm(args, pkg, w):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+
+    cores = os.cpu_count() or 1
+    which = "ref" if O.poplar_ref_lib() is not None and w["case"] == "cavity" and w["mrt"] else "orc"
+    iv = make_case(pkg, w)
+    split = max(1, math.ceil(2 * cores / 27))
+    r = O.Run(iv, init_kind=w["init"], amp=w["amp"], split=split, threads=cores, which=which)
+    t0 = time.perf_counter()
+    r.step(1)
+    per = time.perf_counter() - t0
+    # each step is a bounded sample: the whole run stays within ~2-3 minutes
+    total = args.steps + args.warmup
+    nz_s = iv.nz
+    if per * total > 150.0:
+        nz_s = max(4, int(iv.nz * 150.0 / (per * total)))
+        r.close()
+        iv = pkg.make_inputval(iv.nx, iv.ny, nz_s, casetype=iv.casetype, tau=iv.m_dTau,
+                               u=iv.m_dRefVelx, mrt=iv.bEnableMRT, les=iv.bEnableLES,
+                               cs=iv.m_dSmagorinsky, h=iv.h)
+        r = O.Run(iv, init_kind=w["init"], amp=w["amp"], split=split, threads=cores, which=which)
+    if args.warmup:
+        r.step(args.warmup)
+    t0 = time.perf_counter()
+    r.step(args.steps)
+    dt = time.perf_counter() - t0
+    cells = iv.nx * iv.ny * iv.nz
+    v = cells * args.steps / dt / 1e6
+    sample = (f"each step one full step of {iv.nx}x{iv.ny}x{iv.nz}"
+              + ("" if nz_s == w["nz"] else f" (z cut from {w['nz']} to bound the run)")
+              + f", {27 * split} tiles, {cores} OpenMP threads")
+    line = {
+        "impl": "reference", "metric": "MLUPS", "value": v, "unit": "MLUPS", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": args.workload, "nx": w["nx"], "ny": w["ny"], "nz": w["nz"],
+                   "device": "host CPU"},
+        "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": cores,
+                         "kind": "reference" if which == "ref" else "port", "sample": sample},
+        "e2e": {"value": v, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="cavity256_mrt_les", choices=sorted(WORKLOADS))
+    ap.add_argument("--storage", default="f32", choices=["f32", "f16_shift", "bf16_shift", "f64"])
+    ap.add_argument("--size", type=int, default=0, help="scale the workload to this nx (profiling)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip cpu baseline, e2e and storage forms (profiling runs)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    pkg = load_package()
+    w = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        run_reference_arm(args, pkg, w)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def allmax(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    storage_id = {"f32": pkg.STORE_F32, "f16_shift": pkg.STORE_F16_SHIFT,
+                  "bf16_shift": pkg.STORE_BF16_SHIFT, "f64": pkg.STORE_F64}
+    iv = make_case(pkg, w, args.size or None)
+    cells = iv.nx * iv.ny * iv.nz
+    stream = torch.cuda.current_stream()
+
+    def timed_steps(storage, k, warm, sampler=None):
+        opt = pkg.default_options(storage=storage_id[storage], init_kind=w["init"],
+                                  noise_amp=w["amp"], seed=1, device=local)
+        dom = pkg.Domain(iv, opt)
+        dom.set_stream(stream.cuda_stream)
+        dom.run(warm)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        dom.run(k)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        return dom, ms
+
+    # pre-roll under the clock sampler so that short timed regions still see
+    # several samples under load
+    sampler = ClockSampler(local)
+    dom0, _ = timed_steps(args.storage, max(10, int(0.4 / 0.0005)), args.warmup)
+    dom0.close()
+    dom, ms = timed_steps(args.storage, args.steps, args.warmup)
+    clocks = sampler.stop()
+    ms_max = allmax(ms)
+    per_launch_ms = ms / args.steps
+    value = world * cells * args.steps / (ms_max / 1e3) / 1e6
+
+    peak, peak_kind = measured_peak()
+    bpl = 2 * 19 * BYTES[args.storage]
+    alg_bytes = bpl * cells
+    achieved = alg_bytes / (per_launch_ms / 1e3) / 1e9
+    traffic = traffic_from_profile(args.workload, args.storage)
+
+    line = {
+        "metric": "MLUPS", "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": args.storage, "data": "synthetic",
+        "config": {"workload": args.workload, "nx": iv.nx, "ny": iv.ny, "nz": iv.nz,
+                   "collision": "MRT" if iv.bEnableMRT else "SRT", "les": bool(iv.bEnableLES),
+                   "cs": round(float(iv.m_dSmagorinsky), 6), "tau": round(float(iv.m_dTau), 6),
+                   "storage": args.storage, "streaming": "pull A/B, fused boundaries",
+                   "l2": "inputs larger than L2 (2 lattices of %.2f GB vs 126 MB)" %
+                         (19 * BYTES[args.storage] * cells / 1e9),
+                   "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": alg_bytes,
+                     "bytes_per_lattice_update": bpl},
+        "gpu_launches": args.steps,
+        "clocks": clocks,
+    }
+
+    if not args.no_extras:
+        # end to end through the C ABI with pinned host buffers: import the
+        # padded arF (H2D), K steps, export the padded arF (D2H)
+        shp = (iv.ny + 2, iv.nz + 2, iv.nx + 2, 19)
+        h_in = torch.empty(shp, dtype=torch.float32, pin_memory=True).numpy()
+        h_out = torch.empty(shp, dtype=torch.float32, pin_memory=True).numpy()
+        dom.export_arF(padded=True, out=h_in)
+        dom.import_arF(h_in, padded=True)  # warm the staging buffer
+        dom.run(args.warmup)
+        dom.export_arF(padded=True, out=h_out)
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        dom.import_arF(h_in, padded=True)
+        dom.run(args.steps)
+        dom.export_arF(padded=True, out=h_out)
+        dt = time.perf_counter() - t0
+        barrier()
+        dt = allmax(dt)
+        nbytes = h_in.nbytes
+        line["e2e"] = {"value": world * cells * args.steps / dt / 1e6, "unit": "MLUPS",
+                       "h2d_bytes_per_step": nbytes / args.steps,
+                       "d2h_bytes_per_step": nbytes / args.steps,
+                       "what": "lbm_import_arF(padded host AoS) + lbm_run_simulation(K) + "
+                               "lbm_export_arF(padded host AoS), pinned host memory"}
+        dom.close()
+        # storage forms of the same workload (precision form: throughput)
+        forms = {}
+        for st in ("f32", "f16_shift", "bf16_shift"):
+            d2, ms2 = timed_steps(st, args.steps, args.warmup)
+            d2.close()
+            ms2 = allmax(ms2)
+            forms[st] = {"MLUPS": world * cells * args.steps / (ms2 / 1e3) / 1e6,
+                         "GB_s": 2 * 19 * BYTES[st] * cells / (ms2 / args.steps / 1e3) / 1e9}
+        line["storage_forms"] = forms
+        if rank == 0 and world == 1:
+            line["cpu_baseline"] = cpu_baseline(pkg, w)
+    else:
+        dom.close()
+
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

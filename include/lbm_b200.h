@@ -1,0 +1,304 @@
+/*
+ * lbm_b200.h — C ABI of the B200 D3Q19 lattice-Boltzmann time step.
+ *
+ * This is the drop-in boundary for the hot path of NFLOW-RED-Poplar (the
+ * E8ight LBM3D solver ported to Poplar).  Every entry point below names the
+ * reference interface it replaces (file:line inside the reference project).
+ * Plain C types only: pointers, sizes and the reference's own Inputval
+ * struct, so the header can be bound from C, C++ (lbm_b200_compat.hpp adds
+ * the reference's C++ names), ctypes or any other FFI.
+ *
+ * Conventions kept from the reference
+ *   - axis order [y][z][x], y slowest: node id = x + z*nx + y*nx*nz
+ *     (main.cpp:1, lbm_codelets.cpp:52);
+ *   - D3Q19 velocity ordering, opposite table and weights of main.cpp:87-146;
+ *   - the population array arF at the boundary is AoS with the direction
+ *     fastest: arF[dir + node*19].  Two views are offered:
+ *       unpadded  [ny][nz][nx][19]          (main.cpp:216, the tensor main.cpp
+ *                                            writes with "H2D-arF" and reads
+ *                                            back with "D2H-arF"),
+ *       padded    [ny+2][nz+2][nx+2][19]    (README "Output sliced Tensor",
+ *                                            one ghost layer per side; the
+ *                                            ghost layer is written as 0).
+ *   Internally populations live on the GPU in a private SoA layout; the
+ *   AoS<->SoA transform happens only at import/export.
+ *
+ * Error handling: every call returns an int status (LBM_OK == 0, negative
+ * on failure) and lbm_last_error() returns a per-thread message.  Nothing
+ * calls exit(); the reference exits on a singular MRT matrix
+ * (inverseMRT.cpp:86-90) and on fopen failures (kernel.cu:711, 979).
+ *
+ * Threading: a domain handle may be used by one host thread at a time.
+ * All device work of a handle is ordered on the handle's CUDA stream
+ * (lbm_set_stream); calls that return host data synchronise that stream.
+ */
+#ifndef LBM_B200_H
+#define LBM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+#ifndef __cplusplus
+#include <stdbool.h>
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ */
+/* Parameters of common.h:7-39 (same names and values).                */
+/* ------------------------------------------------------------------ */
+#ifndef DIMENSION
+#define DIMENSION 3
+#endif
+#ifndef DIRECTION_SIZE
+#define DIRECTION_SIZE 19
+#endif
+#ifndef XDIM
+#define XDIM 0
+#define ZDIM 1
+#define YDIM 2
+#endif
+#ifndef XDECOMP
+#define XDECOMP 3
+#define YDECOMP 3
+#define ZDECOMP 3
+#endif
+#ifndef CAVITY
+#define CAVITY 1
+#define POISEUILLE 0
+#endif
+/* Extension: straight channel, parabolic velocity inlet at x=0, constant
+ * pressure outlet at x=nx-1, bounce-back walls on the four side faces. */
+#ifndef CHANNEL
+#define CHANNEL 2
+#endif
+#ifndef NODE_FLUID
+#define NODE_FLUID (1 << 1)
+#define NODE_FIXEDWALL (1 << 2)
+#define NODE_MOVINGWALL (1 << 3)
+#define NODE_INLET (1 << 4)
+#define NODE_OUTLET (1 << 5)
+#define NODE_STRUCT (1 << 6)
+#endif
+#ifndef TILE_NUM
+#define TILE_NUM 1471
+#endif
+
+/* ------------------------------------------------------------------ */
+/* struct.h:78-100 Inputval, field for field (same order and types).    */
+/* `length` is a float in the reference; this library never reads it    */
+/* and sizes every array from nx*ny*nz instead.                          */
+/* ------------------------------------------------------------------ */
+#ifndef LBM_INPUTVAL_DEFINED
+#define LBM_INPUTVAL_DEFINED
+typedef struct Inputval {
+  int h;
+  int nx, ny, nz;
+  int ngrid;
+  int maxitr;
+  int nwrite, irestart, irst;
+  int icycle;
+  float m_dSmagorinsky;
+  float Re, length, nu;
+  float m_dRefViscosity;
+  float m_dRefDen;
+  float m_dTau;
+  float m_dRefVelx, m_dRefVely, m_dRefVelz;
+  float dWeps, dWepsj, dWXX;
+  bool bEnableMRT;
+  bool bEnableLES;
+  int savetype;
+  int casetype;
+} Inputval;
+#endif
+
+/* ------------------------------------------------------------------ */
+/* Status codes                                                         */
+/* ------------------------------------------------------------------ */
+enum {
+  LBM_OK = 0,
+  LBM_ERR_INVALID = -1,   /* bad argument, size or configuration          */
+  LBM_ERR_CUDA = -2,      /* a CUDA runtime/driver call failed            */
+  LBM_ERR_OOM = -3,       /* device allocation failed                      */
+  LBM_ERR_SINGULAR = -4,  /* MRT matrix not invertible                     */
+  LBM_ERR_STATE = -5,     /* call not valid in the handle's current state  */
+  LBM_ERR_TIMEOUT = -6,   /* a bounded device wait gave up                 */
+  LBM_ERR_BUDGET = -7,    /* request exceeds the HBM budget                */
+  LBM_ERR_NOT_FINITE = -8,/* input data holds NaN/Inf                      */
+  LBM_ERR_NO_DEVICE = -9  /* no CUDA device / extension not usable         */
+};
+
+/* Population storage of a domain (all arithmetic is done in FP32 except
+ * LBM_STORE_F64, which is the double-precision build used as the oracle
+ * on the GPU).  The *_SHIFT forms store f_i - w_i (times a per-domain
+ * power-of-two scale) so that the 16-bit format holds the deviation from
+ * the rest state, not the value itself. */
+enum {
+  LBM_STORE_F32 = 0,
+  LBM_STORE_F16_SHIFT = 1,
+  LBM_STORE_BF16_SHIFT = 2,
+  LBM_STORE_F64 = 3
+};
+
+/* Initial condition.  LBM_INIT_REFERENCE reproduces the Initialize
+ * codelet (lbm_codelets.cpp:140-241) / keInitialize (kernel.cu:282-315):
+ * rho = RefDen, u = 0 except the lid (cavity) nodes.  The two seeded forms
+ * add a deterministic counter-based perturbation (splitmix64 of the node id)
+ * so that the CPU oracle and the GPU produce identical initial bits. */
+enum {
+  LBM_INIT_REFERENCE = 0,
+  LBM_INIT_DENSITY_NOISE = 1,   /* rho = RefDen + amp*U(-1,1)                */
+  LBM_INIT_CHANNEL = 2          /* u = inlet profile + amp*u_max*U(-1,1) per */
+                                /* component on non-wall nodes, rho = RefDen */
+};
+
+/* Streaming schedule of the fused kernel. */
+enum {
+  LBM_STREAM_AB = 0,   /* pull, two population lattices (A/B)             */
+  LBM_STREAM_AA = 1    /* in-place AA pattern, one lattice (half memory)   */
+};
+
+typedef struct lbm_options {
+  int storage;          /* LBM_STORE_*                                     */
+  int init_kind;        /* LBM_INIT_*                                      */
+  uint64_t seed;        /* perturbation seed                               */
+  float noise_amp;      /* perturbation amplitude (see LBM_INIT_*)         */
+  float store_scale;    /* *_SHIFT storage scale; 0 = automatic            */
+  int stream_mode;      /* LBM_STREAM_*                                    */
+  int device;           /* CUDA device ordinal                             */
+  int reserved[8];
+} lbm_options;
+
+/* Fill *opt with the defaults: FP32, reference init, A/B streaming. */
+void lbm_default_options(lbm_options* opt);
+
+/* Message of the last failed call made on this host thread. */
+const char* lbm_last_error(void);
+
+/* Library version string. */
+const char* lbm_version(void);
+
+/* ------------------------------------------------------------------ */
+/* Host numerics (no GPU needed).                                       */
+/* ------------------------------------------------------------------ */
+
+/* Replaces `int decomposition(Inputval*, int Slice[][3][2])`
+ * (decomposition.cpp:98-161): cut the domain into XDECOMP*YDECOMP*ZDECOMP
+ * chunks; Slice[t][dim][0/1] = start/end with dim 0=x, 1=y, 2=z.
+ * Returns the tile count (>= 0) or a negative status.  On the GPU these
+ * chunks become the CTA work-list of the fused kernel. */
+int lbm_decomposition(const Inputval* pinput, int Slice[][DIMENSION][2]);
+
+/* Replaces `int set_move_decomp(int NTILE, const int Slice[][3][2],
+ * int Move[][19])` (decomposition.cpp:17-62): per tile, the offset of each
+ * neighbour inside the tile's ghost-padded slice.  Returns 0. */
+int lbm_set_move_decomp(int NTILE, const int Slice[][DIMENSION][2],
+                        int Move[][DIRECTION_SIZE]);
+
+/* Replaces `int slice_chunk(unsigned tile, const int Slice[][3][2], int *xs,
+ * int *xe, int *ys, int *ye, int *zs, int *ze, int *chunk_nx, int *chunk_ny,
+ * int *chunk_nz, int *chunk_len)` (decomposition.cpp:66-94).  Returns 1 when
+ * the tile is empty (skip it), 0 otherwise. */
+int lbm_slice_chunk(unsigned tile, const int Slice[][DIMENSION][2], int* xs,
+                    int* xe, int* ys, int* ye, int* zs, int* ze, int* chunk_nx,
+                    int* chunk_ny, int* chunk_nz, int* chunk_len);
+
+/* Replaces `void inverseMRT(vector<vector<float>>&, vector<vector<float>>&)`
+ * (inverseMRT.cpp:8-92): Gauss-Jordan inverse in FP32 with the same pivot
+ * row rotation.  mat/inv are row-major 19x19.  Returns LBM_ERR_SINGULAR
+ * instead of exit(0). */
+int lbm_inverse_mrt(const float* mat, float* inv);
+
+/* The D3Q19 tables of main.cpp:87-146 and the moment matrix of
+ * main.cpp:149-171: direction[3*19] (rows X, Z, Y as in the reference's
+ * flat Direction tensor), opp[19], w[19], M[19*19] row-major.  Any pointer
+ * may be NULL. */
+void lbm_d3q19_tables(float* direction, int* opp, float* w, float* M);
+
+/* ------------------------------------------------------------------ */
+/* Single domain on one GPU.                                            */
+/* ------------------------------------------------------------------ */
+typedef struct lbm_domain lbm_domain;
+
+/* Allocate a domain for the case in *pinput (nx, ny, nz, casetype, tau,
+ * Smagorinsky constant, reference density/velocity, MRT/LES switches) and
+ * build its constant tables.  opt may be NULL (defaults). */
+int lbm_create(const Inputval* pinput, const lbm_options* opt,
+               lbm_domain** out);
+
+/* Free all device memory of the handle. */
+int lbm_destroy(lbm_domain* d);
+
+/* Use this CUDA stream (a cudaStream_t passed as void*; NULL = the
+ * handle's own stream) for all later work of the handle. */
+int lbm_set_stream(lbm_domain* d, void* cuda_stream);
+
+/* The handle's current CUDA stream (as void*). */
+void* lbm_get_stream(lbm_domain* d);
+
+/* Replaces the `initialize` program (initialize.cpp:23-98, the Initialize
+ * compute set) and the icycle==0 branch of kernel.cu:156-164: node types,
+ * direction masks and the equilibrium populations, on the device. */
+int lbm_initialize(lbm_domain* d);
+
+/* Replaces the `runSimulation` program (runSimulation.cpp:22-168) repeated
+ * nsteps times (main.cpp:290-291 Repeat(maxitr, ...)), and the else-branch
+ * of kernel.cu:166-200.  One fused kernel per step: streaming + boundary
+ * conditions + macroscopic + LES + SRT/MRT collision.  Asynchronous. */
+int lbm_run_simulation(lbm_domain* d, int nsteps);
+
+/* Steps completed since the last initialize/import. */
+int lbm_steps_done(const lbm_domain* d, long long* steps);
+
+/* engine.writeTensor("H2D-arF", ...) (main.cpp:303) followed by a restart
+ * from that state: host AoS populations -> device.  padded != 0 selects the
+ * [ny+2][nz+2][nx+2][19] view (ghost layer ignored).  The macroscopic
+ * fields are recomputed from the imported populations. */
+int lbm_import_arF(lbm_domain* d, const float* arF, int padded);
+
+/* engine.readTensor("D2H-arF", ...) (main.cpp:317): the post-streaming,
+ * post-boundary populations after the last step, device -> host AoS. */
+int lbm_export_arF(lbm_domain* d, float* arF, int padded);
+
+/* CurrDen / CurrVelx / CurrVely / CurrVelz after the last step (the
+ * Macroscopic codelet, lbm_codelets.cpp:248-318), [ny][nz][nx] each.
+ * Any pointer may be NULL. */
+int lbm_get_macroscopic(lbm_domain* d, float* den, float* velx, float* vely,
+                        float* velz);
+
+/* NodeType (common.h:32-37 bits) and DirectionState (19-bit inside mask,
+ * lbm_codelets.cpp:163-178) per node, [ny][nz][nx]. Either may be NULL. */
+int lbm_get_node_info(lbm_domain* d, int* node_type, int* direction_state);
+
+/* Diagnostics of the state after the last step, reduced on the device in
+ * FP64 with a fixed order (bit-reproducible):
+ *   out[0] = mass        sum rho
+ *   out[1..3] = momentum sum rho*u
+ *   out[4] = L1 residual sum |rho - rho_prev| over the last step
+ *            (kernel.cu:232-248 prints the same quantity)
+ *   out[5] = kinetic energy 0.5*sum rho*|u|^2
+ *   out[6] = max |u|
+ *   out[7] = number of non-finite populations (0 when healthy)
+ * Synchronises the handle's stream. */
+int lbm_diagnostics(lbm_domain* d, double out[8]);
+
+/* Block until all work of the handle is done. */
+int lbm_sync(lbm_domain* d);
+
+/* Device bytes held by the handle. */
+int lbm_device_bytes(const lbm_domain* d, size_t* bytes);
+
+/* Bytes a domain of this case would hold (for admission control). */
+int lbm_estimate_bytes(const Inputval* pinput, const lbm_options* opt,
+                       size_t* bytes);
+
+/* Average duration in milliseconds of the fused step kernel over the last
+ * lbm_run_simulation call, measured with CUDA events on the handle's
+ * stream around the kernel launches (synchronises). */
+int lbm_last_run_ms(lbm_domain* d, float* ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LBM_B200_H */

@@ -1,0 +1,273 @@
+"""ctypes binding of the B200 D3Q19 lattice-Boltzmann library (liblbm_b200.so).
+
+The library exposes the C ABI declared in include/lbm_b200.h; this module is
+a thin Python view of it used by the tests and bench.py.  The directory name
+contains dashes, so it is loaded by path (see ``load_package`` in
+tests/conftest.py and bench.py) rather than imported by name.
+
+Nothing here computes: every numeric call goes to the CUDA library, and a
+missing library raises instead of falling back to anything else.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liblbm_b200.so")
+
+DIRECTION_SIZE = 19
+DIMENSION = 3
+XDIM, ZDIM, YDIM = 0, 1, 2
+XDECOMP = YDECOMP = ZDECOMP = 3
+TILE_NUM = 1471
+CAVITY, POISEUILLE, CHANNEL = 1, 0, 2
+NODE_FLUID, NODE_FIXEDWALL, NODE_MOVINGWALL = 1 << 1, 1 << 2, 1 << 3
+NODE_INLET, NODE_OUTLET, NODE_STRUCT = 1 << 4, 1 << 5, 1 << 6
+
+LBM_OK = 0
+LBM_ERR_INVALID = -1
+LBM_ERR_CUDA = -2
+LBM_ERR_OOM = -3
+LBM_ERR_SINGULAR = -4
+LBM_ERR_STATE = -5
+LBM_ERR_TIMEOUT = -6
+LBM_ERR_BUDGET = -7
+LBM_ERR_NOT_FINITE = -8
+LBM_ERR_NO_DEVICE = -9
+
+STORE_F32, STORE_F16_SHIFT, STORE_BF16_SHIFT, STORE_F64 = 0, 1, 2, 3
+INIT_REFERENCE, INIT_DENSITY_NOISE, INIT_CHANNEL = 0, 1, 2
+STREAM_AB, STREAM_AA = 0, 1
+
+
+class Inputval(C.Structure):
+    """struct.h:78-100 of the reference, field for field."""
+
+    _fields_ = [
+        ("h", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+        ("ngrid", C.c_int), ("maxitr", C.c_int), ("nwrite", C.c_int),
+        ("irestart", C.c_int), ("irst", C.c_int), ("icycle", C.c_int),
+        ("m_dSmagorinsky", C.c_float), ("Re", C.c_float), ("length", C.c_float),
+        ("nu", C.c_float), ("m_dRefViscosity", C.c_float), ("m_dRefDen", C.c_float),
+        ("m_dTau", C.c_float), ("m_dRefVelx", C.c_float), ("m_dRefVely", C.c_float),
+        ("m_dRefVelz", C.c_float), ("dWeps", C.c_float), ("dWepsj", C.c_float),
+        ("dWXX", C.c_float), ("bEnableMRT", C.c_bool), ("bEnableLES", C.c_bool),
+        ("savetype", C.c_int), ("casetype", C.c_int),
+    ]
+
+
+class Options(C.Structure):
+    _fields_ = [
+        ("storage", C.c_int), ("init_kind", C.c_int), ("seed", C.c_uint64),
+        ("noise_amp", C.c_float), ("store_scale", C.c_float), ("stream_mode", C.c_int),
+        ("device", C.c_int), ("reserved", C.c_int * 8),
+    ]
+
+
+def make_inputval(nx, ny=None, nz=None, *, casetype=CAVITY, tau=None, re=None, u=0.1,
+                  mrt=False, les=False, cs=0.0, rho0=1.0, h=None):
+    """Fill an Inputval the way main.cpp:59-85 does.
+
+    tau is taken as given, or derived from Re as main.cpp:81 does
+    (tau = 3*u*h/Re + 0.5 with h the grid size).
+    """
+    ny = nx if ny is None else ny
+    nz = nx if nz is None else nz
+    iv = Inputval()
+    iv.h = h if h is not None else nx
+    iv.nx, iv.ny, iv.nz = nx, ny, nz
+    iv.maxitr = 0
+    iv.bEnableMRT = bool(mrt)
+    iv.bEnableLES = bool(les)
+    iv.m_dRefDen = rho0
+    iv.m_dRefVelx, iv.m_dRefVely, iv.m_dRefVelz = u, 0.0, 0.0
+    iv.length = float(nx * ny * nz)
+    if tau is None:
+        if re is None:
+            raise ValueError("give tau or re")
+        iv.Re = re
+        iv.nu = np.float32(u) * np.float32(iv.h) / np.float32(re)
+        tau = np.float32(3.0) * np.float32(u) * np.float32(iv.h) / np.float32(re) + np.float32(0.5)
+    iv.m_dTau = tau
+    iv.m_dSmagorinsky = cs
+    iv.dWeps, iv.dWepsj, iv.dWXX = 3.0, -5.5, -0.5
+    iv.nwrite = 10000
+    iv.savetype = 1
+    iv.casetype = casetype
+    return iv
+
+
+_lib = None
+
+
+def lib():
+    """The loaded liblbm_b200.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: run __graft_entry__.build() first")
+        L = C.CDLL(LIB_PATH)
+        vp, i32, ip = C.c_void_p, C.c_int, C.POINTER(C.c_int)
+        L.lbm_last_error.restype = C.c_char_p
+        L.lbm_version.restype = C.c_char_p
+        L.lbm_default_options.argtypes = [C.POINTER(Options)]
+        L.lbm_decomposition.argtypes = [C.POINTER(Inputval), vp]
+        L.lbm_set_move_decomp.argtypes = [i32, vp, vp]
+        L.lbm_slice_chunk.argtypes = [C.c_uint, vp] + [ip] * 10
+        L.lbm_inverse_mrt.argtypes = [vp, vp]
+        L.lbm_d3q19_tables.argtypes = [vp, vp, vp, vp]
+        L.lbm_create.argtypes = [C.POINTER(Inputval), C.POINTER(Options), C.POINTER(vp)]
+        L.lbm_destroy.argtypes = [vp]
+        L.lbm_set_stream.argtypes = [vp, vp]
+        L.lbm_get_stream.argtypes = [vp]
+        L.lbm_get_stream.restype = vp
+        L.lbm_initialize.argtypes = [vp]
+        L.lbm_run_simulation.argtypes = [vp, i32]
+        L.lbm_steps_done.argtypes = [vp, C.POINTER(C.c_longlong)]
+        L.lbm_import_arF.argtypes = [vp, vp, i32]
+        L.lbm_export_arF.argtypes = [vp, vp, i32]
+        L.lbm_get_macroscopic.argtypes = [vp, vp, vp, vp, vp]
+        L.lbm_get_node_info.argtypes = [vp, vp, vp]
+        L.lbm_diagnostics.argtypes = [vp, vp]
+        L.lbm_sync.argtypes = [vp]
+        L.lbm_device_bytes.argtypes = [vp, C.POINTER(C.c_size_t)]
+        L.lbm_estimate_bytes.argtypes = [C.POINTER(Inputval), C.POINTER(Options),
+                                         C.POINTER(C.c_size_t)]
+        L.lbm_last_run_ms.argtypes = [vp, C.POINTER(C.c_float)]
+        _lib = L
+    return _lib
+
+
+class LbmError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def check(rc):
+    if rc < 0:
+        raise LbmError(rc, lib().lbm_last_error().decode())
+    return rc
+
+
+def default_options(**kw):
+    o = Options()
+    lib().lbm_default_options(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+class Domain:
+    """One resident D3Q19 domain on a GPU (owns its device memory)."""
+
+    def __init__(self, inputval, options=None, initialize=True):
+        self.iv = inputval
+        self.opt = options if options is not None else default_options()
+        h = C.c_void_p()
+        check(lib().lbm_create(C.byref(self.iv), C.byref(self.opt), C.byref(h)))
+        self.h = h
+        self.shape = (inputval.ny, inputval.nz, inputval.nx)
+        if initialize:
+            self.initialize()
+
+    def close(self):
+        if self.h:
+            check(lib().lbm_destroy(self.h))
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def initialize(self):
+        check(lib().lbm_initialize(self.h))
+
+    def run(self, nsteps):
+        check(lib().lbm_run_simulation(self.h, int(nsteps)))
+
+    def sync(self):
+        check(lib().lbm_sync(self.h))
+
+    def set_stream(self, stream_ptr):
+        check(lib().lbm_set_stream(self.h, C.c_void_p(stream_ptr) if stream_ptr else None))
+
+    def steps(self):
+        s = C.c_longlong()
+        check(lib().lbm_steps_done(self.h, C.byref(s)))
+        return s.value
+
+    def export_arF(self, padded=False, out=None):
+        ny, nz, nx = self.shape
+        shp = (ny + 2, nz + 2, nx + 2, 19) if padded else (ny, nz, nx, 19)
+        if out is None:
+            out = np.empty(shp, np.float32)
+        assert out.shape == shp and out.dtype == np.float32 and out.flags.c_contiguous
+        check(lib().lbm_export_arF(self.h, _ptr(out), 1 if padded else 0))
+        return out
+
+    def import_arF(self, arF, padded=False):
+        arF = np.ascontiguousarray(arF, dtype=np.float32)
+        check(lib().lbm_import_arF(self.h, _ptr(arF), 1 if padded else 0))
+
+    def macroscopic(self):
+        out = [np.empty(self.shape, np.float32) for _ in range(4)]
+        check(lib().lbm_get_macroscopic(self.h, *[_ptr(a) for a in out]))
+        return out  # den, ux, uy, uz
+
+    def node_info(self):
+        t = np.empty(self.shape, np.int32)
+        s = np.empty(self.shape, np.int32)
+        check(lib().lbm_get_node_info(self.h, _ptr(t), _ptr(s)))
+        return t, s
+
+    def diagnostics(self):
+        out = np.zeros(8, np.float64)
+        check(lib().lbm_diagnostics(self.h, _ptr(out)))
+        return out
+
+    def device_bytes(self):
+        b = C.c_size_t()
+        check(lib().lbm_device_bytes(self.h, C.byref(b)))
+        return b.value
+
+    def last_run_ms(self):
+        v = C.c_float()
+        check(lib().lbm_last_run_ms(self.h, C.byref(v)))
+        return v.value
+
+
+def decomposition(iv):
+    sl = np.zeros((TILE_NUM, 3, 2), np.int32)
+    n = check(lib().lbm_decomposition(C.byref(iv), _ptr(sl)))
+    return sl[:n]
+
+
+def set_move_decomp(slices):
+    slices = np.ascontiguousarray(slices, np.int32)
+    mv = np.zeros((len(slices), 19), np.int32)
+    check(lib().lbm_set_move_decomp(len(slices), _ptr(slices), _ptr(mv)))
+    return mv
+
+
+def inverse_mrt(mat):
+    mat = np.ascontiguousarray(mat, np.float32)
+    inv = np.zeros((19, 19), np.float32)
+    check(lib().lbm_inverse_mrt(_ptr(mat), _ptr(inv)))
+    return inv
+
+
+def d3q19_tables():
+    d = np.zeros(57, np.float32)
+    o = np.zeros(19, np.int32)
+    w = np.zeros(19, np.float32)
+    m = np.zeros((19, 19), np.float32)
+    lib().lbm_d3q19_tables(_ptr(d), _ptr(o), _ptr(w), _ptr(m))
+    return d, o, w, m

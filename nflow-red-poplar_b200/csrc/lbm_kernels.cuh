@@ -1,0 +1,408 @@
+// lbm_kernels.cuh — device kernels of the fused D3Q19 step.
+//
+// Storage: populations are SoA, pop[q * qstride + x + px*(z + nz*y)]
+// (axis order [y][z][x] as the reference, x fastest, x pitch px padded to a
+// multiple of 8 elements so every row starts 16-byte aligned).  Two
+// lattices A/B: the kernel of step k pulls the post-collision populations
+// f*_{k-1} from one lattice and writes f*_k into the other.
+//
+// One step = one launch of k_step, which per node
+//   1. pulls f_k[q](x) = f*_{k-1}[q](x - c_q)              (Streaming,
+//      lbm_codelets.cpp:57-76: arF[opp d](x) = arFTemp[opp d](x + c_d));
+//   2. replaces every population whose donor x - c_q lies outside the
+//      domain by the boundary rule of the node (BoundaryCavity
+//      lbm_codelets.cpp:373-395, keBoundaryInlet kernel.cu:591-611,
+//      keBoundaryOutlet kernel.cu:639-655), reading f*_{k-1} of the node
+//      itself — the same values the reference reads from arFTemp;
+//   3. forms rho, u (Macroscopic, lbm_codelets.cpp:287-312);
+//   4. forms tau_eddy (ComputeTurbulence_LES) and collides (Collision_MRT
+//      or keCollision_SRT) in registers, and stores f*_k.
+// So one step reads 19 and writes 19 populations per node: the HBM
+// roofline of 2*19*sizeof(storage) bytes per lattice update.
+//
+// The reference's step order LES -> collide -> stream -> BC -> macro is the
+// same computation with the kernel boundary moved: what the reference holds
+// in arF between steps (post-stream) is here reconstructed on demand from
+// the other lattice (k_export), what it holds in arFTemp (post-collision)
+// is the lattice this kernel writes.
+#pragma once
+#include "lbm_d3q19.cuh"
+#include "../../include/lbm_b200.h"
+
+namespace lbm {
+
+template <class S>
+using RealOf = typename StoreTraits<S>::R;
+
+// round-to-nearest primitives that the compiler may not contract into FMA;
+// used where the reference's own rounding sequence is reproduced
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+
+struct Geometry {
+  int nx, ny, nz, px;
+  int casetype;
+};
+
+// node type of keSetNodeType (kernel.cu:1061-1077) / the Initialize codelet
+// (lbm_codelets.cpp:183-201) for CAVITY; CHANNEL: inlet x=0, outlet
+// x=nx-1, the four side faces are fixed walls and override inlet/outlet.
+__device__ __forceinline__ int node_type(const Geometry& g, int x, int y, int z) {
+  int t = NODE_FLUID;
+  if (g.casetype == CAVITY) {
+    if (y == 0) t = NODE_FIXEDWALL;
+    if (y == g.ny - 1) t = NODE_MOVINGWALL;
+    if (x == 0 || x == g.nx - 1 || z == 0 || z == g.nz - 1) t = NODE_FIXEDWALL;
+  } else {  // CHANNEL
+    if (x == 0) t = NODE_INLET;
+    if (x == g.nx - 1) t = NODE_OUTLET;
+    if (y == 0 || y == g.ny - 1 || z == 0 || z == g.nz - 1) t = NODE_FIXEDWALL;
+  }
+  return t;
+}
+
+// 19-bit inside mask of keInitialNodeDirection (kernel.cu:1027-1043):
+// bit q set iff x + c_q lies inside the domain; bit 0 always set.
+__device__ __forceinline__ int direction_state(const Geometry& g, int x, int y, int z) {
+  int ds = 1;
+  static_for<1, Q>([&](auto qc) {
+    constexpr int q = decltype(qc)::value;
+    const int x1 = x + cx(q), y1 = y + cy(q), z1 = z + cz(q);
+    if (x1 >= 0 && x1 < g.nx && y1 >= 0 && y1 < g.ny && z1 >= 0 && z1 < g.nz) ds |= 1 << q;
+  });
+  return ds;
+}
+
+template <class S>
+struct StepArgs {
+  using R = RealOf<S>;
+  const S* __restrict__ src;  // f*_{k-1}
+  S* __restrict__ dst;        // f*_k
+  long long qs;               // population stride (elements)
+  Geometry g;
+  R tau, les_c, rho0;
+  R ulx, uly, ulz;            // lid velocity (cavity)
+  MrtParams<R> mp;
+  float scale, inv_scale;     // shifted 16-bit storage
+  const float* inlet_u;       // [ny*nz] channel inlet profile u_x(y,z)
+  const float* prho_in;       // rho_{k-1} at x = 1        [ny*nz]
+  float* prho_out;            // rho_k at x = 1
+  const float* pu_in;         // u_{k-1} at x = nx-1, nx-2  [2][3][ny*nz]
+  float* pu_out;              // u_k
+  float* den_out;             // optional macroscopic outputs of arF_k
+  float* ux_out;
+  float* uy_out;
+  float* uz_out;
+};
+
+template <class S>
+__device__ __forceinline__ RealOf<S> ld(const S* p, int q, float inv_scale) {
+  return StoreTraits<S>::load(p, weight<RealOf<S>>(q), inv_scale);
+}
+
+// Boundary value of population q at a node whose donor x - c_q is outside
+// the domain.  d = opp(q) is the reference's "outside" direction; fo is
+// f*_{k-1}[d] at the node itself (arFTemp[d](x) in the reference).
+template <class S, int q>
+__device__ __forceinline__ RealOf<S> boundary_value(const StepArgs<S>& a, int t, RealOf<S> fo,
+                                                    int y, int z) {
+  using R = RealOf<S>;
+  constexpr int d = opp(q);
+  if (t == NODE_FIXEDWALL) return fo;
+  if (t == NODE_MOVINGWALL) {
+    // BoundaryCavity: arF[opp d] = ftemp[d] - 6 w_d RefDen (c_d . u_lid)
+    R eu = add_rn(add_rn(mul_rn(R(cx(d)), a.ulx), mul_rn(R(cy(d)), a.uly)),
+                  mul_rn(R(cz(d)), a.ulz));
+    R term = mul_rn(mul_rn(mul_rn(R(6), weight<R>(d)), a.rho0), eu);
+    return sub_rn(fo, term);
+  }
+  const int yz = y * a.g.nz + z;
+  if (t == NODE_INLET) {
+    // keBoundaryInlet: ftemp[d] - 6.0 w_d rho(x+1) (c_d . u_in), FP64 literal
+    const R uin = R(a.inlet_u[yz]);
+    const R eu = mul_rn(R(cx(d)), uin);
+    const double v = (double)fo - 6.0 * (double)weight<R>(d) * (double)a.prho_in[yz] * (double)eu;
+    return R(v);
+  }
+  if (t == NODE_OUTLET) {
+    // keBoundaryOutlet: anti-bounce-back at RefDen with u extrapolated
+    // from the node and its inner neighbour of the previous step
+    const int P = a.g.ny * a.g.nz;
+    const float* u0 = a.pu_in;          // x = nx-1
+    const float* u1 = a.pu_in + 3 * P;  // x = nx-2
+    const R bx = R((double)u0[yz] + 0.5 * (double)(u0[yz] - u1[yz]));
+    const R by = R((double)u0[P + yz] + 0.5 * (double)(u0[P + yz] - u1[P + yz]));
+    const R bz = R((double)u0[2 * P + yz] + 0.5 * (double)(u0[2 * P + yz] - u1[2 * P + yz]));
+    const R usq = bx * bx + by * by + bz * bz;
+    const R eu = R(cx(d)) * bx + R(cy(d)) * by + R(cz(d)) * bz;
+    const double v = -(double)fo + 2.0 * (double)weight<R>(d) * (double)a.rho0 *
+                                       (1.0 + 4.5 * ((double)eu * (double)eu) - 1.5 * (double)usq);
+    return R(v);
+  }
+  return fo;  // no rule for this node type: plain bounce-back
+}
+
+// Steps 1-2: the post-stream, post-boundary populations f_k at (x,y,z).
+template <class S>
+__device__ __forceinline__ void pull(RealOf<S> (&f)[Q], const StepArgs<S>& a, int x, int y, int z,
+                                     long long cell) {
+  const long long sz = a.g.px, sy = (long long)a.g.px * a.g.nz;
+  const bool edge = (x == 0) | (x == a.g.nx - 1) | (y == 0) | (y == a.g.ny - 1) | (z == 0) |
+                    (z == a.g.nz - 1);
+  if (!edge) {
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      f[q] = ld(a.src + q * a.qs + cell - (cx(q) + cz(q) * sz + cy(q) * sy), q, a.inv_scale);
+    });
+  } else {
+    const int t = node_type(a.g, x, y, z);
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      const int xs = x - cx(q), ys = y - cy(q), zs = z - cz(q);
+      const bool inside = (unsigned)xs < (unsigned)a.g.nx && (unsigned)ys < (unsigned)a.g.ny &&
+                          (unsigned)zs < (unsigned)a.g.nz;
+      if (inside) {
+        f[q] = ld(a.src + q * a.qs + cell - (cx(q) + cz(q) * sz + cy(q) * sy), q, a.inv_scale);
+      } else {
+        const RealOf<S> fo = ld(a.src + opp(q) * a.qs + cell, opp(q), a.inv_scale);
+        f[q] = boundary_value<S, q>(a, t, fo, y, z);
+      }
+    });
+  }
+}
+
+enum { COLL_SRT = 0, COLL_MRT = 1 };
+
+template <class S, int COLL, bool LES>
+__device__ __forceinline__ void collide(RealOf<S> (&f)[Q], RealOf<S> rho, RealOf<S> ux,
+                                        RealOf<S> uy, RealOf<S> uz, const StepArgs<S>& a) {
+  using R = RealOf<S>;
+  R te = R(0);
+  if constexpr (LES) te = les_tau_eddy<R>(f, rho, ux, uy, uz, a.tau, a.les_c);
+  const R inv = R(1) / (a.tau + te);
+  if constexpr (COLL == COLL_SRT)
+    collide_srt<R>(f, rho, ux, uy, uz, inv);
+  else
+    collide_mrt<R>(f, rho, ux, uy, uz, inv, a.mp);
+}
+
+// Side outputs of the macroscopic state of arF_k.
+template <class S>
+__device__ __forceinline__ void write_macro(const StepArgs<S>& a, int x, int y, int z,
+                                            RealOf<S> rho, RealOf<S> ux, RealOf<S> uy,
+                                            RealOf<S> uz) {
+  const long long n = x + (long long)a.g.nx * (z + (long long)a.g.nz * y);
+  if (a.den_out) a.den_out[n] = (float)rho;
+  if (a.ux_out) {
+    a.ux_out[n] = (float)ux;
+    a.uy_out[n] = (float)uy;
+    a.uz_out[n] = (float)uz;
+  }
+  if (a.g.casetype == CHANNEL) {
+    const int P = a.g.ny * a.g.nz, yz = y * a.g.nz + z;
+    if (x == 1) a.prho_out[yz] = (float)rho;
+    if (x == a.g.nx - 1) {
+      a.pu_out[yz] = (float)ux;
+      a.pu_out[P + yz] = (float)uy;
+      a.pu_out[2 * P + yz] = (float)uz;
+    }
+    if (x == a.g.nx - 2) {
+      a.pu_out[3 * P + yz] = (float)ux;
+      a.pu_out[4 * P + yz] = (float)uy;
+      a.pu_out[5 * P + yz] = (float)uz;
+    }
+  }
+}
+
+template <class S>
+__device__ __forceinline__ void store_all(const StepArgs<S>& a, const RealOf<S> (&f)[Q],
+                                          long long cell) {
+  static_for<0, Q>([&](auto qc) {
+    constexpr int q = decltype(qc)::value;
+    StoreTraits<S>::store(a.dst + q * a.qs + cell, f[q], weight<RealOf<S>>(q), a.scale);
+  });
+}
+
+// The fused step.  grid = (ceil(nx/blockDim.x), nz, ny), one thread per node.
+template <class S, int COLL, bool LES>
+__global__ void __launch_bounds__(128) k_step(const __grid_constant__ StepArgs<S> a) {
+  using R = RealOf<S>;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int z = blockIdx.y, y = blockIdx.z;
+  if (x >= a.g.nx) return;
+  const long long cell = x + (long long)a.g.px * (z + (long long)a.g.nz * y);
+  R f[Q];
+  pull<S>(f, a, x, y, z, cell);
+  R rho, ux, uy, uz;
+  macroscopic<R>(f, rho, ux, uy, uz);
+  write_macro<S>(a, x, y, z, rho, ux, uy, uz);
+  collide<S, COLL, LES>(f, rho, ux, uy, uz, a);
+  store_all<S>(a, f, cell);
+}
+
+// ------------------------------------------------------------------ //
+// Initial state (Initialize codelet lbm_codelets.cpp:140-241 and the
+// seeded perturbations of LBM_INIT_*): writes arF_0 into a.dst as plain
+// post-stream populations (the "post" lattice) and collides it with the
+// initial rho, u (as the reference's first step does with the CurrDen /
+// CurrVel that Initialize stored) into post_collided.
+// ------------------------------------------------------------------ //
+struct InitParams {
+  int kind;
+  uint64_t seed;
+  float noise_amp;
+  float rho0, ulx, uly, ulz;  // RefDen, RefVel*
+};
+
+__device__ __forceinline__ uint64_t splitmix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+// uniform in [-1, 1) from 24 hash bits; exact in double on any IEEE machine
+__device__ __forceinline__ double unit_noise(uint64_t seed, uint64_t node, uint64_t comp) {
+  const uint64_t r = splitmix64(seed * 0x9E3779B97F4A7C15ull + node * 4ull + comp);
+  return __dadd_rn(__dmul_rn(__dmul_rn((double)(r >> 40), 1.0 / 16777216.0), 2.0), -1.0);
+}
+
+template <class S, int COLL, bool LES>
+__global__ void __launch_bounds__(128)
+    k_init(const __grid_constant__ StepArgs<S> a, S* __restrict__ collided, InitParams ip) {
+  using R = RealOf<S>;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int z = blockIdx.y, y = blockIdx.z;
+  if (x >= a.g.nx) return;
+  const long long cell = x + (long long)a.g.px * (z + (long long)a.g.nz * y);
+  const long long n = x + (long long)a.g.nx * (z + (long long)a.g.nz * y);
+  const int t = node_type(a.g, x, y, z);
+  float den = ip.rho0, velx = 0.f, vely = 0.f, velz = 0.f;
+  if (t == NODE_MOVINGWALL) {
+    velx = ip.ulx;
+    vely = ip.uly;
+    velz = ip.ulz;
+  }
+  // separately rounded products and sums (no FMA), as in the CPU oracle
+  if (ip.kind == LBM_INIT_DENSITY_NOISE) {
+    den = (float)__dadd_rn((double)ip.rho0,
+                           __dmul_rn((double)ip.noise_amp, unit_noise(ip.seed, (uint64_t)n, 0)));
+  } else if (ip.kind == LBM_INIT_CHANNEL &&
+             (t == NODE_FLUID || t == NODE_INLET || t == NODE_OUTLET)) {
+    const double au = __dmul_rn((double)ip.noise_amp, (double)ip.ulx);
+    const float prof = a.g.casetype == CHANNEL ? a.inlet_u[y * a.g.nz + z] : 0.0f;
+    velx = (float)__dadd_rn((double)prof, __dmul_rn(au, unit_noise(ip.seed, (uint64_t)n, 0)));
+    vely = (float)__dmul_rn(au, unit_noise(ip.seed, (uint64_t)n, 1));
+    velz = (float)__dmul_rn(au, unit_noise(ip.seed, (uint64_t)n, 2));
+  }
+  R f[Q];
+  const R rd = R(den), ux = R(velx), uy = R(vely), uz = R(velz);
+  // feq of lbm_codelets.cpp:225-230, in the codelet's rounding order
+  static_for<0, Q>([&](auto qc) {
+    constexpr int q = decltype(qc)::value;
+    const R eu = add_rn(add_rn(mul_rn(R(cx(q)), ux), mul_rn(R(cy(q)), uy)), mul_rn(R(cz(q)), uz));
+    const R usq = add_rn(add_rn(mul_rn(ux, ux), mul_rn(uy, uy)), mul_rn(uz, uz));
+    const R br = sub_rn(add_rn(add_rn(R(1), mul_rn(R(3), eu)), mul_rn(mul_rn(R(4.5), eu), eu)),
+                        mul_rn(R(1.5), usq));
+    f[q] = mul_rn(mul_rn(weight<R>(q), rd), br);
+  });
+  store_all<S>(a, f, cell);  // post-stream lattice
+  write_macro<S>(a, x, y, z, rd, ux, uy, uz);
+  collide<S, COLL, LES>(f, rd, ux, uy, uz, a);
+  static_for<0, Q>([&](auto qc) {
+    constexpr int q = decltype(qc)::value;
+    StoreTraits<S>::store(collided + q * a.qs + cell, f[q], weight<R>(q), a.scale);
+  });
+}
+
+// ------------------------------------------------------------------ //
+// Import of host populations (AoS, direction fastest, optional ghost layer)
+// into the post lattice, then macro + collision into `collided`.
+// ------------------------------------------------------------------ //
+template <class S, int COLL, bool LES>
+__global__ void __launch_bounds__(128)
+    k_import(const __grid_constant__ StepArgs<S> a, const float* __restrict__ aos, int padded,
+             S* __restrict__ collided) {
+  using R = RealOf<S>;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int z = blockIdx.y, y = blockIdx.z;
+  if (x >= a.g.nx) return;
+  const long long cell = x + (long long)a.g.px * (z + (long long)a.g.nz * y);
+  long long node;
+  if (padded)
+    node = (x + 1) + (long long)(a.g.nx + 2) * ((z + 1) + (long long)(a.g.nz + 2) * (y + 1));
+  else
+    node = x + (long long)a.g.nx * (z + (long long)a.g.nz * y);
+  R f[Q];
+  static_for<0, Q>([&](auto qc) {
+    constexpr int q = decltype(qc)::value;
+    f[q] = R(aos[q + node * Q]);
+  });
+  store_all<S>(a, f, cell);
+  // re-read through the storage format so that the collided state starts
+  // from exactly what the post lattice holds
+  static_for<0, Q>([&](auto qc) {
+    constexpr int q = decltype(qc)::value;
+    f[q] = ld(a.dst + q * a.qs + cell, q, a.inv_scale);
+  });
+  R rho, ux, uy, uz;
+  macroscopic<R>(f, rho, ux, uy, uz);
+  write_macro<S>(a, x, y, z, rho, ux, uy, uz);
+  collide<S, COLL, LES>(f, rho, ux, uy, uz, a);
+  static_for<0, Q>([&](auto qc) {
+    constexpr int q = decltype(qc)::value;
+    StoreTraits<S>::store(collided + q * a.qs + cell, f[q], weight<R>(q), a.scale);
+  });
+}
+
+// ------------------------------------------------------------------ //
+// Export of arF_k into a device AoS buffer.  post_direct: a.src already
+// holds arF_k (right after initialize/import); otherwise a.src holds
+// f*_{k-1} and arF_k is reconstructed by the same pull + boundary code as
+// the step kernel.  Padded output zeroes the ghost layer.
+// ------------------------------------------------------------------ //
+template <class S>
+__global__ void __launch_bounds__(128)
+    k_export(const __grid_constant__ StepArgs<S> a, float* __restrict__ aos, int padded,
+             int post_direct) {
+  using R = RealOf<S>;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int z = blockIdx.y, y = blockIdx.z;
+  if (x >= a.g.nx) return;
+  const long long cell = x + (long long)a.g.px * (z + (long long)a.g.nz * y);
+  R f[Q];
+  if (post_direct) {
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      f[q] = ld(a.src + q * a.qs + cell, q, a.inv_scale);
+    });
+  } else {
+    pull<S>(f, a, x, y, z, cell);
+  }
+  long long node;
+  if (padded)
+    node = (x + 1) + (long long)(a.g.nx + 2) * ((z + 1) + (long long)(a.g.nz + 2) * (y + 1));
+  else
+    node = x + (long long)a.g.nx * (z + (long long)a.g.nz * y);
+  static_for<0, Q>([&](auto qc) {
+    constexpr int q = decltype(qc)::value;
+    aos[q + node * Q] = (float)f[q];
+  });
+}
+
+// node type and inside mask per node, [ny][nz][nx]
+__global__ void k_node_info(Geometry g, int* __restrict__ type, int* __restrict__ ds);
+
+// Deterministic FP64 reductions of the macroscopic state:
+// partial[b*8 + i] for block b, then k_diag_final sums blocks in order.
+__global__ void k_diag_partial(const float* __restrict__ den, const float* __restrict__ den_prev,
+                               const float* __restrict__ ux, const float* __restrict__ uy,
+                               const float* __restrict__ uz, long long n, int has_prev,
+                               double* __restrict__ partial);
+__global__ void k_diag_final(const double* __restrict__ partial, int nblocks,
+                             double* __restrict__ out);
+
+}  // namespace lbm
