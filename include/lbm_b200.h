@@ -230,8 +230,9 @@ int lbm_create(const Inputval* pinput, const lbm_options* opt,
 /* Free all device memory of the handle. */
 int lbm_destroy(lbm_domain* d);
 
-/* Use this CUDA stream (a cudaStream_t passed as void*; NULL = the
- * handle's own stream) for all later work of the handle. */
+/* Use this CUDA stream (a cudaStream_t passed as void*; NULL is the CUDA
+ * default stream, as everywhere in CUDA) for all later work of the handle.
+ * A new handle uses its own non-blocking stream. */
 int lbm_set_stream(lbm_domain* d, void* cuda_stream);
 
 /* The handle's current CUDA stream (as void*). */

@@ -424,7 +424,7 @@ int lbm_destroy(lbm_domain* d) {
 
 int lbm_set_stream(lbm_domain* d, void* s) {
   if (!d) return set_error(LBM_ERR_INVALID, "NULL domain");
-  d->stream = s ? (cudaStream_t)s : d->own;
+  d->stream = (cudaStream_t)s;  // NULL: the CUDA default stream
   return LBM_OK;
 }
 

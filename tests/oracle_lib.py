@@ -144,6 +144,17 @@ def kernelcu_run(iv, nsteps, init_kind=0, seed=1, amp=0.0):
     return dict(arF=arF, den=out[0], ux=out[1], uy=out[2], uz=out[3])
 
 
+def rel_vel_err(u, ref):
+    """Velocity error relative to the velocity field's magnitude maximum:
+    max over components of max|u_c - ref_c| / max|ref|.  Each of u, ref is a
+    (ux, uy, uz) triple.  (A per-component normalisation is ill-posed for a
+    component that is ~0 by symmetry, e.g. u_z in the cavity.)"""
+    r = [np.asarray(c, np.float64) for c in ref]
+    mag = np.sqrt(r[0] ** 2 + r[1] ** 2 + r[2] ** 2).max()
+    mag = mag if mag > 0 else 1.0
+    return float(max(np.abs(np.asarray(a, np.float64) - b).max() for a, b in zip(u, r)) / mag)
+
+
 def rel_field_err(a, b):
     """max |a - b| / max |b| (pointwise relative error on u ~ 0 is ill-posed)."""
     a = np.asarray(a, np.float64)

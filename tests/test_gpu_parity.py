@@ -1,9 +1,11 @@
 """Parity of the CUDA path (through the C ABI) with the oracle, on a B200.
 
-Tolerances: after N steps the FP32 fields satisfy
-max|rho_gpu - rho_ref| / max|rho_ref| <= 1e-5 and the same for each velocity
-component (relative to the field maximum; a pointwise relative error on
-u ~ 0 is ill-posed); the FP64 build matches the FP64 oracle to 1e-12.
+Tolerance of the FP32 path: after N steps
+max|rho_gpu - rho_ref| / max|rho_ref| <= 1e-5 and, for every velocity
+component c, max|u_c,gpu - u_c,ref| / max|u_ref| <= 1e-5 (relative to the
+velocity field's magnitude maximum: a pointwise or per-component relative
+error on a component that is ~0 by symmetry is ill-posed).  The FP64 build
+is compared with the FP64 oracle through the FP32 export, to 1e-6.
 """
 import os
 
@@ -36,10 +38,13 @@ def gpu_run(iv, steps, storage=pkg.STORE_F32, kind=0, amp=0.0, seed=1):
     return d
 
 
-def assert_fields_close(dom, ref, tol=TOL, keys=("den", "ux", "uy", "uz")):
-    den, ux, uy, uz = dom.macroscopic()
-    got = dict(den=den, ux=ux, uy=uy, uz=uz)
-    errs = {k: O.rel_field_err(got[k], ref[k]) for k in keys}
+def field_errs(den, ux, uy, uz, ref):
+    return {"den": O.rel_field_err(den, ref["den"]),
+            "u": O.rel_vel_err((ux, uy, uz), (ref["ux"], ref["uy"], ref["uz"]))}
+
+
+def assert_fields_close(dom, ref, tol=TOL):
+    errs = field_errs(*dom.macroscopic(), ref)
     for k, e in errs.items():
         assert e <= tol, (k, e, errs)
     return errs
@@ -180,8 +185,8 @@ def test_fp64_build_matches_fp64_oracle(iv):
     f = dom.export_arF()  # FP64 state exported as float32
     assert O.rel_field_err(f, r["arF"]) < 1e-6
     den, ux, uy, uz = dom.macroscopic()
-    for got, want in ((den, r["den"]), (ux, r["ux"]), (uy, r["uy"])):
-        assert O.rel_field_err(got, want) < 1e-6
+    assert O.rel_field_err(den, r["den"]) < 1e-6
+    assert O.rel_vel_err((ux, uy, uz), (r["ux"], r["uy"], r["uz"])) < 1e-6
 
 
 @pytest.mark.parametrize("storage,tol", [(pkg.STORE_F16_SHIFT, 1e-3), (pkg.STORE_BF16_SHIFT, 3e-2)])
@@ -223,8 +228,8 @@ def test_kernelcu_reference_pins_oracle_and_library(mrt, les, cs):
     ref = O.Run(iv, init_kind=1, amp=1e-6)
     ref.step(150)
     r = ref.fields()
-    for key in ("den", "ux", "uy", "uz"):
-        assert O.rel_field_err(r[key], k[key]) <= TOL, key
+    errs = field_errs(r["den"], r["ux"], r["uy"], r["uz"], k)
+    assert max(errs.values()) <= TOL, errs
     dom = gpu_run(iv, 150, kind=1, amp=1e-6)
     assert_fields_close(dom, k)
 
@@ -240,8 +245,8 @@ def test_kernelcu_golden(name):
     ref = O.Run(iv, init_kind=int(g["init_kind"]), amp=float(g["noise_amp"]))
     ref.step(int(g["steps"]))
     r = ref.fields()
-    for key in ("den", "ux", "uy", "uz"):
-        assert O.rel_field_err(r[key], g[key]) <= TOL, key
+    errs = field_errs(r["den"], r["ux"], r["uy"], r["uz"], g)
+    assert max(errs.values()) <= TOL, errs
     dom = gpu_run(iv, int(g["steps"]), kind=int(g["init_kind"]), amp=float(g["noise_amp"]))
     assert_fields_close(dom, dict(den=g["den"], ux=g["ux"], uy=g["uy"], uz=g["uz"]))
 
@@ -261,8 +266,8 @@ def test_c2_full_size_properties():
     denb, uxb, uyb, uzb = b.macroscopic()
     db = b.diagnostics()
     b.close()
-    for g, w in ((den, denb), (ux, uxb), (uy, uyb), (uz, uzb)):
-        assert O.rel_field_err(g, w) <= TOL
+    assert O.rel_field_err(den, denb) <= TOL
+    assert O.rel_vel_err((ux, uy, uz), (uxb, uyb, uzb)) <= TOL
     n = 256.0 ** 3
     assert abs(da[0] - db[0]) / n < 1e-6
     assert abs(db[0] - n * 1.0) / n < 1e-6  # noise has zero mean to ~1e-9
