@@ -236,6 +236,7 @@ def main():
     ap.add_argument("--workload", default="cavity256_mrt_les", choices=sorted(WORKLOADS))
     ap.add_argument("--storage", default="f32", choices=["f32", "f16_shift", "bf16_shift", "f64"])
     ap.add_argument("--size", type=int, default=0, help="scale the workload to this nx (profiling)")
+    ap.add_argument("--kernel", default="auto", choices=["auto", "scalar", "packed"])
     ap.add_argument("--no-extras", action="store_true",
                     help="skip cpu baseline, e2e and storage forms (profiling runs)")
     args = ap.parse_args()
@@ -280,7 +281,9 @@ def main():
 
     def timed_steps(storage, k, warm, sampler=None):
         opt = pkg.default_options(storage=storage_id[storage], init_kind=w["init"],
-                                  noise_amp=w["amp"], seed=1, device=local)
+                                  noise_amp=w["amp"], seed=1, device=local,
+                                  kernel={"auto": pkg.KERNEL_AUTO, "scalar": pkg.KERNEL_SCALAR,
+                                          "packed": pkg.KERNEL_PACKED}[args.kernel])
         dom = pkg.Domain(iv, opt)
         dom.set_stream(stream.cuda_stream)
         dom.run(warm)
@@ -324,6 +327,7 @@ def main():
                    "collision": "MRT" if iv.bEnableMRT else "SRT", "les": bool(iv.bEnableLES),
                    "cs": round(float(iv.m_dSmagorinsky), 6), "tau": round(float(iv.m_dTau), 6),
                    "storage": args.storage, "streaming": "pull A/B, fused boundaries",
+                   "kernel": args.kernel,
                    "l2": "inputs larger than L2 (2 lattices of %.2f GB vs 126 MB)" %
                          (19 * BYTES[args.storage] * cells / 1e9),
                    "parallelism": f"replicas x{world}"},

@@ -159,6 +159,13 @@ enum {
   LBM_STREAM_AA = 1    /* in-place AA pattern, one lattice (half memory)   */
 };
 
+/* Kernel variant of the fused step (FP32-arithmetic storage formats). */
+enum {
+  LBM_KERNEL_AUTO = 0,    /* the fastest variant for the format             */
+  LBM_KERNEL_SCALAR = 1,  /* one node per thread                            */
+  LBM_KERNEL_PACKED = 2   /* two nodes per thread, packed FP32 arithmetic   */
+};
+
 typedef struct lbm_options {
   int storage;          /* LBM_STORE_*                                     */
   int init_kind;        /* LBM_INIT_*                                      */
@@ -167,7 +174,8 @@ typedef struct lbm_options {
   float store_scale;    /* *_SHIFT storage scale; 0 = automatic            */
   int stream_mode;      /* LBM_STREAM_*                                    */
   int device;           /* CUDA device ordinal                             */
-  int reserved[8];
+  int kernel;           /* LBM_KERNEL_*                                    */
+  int reserved[7];
 } lbm_options;
 
 /* Fill *opt with the defaults: FP32, reference init, A/B streaming. */

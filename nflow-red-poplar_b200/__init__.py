@@ -39,6 +39,7 @@ LBM_ERR_NO_DEVICE = -9
 STORE_F32, STORE_F16_SHIFT, STORE_BF16_SHIFT, STORE_F64 = 0, 1, 2, 3
 INIT_REFERENCE, INIT_DENSITY_NOISE, INIT_CHANNEL = 0, 1, 2
 STREAM_AB, STREAM_AA = 0, 1
+KERNEL_AUTO, KERNEL_SCALAR, KERNEL_PACKED = 0, 1, 2
 
 
 class Inputval(C.Structure):
@@ -61,7 +62,7 @@ class Options(C.Structure):
     _fields_ = [
         ("storage", C.c_int), ("init_kind", C.c_int), ("seed", C.c_uint64),
         ("noise_amp", C.c_float), ("store_scale", C.c_float), ("stream_mode", C.c_int),
-        ("device", C.c_int), ("reserved", C.c_int * 8),
+        ("device", C.c_int), ("kernel", C.c_int), ("reserved", C.c_int * 7),
     ]
 
 

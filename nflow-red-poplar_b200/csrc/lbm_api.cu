@@ -195,6 +195,26 @@ int with_model(const lbm_domain* d, F&& f) {
   return f(std::integral_constant<int, COLL_SRT>{}, std::false_type{});
 }
 
+// the fused step kernel of the domain's storage: the packed two-node kernel
+// for the FP32-arithmetic formats (unless the scalar one is requested),
+// the scalar kernel for the FP64 build
+template <class S, int COLL, bool LES>
+void launch_step(const lbm_domain* d, const StepArgs<S>& a) {
+  if constexpr (std::is_same<S, double>::value) {
+    const dim3 b = block_of(d->g.nx), gr = grid_of(d->g, b);
+    k_step<S, COLL, LES><<<gr, b, 0, d->stream>>>(a);
+  } else {
+    if (d->opt.kernel == LBM_KERNEL_SCALAR) {
+      const dim3 b = block_of(d->g.nx), gr = grid_of(d->g, b);
+      k_step<S, COLL, LES><<<gr, b, 0, d->stream>>>(a);
+    } else {
+      const int pairs = (d->g.nx + 1) / 2;
+      const dim3 b(64, 1, 1), gr((pairs + 63) / 64, d->g.nz, d->g.ny);
+      k_step2<S, COLL, LES><<<gr, b, 0, d->stream>>>(a);
+    }
+  }
+}
+
 int ensure_device(const lbm_domain* d) {
   CK(cudaSetDevice(d->opt.device));
   return LBM_OK;
@@ -477,7 +497,6 @@ int lbm_run_simulation(lbm_domain* d, int nsteps) {
   rc = with_storage(d->opt.storage, [&](auto tag) -> int {
     using S = typename decltype(tag)::type;
     return with_model<S>(d, [&](auto coll, auto les) -> int {
-      const dim3 b = block_of(d->g.nx), gr = grid_of(d->g, b);
       for (int i = 0; i < nsteps; ++i) {
         const long long k = d->step + 1;
         StepArgs<S> a = make_args<S>(d, d->lat[d->cur], d->lat[d->cur ^ 1], k);
@@ -487,7 +506,7 @@ int lbm_run_simulation(lbm_domain* d, int nsteps) {
           a.uy_out = d->uy;
           a.uz_out = d->uz;
         }
-        k_step<S, decltype(coll)::value, decltype(les)::value><<<gr, b, 0, d->stream>>>(a);
+        launch_step<S, decltype(coll)::value, decltype(les)::value>(d, a);
         d->cur ^= 1;
         d->step = k;
         d->post_direct = false;

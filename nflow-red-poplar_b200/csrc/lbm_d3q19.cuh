@@ -129,29 +129,93 @@ __host__ __device__ constexpr R weight(int q) {
 }
 
 // ------------------------------------------------------------------ //
+// Arithmetic over "lanes": the node arithmetic below is written once for
+// V = float (one node per thread), V = double (the FP64 build) and V = F2
+// (two neighbouring nodes per thread in one register pair, evaluated with
+// the sm_100 packed FP32 instructions: one FFMA2 / FADD2 / FMUL2 does the
+// work of two scalar instructions).
+// ------------------------------------------------------------------ //
+struct F2 {
+  float2 v;
+};
+__host__ __device__ __forceinline__ F2 mk2(float a, float b) {
+  F2 r;
+  r.v = make_float2(a, b);
+  return r;
+}
+__device__ __forceinline__ F2 operator+(F2 a, F2 b) { return F2{__fadd2_rn(a.v, b.v)}; }
+__device__ __forceinline__ F2 operator*(F2 a, F2 b) { return F2{__fmul2_rn(a.v, b.v)}; }
+// a - b as a + b*(-1): the product is exact, so this rounds like a subtraction
+__device__ __forceinline__ F2 operator-(F2 a, F2 b) {
+  return F2{__ffma2_rn(b.v, make_float2(-1.0f, -1.0f), a.v)};
+}
+__device__ __forceinline__ F2 operator-(F2 a) { return mk2(-a.v.x, -a.v.y); }
+__device__ __forceinline__ F2 operator/(F2 a, F2 b) { return mk2(a.v.x / b.v.x, a.v.y / b.v.y); }
+
+__host__ __device__ __forceinline__ float fma_(float a, float b, float c) { return fmaf(a, b, c); }
+__host__ __device__ __forceinline__ double fma_(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ F2 fma_(F2 a, F2 b, F2 c) { return F2{__ffma2_rn(a.v, b.v, c.v)}; }
+
+__host__ __device__ __forceinline__ float vsqrt(float a) { return sqrtf(a); }
+__host__ __device__ __forceinline__ double vsqrt(double a) { return sqrt(a); }
+__device__ __forceinline__ F2 vsqrt(F2 a) { return mk2(sqrtf(a.v.x), sqrtf(a.v.y)); }
+
+// broadcast a compile-time constant to a lane value (rounded once to the
+// lane's precision, like a float literal)
+template <class V>
+__host__ __device__ __forceinline__ V bc(double c);
+template <>
+__host__ __device__ __forceinline__ float bc<float>(double c) { return (float)c; }
+template <>
+__host__ __device__ __forceinline__ double bc<double>(double c) { return c; }
+template <>
+__host__ __device__ __forceinline__ F2 bc<F2>(double c) { return mk2((float)c, (float)c); }
+
+// broadcast a run-time scalar parameter to a lane value
+template <class V, class T>
+__host__ __device__ __forceinline__ V bcast_param(T x) {
+  if constexpr (std::is_same<V, F2>::value) return mk2((float)x, (float)x);
+  else return (V)x;
+}
+
+// acc + c*x for a small integer c (exact for |c| == 1)
+template <int C, class V>
+__host__ __device__ __forceinline__ V acc_term(V acc, V x) {
+  if constexpr (C == 1) return acc + x;
+  else if constexpr (C == -1) return acc - x;
+  else return fma_(bc<V>(C), x, acc);
+}
+template <int C, class V>
+__host__ __device__ __forceinline__ V first_term(V x) {
+  if constexpr (C == 1) return x;
+  else if constexpr (C == -1) return -x;
+  else return bc<V>(C) * x;
+}
+
+// ------------------------------------------------------------------ //
 // Macroscopic moments of the Macroscopic codelet
 // (lbm_codelets.cpp:287-306): rho = sum f, u = (sum c f) / rho, summed in
 // direction order so that the result is bit-identical to the codelet
 // (the skipped terms are exact zeros, the +-1 products are exact).
 // ------------------------------------------------------------------ //
-template <class R>
-__device__ __forceinline__ void macroscopic(const R (&f)[Q], R& rho, R& ux, R& uy, R& uz) {
-  R d = f[0], jx = R(0), jy = R(0), jz = R(0);
+template <class V>
+__device__ __forceinline__ void macroscopic(const V (&f)[Q], V& rho, V& ux, V& uy, V& uz) {
+  V d = f[0], jx, jy, jz;
   static_for<1, Q>([&](auto qc) {
     constexpr int q = decltype(qc)::value;
     d = d + f[q];
     // first non-zero term of each component: q = 1 (x), 5 (y), 3 (z)
     if constexpr (cx(q) != 0) {
       if constexpr (q == 1) jx = f[q];
-      else jx = cx(q) > 0 ? jx + f[q] : jx - f[q];
+      else jx = acc_term<cx(q)>(jx, f[q]);
     }
     if constexpr (cy(q) != 0) {
       if constexpr (q == 5) jy = f[q];
-      else jy = cy(q) > 0 ? jy + f[q] : jy - f[q];
+      else jy = acc_term<cy(q)>(jy, f[q]);
     }
     if constexpr (cz(q) != 0) {
       if constexpr (q == 3) jz = -f[q];
-      else jz = cz(q) > 0 ? jz + f[q] : jz - f[q];
+      else jz = acc_term<cz(q)>(jz, f[q]);
     }
   });
   rho = d;
@@ -169,27 +233,54 @@ __device__ __forceinline__ void macroscopic(const R (&f)[Q], R& rho, R& ux, R& u
 //   tau_eddy = -tau/2 + 1/2 sqrt(tau^2 + 18 sqrt(2) Cs^2 sqrt(Pi:Pi) / rho)
 // les_c = 18*sqrt(2)*Cs^2 (host constant).
 // ------------------------------------------------------------------ //
-template <class R>
-__device__ __forceinline__ R les_tau_eddy(const R (&f)[Q], R rho, R ux, R uy, R uz, R tau, R les_c) {
-  R pxx = R(0), pyy = R(0), pzz = R(0), pxy = R(0), pxz = R(0), pyz = R(0);
+template <class V>
+__device__ __forceinline__ V les_tau_eddy(const V (&f)[Q], V rho, V ux, V uy, V uz, V tau,
+                                          V les_c) {
+  V pxx, pyy, pzz, pxy, pxz, pyz;
   static_for<1, Q>([&](auto qc) {
     constexpr int q = decltype(qc)::value;
-    if constexpr (cx(q) != 0) pxx += f[q];
-    if constexpr (cy(q) != 0) pyy += f[q];
-    if constexpr (cz(q) != 0) pzz += f[q];
-    if constexpr (cx(q) * cy(q) != 0) pxy += (cx(q) * cy(q) > 0 ? f[q] : -f[q]);
-    if constexpr (cx(q) * cz(q) != 0) pxz += (cx(q) * cz(q) > 0 ? f[q] : -f[q]);
-    if constexpr (cy(q) * cz(q) != 0) pyz += (cy(q) * cz(q) > 0 ? f[q] : -f[q]);
+    // first terms: xx q=1, yy q=5, zz q=3, xy q=11, xz q=7, yz q=15
+    if constexpr (cx(q) != 0) {
+      if constexpr (q == 1) pxx = f[q];
+      else pxx = pxx + f[q];
+    }
+    if constexpr (cy(q) != 0) {
+      if constexpr (q == 5) pyy = f[q];
+      else pyy = pyy + f[q];
+    }
+    if constexpr (cz(q) != 0) {
+      if constexpr (q == 3) pzz = f[q];
+      else pzz = pzz + f[q];
+    }
+    if constexpr (cx(q) * cy(q) != 0) {
+      if constexpr (q == 11) pxy = f[q];
+      else pxy = acc_term<cx(q) * cy(q)>(pxy, f[q]);
+    }
+    if constexpr (cx(q) * cz(q) != 0) {
+      if constexpr (q == 7) pxz = -f[q];
+      else pxz = acc_term<cx(q) * cz(q)>(pxz, f[q]);
+    }
+    if constexpr (cy(q) * cz(q) != 0) {
+      if constexpr (q == 15) pyz = -f[q];
+      else pyz = acc_term<cy(q) * cz(q)>(pyz, f[q]);
+    }
   });
-  const R r3 = rho * (R(1) / R(3));
-  const R txx = pxx - r3 - rho * ux * ux;
-  const R tyy = pyy - r3 - rho * uy * uy;
-  const R tzz = pzz - r3 - rho * uz * uz;
-  const R txy = pxy - rho * ux * uy;
-  const R txz = pxz - rho * ux * uz;
-  const R tyz = pyz - rho * uy * uz;
-  const R qq = txx * txx + tyy * tyy + tzz * tzz + R(2) * (txy * txy + txz * txz + tyz * tyz);
-  return R(-0.5) * tau + R(0.5) * sqrt(tau * tau + les_c * sqrt(qq) / rho);
+  const V r3 = rho * bc<V>(1.0 / 3.0);
+  const V jx = rho * ux, jy = rho * uy, jz = rho * uz;
+  const V txx = pxx - fma_(jx, ux, r3);
+  const V tyy = pyy - fma_(jy, uy, r3);
+  const V tzz = pzz - fma_(jz, uz, r3);
+  const V txy = pxy - jx * uy;
+  const V txz = pxz - jx * uz;
+  const V tyz = pyz - jy * uz;
+  V off = txy * txy;
+  off = fma_(txz, txz, off);
+  off = fma_(tyz, tyz, off);
+  V qq = txx * txx;
+  qq = fma_(tyy, tyy, qq);
+  qq = fma_(tzz, tzz, qq);
+  qq = fma_(bc<V>(2), off, qq);
+  return fma_(bc<V>(0.5), vsqrt(fma_(tau, tau, les_c * vsqrt(qq) / rho)), bc<V>(-0.5) * tau);
 }
 
 // ------------------------------------------------------------------ //
@@ -197,17 +288,40 @@ __device__ __forceinline__ R les_tau_eddy(const R (&f)[Q], R rho, R ux, R uy, R 
 //   f* = f - (f - feq)/(tau + tau_eddy),
 //   feq = w rho (1 + 3 c.u + 4.5 (c.u)^2 - 1.5 u^2)
 // ------------------------------------------------------------------ //
-template <class R>
-__device__ __forceinline__ void collide_srt(R (&f)[Q], R rho, R ux, R uy, R uz, R inv_tau) {
-  const R usq15 = R(1.5) * (ux * ux + uy * uy + uz * uz);
+template <class V>
+__device__ __forceinline__ void collide_srt(V (&f)[Q], V rho, V ux, V uy, V uz, V inv_tau) {
+  V usq = ux * ux;
+  usq = fma_(uy, uy, usq);
+  usq = fma_(uz, uz, usq);
+  const V c0 = fma_(bc<V>(-1.5), usq, bc<V>(1));  // 1 - 1.5 u^2
+  const V wr0 = rho * bc<V>(1.0 / 3.0), wr1 = rho * bc<V>(1.0 / 18.0),
+          wr2 = rho * bc<V>(1.0 / 36.0);
   static_for<0, Q>([&](auto qc) {
     constexpr int q = decltype(qc)::value;
-    R eu = R(0);
-    if constexpr (cx(q) != 0) eu = (cx(q) > 0 ? ux : -ux);
-    if constexpr (cy(q) != 0) eu = eu + (cy(q) > 0 ? uy : -uy);
-    if constexpr (cz(q) != 0) eu = eu + (cz(q) > 0 ? uz : -uz);
-    const R feq = weight<R>(q) * rho * (R(1) + R(3) * eu + R(4.5) * eu * eu - usq15);
-    f[q] = f[q] - (f[q] - feq) * inv_tau;
+    V br;
+    if constexpr (q == 0) {
+      br = c0;
+    } else {
+      V eu;
+      bool first = true;
+      if constexpr (cx(q) != 0) {
+        eu = first_term<cx(q)>(ux);
+        first = false;
+      }
+      if constexpr (cy(q) != 0) {
+        if (first) eu = first_term<cy(q)>(uy);
+        else eu = acc_term<cy(q)>(eu, uy);
+        first = false;
+      }
+      if constexpr (cz(q) != 0) {
+        if (first) eu = first_term<cz(q)>(uz);
+        else eu = acc_term<cz(q)>(eu, uz);
+      }
+      br = fma_(eu, fma_(bc<V>(4.5), eu, bc<V>(3)), c0);
+    }
+    const V wr = wclass(q) == 0 ? wr0 : (wclass(q) == 1 ? wr1 : wr2);
+    const V feq = wr * br;
+    f[q] = fma_(feq - f[q], inv_tau, f[q]);
   });
 }
 
@@ -229,79 +343,305 @@ template <int K>
 __host__ __device__ constexpr bool mrt_relaxed() {
   return !(K == 0 || K == 3 || K == 5 || K == 7);
 }
-
-template <class R>
-__device__ __forceinline__ R mrt_rate(int k, R s_nu) {
-  // compile-time k in callers; the switch folds away
-  switch (k) {
-    case 1: return R(1.19);
-    case 2: return R(1.4);
-    case 4: case 6: case 8: return R(1.2);
-    case 10: case 12: return R(1.4);
-    case 16: case 17: case 18: return R(1.98);
-    default: return s_nu;  // 9, 11, 13, 14, 15
-  }
+// relaxation rate of moment K when it is a constant (0 = uses s_nu)
+template <int K>
+__host__ __device__ constexpr double mrt_rate_const() {
+  return K == 1 ? 1.19 : (K == 2 || K == 10 || K == 12) ? 1.4
+       : (K == 4 || K == 6 || K == 8) ? 1.2 : (K >= 16) ? 1.98 : 0.0;
 }
 
-template <class R>
-__device__ __forceinline__ void collide_mrt(R (&f)[Q], R rho, R ux, R uy, R uz, R s_nu,
+template <class V, class R>
+__device__ __forceinline__ void collide_mrt(V (&f)[Q], V rho, V ux, V uy, V uz, V s_nu,
                                             const MrtParams<R>& p) {
-  const R jx = rho * ux, jy = rho * uy, jz = rho * uz;
-  const R jj = jx * jx + jy * jy + jz * jz;
-  const R meq9 = p.rho0_inv * (R(2) * jx * jx - (jy * jy + jz * jz));
-  const R meq11 = p.rho0_inv * (jy * jy - jz * jz);
-  R dm[Q];
+  const V rho0_inv = bcast_param<V>(p.rho0_inv);
+  const V jx = rho * ux, jy = rho * uy, jz = rho * uz;
+  V jj = jx * jx;
+  jj = fma_(jy, jy, jj);
+  jj = fma_(jz, jz, jj);
+  const V jj0 = jj * rho0_inv;
+  const V jyy = jy * jy, jzz = jz * jz;
+  const V meq9 = rho0_inv * fma_(bc<V>(2) * jx, jx, -(jyy + jzz));
+  const V meq11 = rho0_inv * (jyy - jzz);
+  V dm[Q];
   static_for<1, Q>([&](auto kc) {
     constexpr int k = decltype(kc)::value;
     if constexpr (mrt_relaxed<k>()) {
-      R m = R(0);
+      V m;
       bool first = true;
       static_for<0, Q>([&](auto jc) {
         constexpr int j = decltype(jc)::value;
         constexpr int c = mrt_m(k, j);
         if constexpr (c != 0) {
-          if (first) {
-            m = (c == 1) ? f[j] : (c == -1 ? -f[j] : R(c) * f[j]);
-            first = false;
-          } else {
-            m = (c == 1) ? m + f[j] : (c == -1 ? m - f[j] : m + R(c) * f[j]);
-          }
+          if (first) m = first_term<c>(f[j]);
+          else m = acc_term<c>(m, f[j]);
+          first = false;
         }
       });
-      R meq;
-      if constexpr (k == 1) meq = R(-11) * rho + R(19) * p.rho0_inv * jj;
-      if constexpr (k == 2) meq = p.weps * rho + p.wepsj * p.rho0_inv * jj;
-      if constexpr (k == 4) meq = R(-2.0 / 3.0) * jx;
-      if constexpr (k == 6) meq = R(-2.0 / 3.0) * jy;
-      if constexpr (k == 8) meq = R(-2.0 / 3.0) * jz;
+      V meq;
+      if constexpr (k == 1) meq = fma_(bc<V>(19), jj0, bc<V>(-11) * rho);
+      if constexpr (k == 2) meq = fma_(bcast_param<V>(p.wepsj), jj0, bcast_param<V>(p.weps) * rho);
+      if constexpr (k == 4) meq = bc<V>(-2.0 / 3.0) * jx;
+      if constexpr (k == 6) meq = bc<V>(-2.0 / 3.0) * jy;
+      if constexpr (k == 8) meq = bc<V>(-2.0 / 3.0) * jz;
       if constexpr (k == 9) meq = meq9;
-      if constexpr (k == 10) meq = p.wxx * meq9;
+      if constexpr (k == 10) meq = bcast_param<V>(p.wxx) * meq9;
       if constexpr (k == 11) meq = meq11;
-      if constexpr (k == 12) meq = p.wxx * meq11;
-      if constexpr (k == 13) meq = jx * jy * p.rho0_inv;
-      if constexpr (k == 14) meq = jy * jz * p.rho0_inv;
-      if constexpr (k == 15) meq = jz * jx * p.rho0_inv;
-      if constexpr (k >= 16) meq = R(0);
-      dm[k] = mrt_rate<R>(k, s_nu) * (R(1) / R(mrt_norm2(k))) * (m - meq);
+      if constexpr (k == 12) meq = bcast_param<V>(p.wxx) * meq11;
+      if constexpr (k == 13) meq = jx * jy * rho0_inv;
+      if constexpr (k == 14) meq = jy * jz * rho0_inv;
+      if constexpr (k == 15) meq = jz * jx * rho0_inv;
+      constexpr double inv_n2 = 1.0 / (double)mrt_norm2(k);
+      if constexpr (mrt_rate_const<k>() != 0.0) {
+        // constant rate: fold 1/|row|^2 into it at compile time
+        constexpr double sk = mrt_rate_const<k>() * inv_n2;
+        if constexpr (k >= 16)
+          dm[k] = bc<V>(sk) * m;
+        else
+          dm[k] = bc<V>(sk) * (m - meq);
+      } else {
+        dm[k] = (s_nu * bc<V>(inv_n2)) * (m - meq);
+      }
     }
   });
   static_for<0, Q>([&](auto ic) {
     constexpr int i = decltype(ic)::value;
-    R acc = R(0);
+    V acc;
     bool first = true;
     static_for<1, Q>([&](auto kc) {
       constexpr int k = decltype(kc)::value;
       constexpr int c = mrt_m(k, i);
       if constexpr (mrt_relaxed<k>() && c != 0) {
-        if (first) {
-          acc = (c == 1) ? dm[k] : (c == -1 ? -dm[k] : R(c) * dm[k]);
-          first = false;
-        } else {
-          acc = (c == 1) ? acc + dm[k] : (c == -1 ? acc - dm[k] : acc + R(c) * dm[k]);
-        }
+        if (first) acc = first_term<c>(dm[k]);
+        else acc = acc_term<c>(acc, dm[k]);
+        first = false;
       }
     });
     f[i] = f[i] - acc;
+  });
+}
+
+
+// ------------------------------------------------------------------ //
+// Opposite-pair form of the node arithmetic.  With s_p = f_a + f_abar and
+// d_p = f_a - f_abar for the nine pairs (a, abar = opp(a)), every even
+// moment row of M (symmetric under c -> -c: rho, e, eps, the stress rows
+// 9-15) reads only s, every odd row (momentum, energy flux, 16-18) only d,
+// and the back transform M^T dm splits into a part E_p common to a and abar
+// and a part O_p of opposite sign.  This is the same linear algebra as
+// collide_mrt above with about half the operations.
+// ------------------------------------------------------------------ //
+__host__ __device__ constexpr int pair_a(int p) {
+  constexpr int t[9] = {1, 3, 5, 7, 8, 11, 12, 15, 16};
+  return t[p];
+}
+
+template <class V>
+struct PairState {
+  V f0, s[9], d[9];
+  V rho, jx, jy, jz;  // rho and momentum sum c f
+};
+
+template <class V>
+__host__ __device__ __forceinline__ void make_pairs(const V (&f)[Q], PairState<V>& ps) {
+  ps.f0 = f[0];
+  static_for<0, 9>([&](auto pc) {
+    constexpr int p = decltype(pc)::value;
+    ps.s[p] = f[pair_a(p)] + f[opp(pair_a(p))];
+    ps.d[p] = f[pair_a(p)] - f[opp(pair_a(p))];
+  });
+  // rho = f0 + sum s; j_alpha = sum_p c_alpha(a_p) d_p
+  V acc = ps.s[0] + ps.s[1];
+  acc = acc + ps.s[2];
+  V diag = ps.s[3] + ps.s[4];
+  diag = diag + ps.s[5];
+  diag = diag + ps.s[6];
+  diag = diag + ps.s[7];
+  diag = diag + ps.s[8];
+  ps.rho = ps.f0 + (acc + diag);
+  V jx = ps.d[0] + ps.d[3];
+  jx = jx - ps.d[4];
+  jx = jx + ps.d[5];
+  ps.jx = jx - ps.d[6];
+  V jy = ps.d[2] + ps.d[5];
+  jy = jy + ps.d[6];
+  jy = jy + ps.d[7];
+  ps.jy = jy + ps.d[8];
+  V jz = ps.d[8] - ps.d[1];
+  jz = jz - ps.d[3];
+  jz = jz - ps.d[4];
+  ps.jz = jz - ps.d[7];
+}
+
+// Smagorinsky tau_eddy from the pair sums (same closed form as les_tau_eddy)
+template <class V>
+__host__ __device__ __forceinline__ V les_tau_eddy_pairs(const PairState<V>& ps, V ux, V uy, V uz,
+                                                         V tau, V les_c) {
+  const V* s = ps.s;
+  V pxx = s[0] + s[3];
+  pxx = pxx + s[4];
+  pxx = pxx + s[5];
+  pxx = pxx + s[6];
+  V pyy = s[2] + s[5];
+  pyy = pyy + s[6];
+  pyy = pyy + s[7];
+  pyy = pyy + s[8];
+  V pzz = s[1] + s[3];
+  pzz = pzz + s[4];
+  pzz = pzz + s[7];
+  pzz = pzz + s[8];
+  const V pxy = s[5] - s[6];  // f11 - f12 - f13 + f14
+  const V pxz = s[4] - s[3];  // -f7 + f8 + f9 - f10
+  const V pyz = s[8] - s[7];  // -f15 + f16 + f17 - f18
+  const V r3 = ps.rho * bc<V>(1.0 / 3.0);
+  const V txx = pxx - fma_(ps.jx, ux, r3);
+  const V tyy = pyy - fma_(ps.jy, uy, r3);
+  const V tzz = pzz - fma_(ps.jz, uz, r3);
+  const V txy = pxy - ps.jx * uy;
+  const V txz = pxz - ps.jx * uz;
+  const V tyz = pyz - ps.jy * uz;
+  V off = txy * txy;
+  off = fma_(txz, txz, off);
+  off = fma_(tyz, tyz, off);
+  V qq = txx * txx;
+  qq = fma_(tyy, tyy, qq);
+  qq = fma_(tzz, tzz, qq);
+  qq = fma_(bc<V>(2), off, qq);
+  return fma_(bc<V>(0.5), vsqrt(fma_(tau, tau, les_c * vsqrt(qq) / ps.rho)),
+              bc<V>(-0.5) * tau);
+}
+
+// SRT in pair form: feq_a, feq_abar share w rho (1 - 1.5u^2 + 4.5 (c.u)^2)
+// and differ in the sign of 3 w rho c.u.
+template <class V>
+__host__ __device__ __forceinline__ void collide_srt_pairs(V (&f)[Q], const PairState<V>& ps,
+                                                           V ux, V uy, V uz, V inv_tau) {
+  V usq = ux * ux;
+  usq = fma_(uy, uy, usq);
+  usq = fma_(uz, uz, usq);
+  const V c0 = fma_(bc<V>(-1.5), usq, bc<V>(1));
+  const V rho = ps.rho;
+  f[0] = fma_((rho * bc<V>(1.0 / 3.0)) * c0 - f[0], inv_tau, f[0]);
+  const V wr1 = rho * bc<V>(1.0 / 18.0), wr2 = rho * bc<V>(1.0 / 36.0);
+  static_for<0, 9>([&](auto pc) {
+    constexpr int p = decltype(pc)::value;
+    constexpr int a = pair_a(p), b = opp(a);
+    V eu;
+    bool first = true;
+    if constexpr (cx(a) != 0) {
+      eu = first_term<cx(a)>(ux);
+      first = false;
+    }
+    if constexpr (cy(a) != 0) {
+      if (first) eu = first_term<cy(a)>(uy);
+      else eu = acc_term<cy(a)>(eu, uy);
+      first = false;
+    }
+    if constexpr (cz(a) != 0) {
+      if (first) eu = first_term<cz(a)>(uz);
+      else eu = acc_term<cz(a)>(eu, uz);
+    }
+    const V wr = wclass(a) == 1 ? wr1 : wr2;
+    const V even = wr * fma_(bc<V>(4.5) * eu, eu, c0);
+    const V odd = (bc<V>(3) * wr) * eu;
+    const V fa = even + odd, fb = even - odd;
+    f[a] = fma_(fa - f[a], inv_tau, f[a]);
+    f[b] = fma_(fb - f[b], inv_tau, f[b]);
+  });
+}
+
+// MRT in pair form (Collision_MRT, lbm_codelets.cpp:449-544), moments
+// formed from s/d, relaxation dm'_k = s_k (m_k - meq_k) / |row_k|^2, back
+// transform f_a -= E_p + O_p, f_abar -= E_p - O_p.
+template <class V, class R>
+__host__ __device__ __forceinline__ void collide_mrt_pairs(V (&f)[Q], const PairState<V>& ps,
+                                                           V s_nu, const MrtParams<R>& p) {
+  const V* s = ps.s;
+  const V* d = ps.d;
+  const V rho = ps.rho, jx = ps.jx, jy = ps.jy, jz = ps.jz;
+  const V rho0_inv = bcast_param<V>(p.rho0_inv);
+  // ---- moments (rows of main.cpp:150-171 expressed in s, d) ----
+  const V A = (s[0] + s[1]) + s[2];                                  // axis pairs
+  const V B = ((((s[3] + s[4]) + s[5]) + s[6]) + s[7]) + s[8];       // diagonal pairs
+  const V m1 = fma_(bc<V>(-30), ps.f0, fma_(bc<V>(-11), A, bc<V>(8) * B));
+  const V m2 = fma_(bc<V>(12), ps.f0, fma_(bc<V>(-4), A, B));
+  const V G = ((s[3] + s[4]) + s[5]) + s[6];                          // x-diagonals
+  const V H = s[7] + s[8];                                             // yz-diagonals
+  const V s12 = s[1] + s[2];
+  const V GmH = fma_(bc<V>(-2), H, G);
+  const V m9 = fma_(bc<V>(2), s[0], GmH - s12);
+  const V m10 = fma_(bc<V>(-4), s[0], fma_(bc<V>(2), s12, GmH));
+  const V K = (s[5] + s[6]) - (s[3] + s[4]);
+  const V m11 = (s[2] - s[1]) + K;
+  const V m12 = fma_(bc<V>(2), s[1] - s[2], K);
+  const V m13 = s[5] - s[6];
+  const V m14 = s[8] - s[7];
+  const V m15 = s[4] - s[3];
+  const V m4 = fma_(bc<V>(-5), d[0], jx);
+  const V m6 = fma_(bc<V>(-5), d[2], jy);
+  const V m8 = fma_(bc<V>(5), d[1], jz);
+  const V m16 = ((d[4] - d[3]) + d[5]) - d[6];
+  const V m17 = ((d[7] - d[5]) - d[6]) + d[8];
+  const V m18 = ((d[7] - d[3]) - d[4]) - d[8];
+  // ---- equilibrium moments (lbm_codelets.cpp:468-486) ----
+  V jj = jx * jx;
+  jj = fma_(jy, jy, jj);
+  jj = fma_(jz, jz, jj);
+  const V jj0 = jj * rho0_inv;
+  const V jyy = jy * jy, jzz = jz * jz;
+  const V meq9 = rho0_inv * fma_(bc<V>(2) * jx, jx, -(jyy + jzz));
+  const V meq11 = rho0_inv * (jyy - jzz);
+  // ---- relaxed, pre-scaled differences dm'_k = s_k (m_k - meq_k)/|row|^2 ----
+  const V e1 = bc<V>(1.19 / 2394.0) * (m1 - fma_(bc<V>(19), jj0, bc<V>(-11) * rho));
+  const V e2 = bc<V>(1.4 / 252.0) *
+               (m2 - fma_(bcast_param<V>(p.wepsj), jj0, bcast_param<V>(p.weps) * rho));
+  const V e4 = bc<V>(1.2 / 40.0) * fma_(bc<V>(2.0 / 3.0), jx, m4);
+  const V e6 = bc<V>(1.2 / 40.0) * fma_(bc<V>(2.0 / 3.0), jy, m6);
+  const V e8 = bc<V>(1.2 / 40.0) * fma_(bc<V>(2.0 / 3.0), jz, m8);
+  const V e9 = (s_nu * bc<V>(1.0 / 36.0)) * (m9 - meq9);
+  const V e10 = bc<V>(1.4 / 72.0) * (m10 - bcast_param<V>(p.wxx) * meq9);
+  const V e11 = (s_nu * bc<V>(1.0 / 12.0)) * (m11 - meq11);
+  const V e12 = bc<V>(1.4 / 24.0) * (m12 - bcast_param<V>(p.wxx) * meq11);
+  const V snu4 = s_nu * bc<V>(1.0 / 4.0);
+  const V e13 = snu4 * (m13 - (jx * jy) * rho0_inv);
+  const V e14 = snu4 * (m14 - (jy * jz) * rho0_inv);
+  const V e15 = snu4 * (m15 - (jz * jx) * rho0_inv);
+  const V e16 = bc<V>(1.98 / 8.0) * m16;
+  const V e17 = bc<V>(1.98 / 8.0) * m17;
+  const V e18 = bc<V>(1.98 / 8.0) * m18;
+  // ---- back transform, f -= M^T dm' ----
+  f[0] = f[0] - fma_(bc<V>(-30), e1, bc<V>(12) * e2);
+  const V eax = fma_(bc<V>(-11), e1, bc<V>(-4) * e2);  // rows 1,2 on axis directions
+  const V edg = fma_(bc<V>(8), e1, e2);                 // rows 1,2 on diagonals
+  const V g910 = e9 + e10;
+  const V g1112 = e11 + e12;
+  const V ax_yz = fma_(bc<V>(2), e10, eax - e9);       // -e9 + 2 e10 + eax (z and y axes)
+  const V dxz = edg + (g910 - g1112);                   // x-z diagonals share
+  const V dxy = edg + (g910 + g1112);                   // x-y diagonals share
+  const V dyz = fma_(bc<V>(-2), g910, edg);             // y-z diagonals share
+  V E[9], O[9];
+  E[0] = fma_(bc<V>(2), e9, fma_(bc<V>(-4), e10, eax));  // a=1
+  O[0] = bc<V>(-4) * e4;
+  E[1] = fma_(bc<V>(2), e12, ax_yz - e11);                // a=3 (0,0,-1)
+  O[1] = bc<V>(4) * e8;
+  E[2] = fma_(bc<V>(-2), e12, ax_yz + e11);               // a=5 (0,1,0)
+  O[2] = bc<V>(-4) * e6;
+  E[3] = dxz - e15;                                       // a=7 (1,0,-1)
+  O[3] = ((e4 - e8) - e16) - e18;
+  E[4] = dxz + e15;                                       // a=8 (-1,0,-1)
+  O[4] = ((e16 - e4) - e8) - e18;
+  E[5] = dxy + e13;                                       // a=11 (1,1,0)
+  O[5] = ((e4 + e6) + e16) - e17;
+  E[6] = dxy - e13;                                       // a=12 (-1,1,0)
+  O[6] = ((e6 - e4) - e16) - e17;
+  E[7] = dyz - e14;                                       // a=15 (0,1,-1)
+  O[7] = ((e6 - e8) + e17) + e18;
+  E[8] = dyz + e14;                                       // a=16 (0,1,1)
+  O[8] = ((e6 + e8) + e17) - e18;
+  static_for<0, 9>([&](auto pc) {
+    constexpr int q = decltype(pc)::value;
+    constexpr int a = pair_a(q), b = opp(a);
+    f[a] = f[a] - (E[q] + O[q]);
+    f[b] = f[b] - (E[q] - O[q]);
   });
 }
 

@@ -177,17 +177,29 @@ __device__ __forceinline__ void pull(RealOf<S> (&f)[Q], const StepArgs<S>& a, in
 
 enum { COLL_SRT = 0, COLL_MRT = 1 };
 
-template <class S, int COLL, bool LES>
-__device__ __forceinline__ void collide(RealOf<S> (&f)[Q], RealOf<S> rho, RealOf<S> ux,
-                                        RealOf<S> uy, RealOf<S> uz, const StepArgs<S>& a) {
-  using R = RealOf<S>;
-  R te = R(0);
-  if constexpr (LES) te = les_tau_eddy<R>(f, rho, ux, uy, uz, a.tau, a.les_c);
-  const R inv = R(1) / (a.tau + te);
+// LES + collision of one node (or one F2 pair of nodes) in pair form.  ps
+// holds the pair sums of f and the density / momentum the equilibrium is
+// built from; u = j / rho.
+template <class S, int COLL, bool LES, class V>
+__device__ __forceinline__ void collide_node(V (&f)[Q], const PairState<V>& ps, V ux, V uy,
+                                             V uz, const StepArgs<S>& a) {
+  const V tau = bcast_param<V>(a.tau);
+  V te = bc<V>(0);
+  if constexpr (LES) te = les_tau_eddy_pairs<V>(ps, ux, uy, uz, tau, bcast_param<V>(a.les_c));
+  const V inv = bc<V>(1) / (tau + te);
   if constexpr (COLL == COLL_SRT)
-    collide_srt<R>(f, rho, ux, uy, uz, inv);
+    collide_srt_pairs<V>(f, ps, ux, uy, uz, inv);
   else
-    collide_mrt<R>(f, rho, ux, uy, uz, inv, a.mp);
+    collide_mrt_pairs<V>(f, ps, inv, a.mp);
+}
+
+// rho, u of a node from its pair sums (u = j * (1/rho))
+template <class V>
+__device__ __forceinline__ void velocity(const PairState<V>& ps, V& ux, V& uy, V& uz) {
+  const V inv = bc<V>(1) / ps.rho;
+  ux = ps.jx * inv;
+  uy = ps.jy * inv;
+  uz = ps.jz * inv;
 }
 
 // Side outputs of the macroscopic state of arF_k.
@@ -237,10 +249,12 @@ __global__ void __launch_bounds__(128) k_step(const __grid_constant__ StepArgs<S
   const long long cell = x + (long long)a.g.px * (z + (long long)a.g.nz * y);
   R f[Q];
   pull<S>(f, a, x, y, z, cell);
-  R rho, ux, uy, uz;
-  macroscopic<R>(f, rho, ux, uy, uz);
-  write_macro<S>(a, x, y, z, rho, ux, uy, uz);
-  collide<S, COLL, LES>(f, rho, ux, uy, uz, a);
+  PairState<R> ps;
+  make_pairs<R>(f, ps);
+  R ux, uy, uz;
+  velocity<R>(ps, ux, uy, uz);
+  write_macro<S>(a, x, y, z, ps.rho, ux, uy, uz);
+  collide_node<S, COLL, LES, R>(f, ps, ux, uy, uz, a);
   store_all<S>(a, f, cell);
 }
 
@@ -311,7 +325,14 @@ __global__ void __launch_bounds__(128)
   });
   store_all<S>(a, f, cell);  // post-stream lattice
   write_macro<S>(a, x, y, z, rd, ux, uy, uz);
-  collide<S, COLL, LES>(f, rd, ux, uy, uz, a);
+  // the first step collides with the rho, u that Initialize stored
+  PairState<R> ps;
+  make_pairs<R>(f, ps);
+  ps.rho = rd;
+  ps.jx = rd * ux;
+  ps.jy = rd * uy;
+  ps.jz = rd * uz;
+  collide_node<S, COLL, LES, R>(f, ps, ux, uy, uz, a);
   static_for<0, Q>([&](auto qc) {
     constexpr int q = decltype(qc)::value;
     StoreTraits<S>::store(collided + q * a.qs + cell, f[q], weight<R>(q), a.scale);
@@ -349,9 +370,12 @@ __global__ void __launch_bounds__(128)
     f[q] = ld(a.dst + q * a.qs + cell, q, a.inv_scale);
   });
   R rho, ux, uy, uz;
-  macroscopic<R>(f, rho, ux, uy, uz);
+  macroscopic<R>(f, rho, ux, uy, uz);  // CurrDen / CurrVel in the codelet's order
   write_macro<S>(a, x, y, z, rho, ux, uy, uz);
-  collide<S, COLL, LES>(f, rho, ux, uy, uz, a);
+  PairState<R> ps;
+  make_pairs<R>(f, ps);
+  velocity<R>(ps, ux, uy, uz);
+  collide_node<S, COLL, LES, R>(f, ps, ux, uy, uz, a);
   static_for<0, Q>([&](auto qc) {
     constexpr int q = decltype(qc)::value;
     StoreTraits<S>::store(collided + q * a.qs + cell, f[q], weight<R>(q), a.scale);
@@ -391,6 +415,110 @@ __global__ void __launch_bounds__(128)
     constexpr int q = decltype(qc)::value;
     aos[q + node * Q] = (float)f[q];
   });
+}
+
+// ------------------------------------------------------------------ //
+// Two nodes per thread: the pair (x0, x0+1), x0 even.  Populations with
+// c_x = 0 are read as one aligned 2-element vector, the others as two
+// scalars; all node arithmetic runs on F2 lanes (packed FP32), and the
+// pair is stored as one vector per population.  A pair that touches the
+// domain boundary takes the per-node boundary path and is packed after.
+// ------------------------------------------------------------------ //
+template <class S>
+__device__ __forceinline__ F2 ld_pair(const S* p, int q, float inv_scale);
+template <>
+__device__ __forceinline__ F2 ld_pair<float>(const float* p, int, float) {
+  return F2{*reinterpret_cast<const float2*>(p)};
+}
+template <>
+__device__ __forceinline__ F2 ld_pair<__half>(const __half* p, int q, float inv_scale) {
+  const float2 h = __half22float2(*reinterpret_cast<const __half2*>(p));
+  const float w = weight<float>(q);
+  return F2{__ffma2_rn(h, make_float2(inv_scale, inv_scale), make_float2(w, w))};
+}
+template <>
+__device__ __forceinline__ F2 ld_pair<__nv_bfloat16>(const __nv_bfloat16* p, int q,
+                                                     float inv_scale) {
+  const float2 h = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(p));
+  const float w = weight<float>(q);
+  return F2{__ffma2_rn(h, make_float2(inv_scale, inv_scale), make_float2(w, w))};
+}
+
+template <class S>
+__device__ __forceinline__ void st_pair(S* p, F2 v, int q, float scale);
+template <>
+__device__ __forceinline__ void st_pair<float>(float* p, F2 v, int, float) {
+  *reinterpret_cast<float2*>(p) = v.v;
+}
+template <>
+__device__ __forceinline__ void st_pair<__half>(__half* p, F2 v, int q, float scale) {
+  const float w = weight<float>(q);
+  const float2 d = __fmul2_rn(__fadd2_rn(v.v, make_float2(-w, -w)), make_float2(scale, scale));
+  *reinterpret_cast<__half2*>(p) = __float22half2_rn(d);
+}
+template <>
+__device__ __forceinline__ void st_pair<__nv_bfloat16>(__nv_bfloat16* p, F2 v, int q,
+                                                       float scale) {
+  const float w = weight<float>(q);
+  const float2 d = __fmul2_rn(__fadd2_rn(v.v, make_float2(-w, -w)), make_float2(scale, scale));
+  *reinterpret_cast<__nv_bfloat162*>(p) = __float22bfloat162_rn(d);
+}
+
+template <class S, int COLL, bool LES>
+__global__ void __launch_bounds__(64) k_step2(const __grid_constant__ StepArgs<S> a) {
+  static_assert(std::is_same<RealOf<S>, float>::value, "packed kernel is FP32 arithmetic");
+  const int x0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  const int z = blockIdx.y, y = blockIdx.z;
+  if (x0 >= a.g.nx) return;
+  const long long cell = x0 + (long long)a.g.px * (z + (long long)a.g.nz * y);
+  const bool two = x0 + 1 < a.g.nx;
+  const bool interior = x0 >= 1 && x0 + 1 <= a.g.nx - 2 && y >= 1 && y <= a.g.ny - 2 && z >= 1 &&
+                        z <= a.g.nz - 2;
+  F2 f[Q];
+  if (interior) {
+    const long long sz = a.g.px, sy = (long long)a.g.px * a.g.nz;
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      const S* p = a.src + q * a.qs + cell - (cz(q) * sz + cy(q) * sy);
+      if constexpr (cx(q) == 0) {
+        f[q] = ld_pair<S>(p, q, a.inv_scale);
+      } else {
+        f[q] = mk2(ld(p - cx(q), q, a.inv_scale), ld(p + 1 - cx(q), q, a.inv_scale));
+      }
+    });
+  } else {
+    float fa[Q], fb[Q];
+    pull<S>(fa, a, x0, y, z, cell);
+    if (two) {
+      pull<S>(fb, a, x0 + 1, y, z, cell + 1);
+    } else {
+      static_for<0, Q>([&](auto qc) { fb[decltype(qc)::value] = fa[decltype(qc)::value]; });
+    }
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      f[q] = mk2(fa[q], fb[q]);
+    });
+  }
+  PairState<F2> ps;
+  make_pairs<F2>(f, ps);
+  F2 ux, uy, uz;
+  velocity<F2>(ps, ux, uy, uz);
+  if (a.den_out || a.ux_out || a.g.casetype == CHANNEL) {
+    write_macro<S>(a, x0, y, z, ps.rho.v.x, ux.v.x, uy.v.x, uz.v.x);
+    if (two) write_macro<S>(a, x0 + 1, y, z, ps.rho.v.y, ux.v.y, uy.v.y, uz.v.y);
+  }
+  collide_node<S, COLL, LES, F2>(f, ps, ux, uy, uz, a);
+  if (two) {
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      st_pair<S>(a.dst + q * a.qs + cell, f[q], q, a.scale);
+    });
+  } else {
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      StoreTraits<S>::store(a.dst + q * a.qs + cell, f[q].v.x, weight<float>(q), a.scale);
+    });
+  }
 }
 
 // node type and inside mask per node, [ny][nz][nx]

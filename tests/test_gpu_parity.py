@@ -271,9 +271,15 @@ def test_c2_full_size_properties():
     n = 256.0 ** 3
     assert abs(da[0] - db[0]) / n < 1e-6
     assert abs(db[0] - n * 1.0) / n < 1e-6  # noise has zero mean to ~1e-9
-    mirror = ux[:, ::-1, :]
-    assert np.abs(ux - mirror).max() <= 1e-6 * np.abs(ux).max() + 1e-9
-    assert np.abs(uz + uz[:, ::-1, :]).max() <= 1e-5 * np.abs(ux).max()
+    # z-mirror symmetry holds up to FP32 rounding when the initial state is
+    # symmetric (the seeded noise is not), so check it on the reference init
+    c = gpu_run(iv, 60, kind=pkg.INIT_REFERENCE)
+    den, ux, uy, uz = c.macroscopic()
+    c.close()
+    um = np.abs(ux).max()
+    assert np.abs(ux - ux[:, ::-1, :]).max() <= 1e-5 * um
+    assert np.abs(uy - uy[:, ::-1, :]).max() <= 1e-5 * um
+    assert np.abs(uz + uz[:, ::-1, :]).max() <= 1e-5 * um
 
 
 def test_run_ms_and_external_stream():
