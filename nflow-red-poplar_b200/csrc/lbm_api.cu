@@ -57,7 +57,14 @@ struct lbm_domain {
   int last_steps = 0;
   float scale = 1.f, inv_scale = 1.f;
   size_t bytes = 0;
+  // CUDA graphs of kGraphSteps plain steps, one per starting lattice
+  cudaGraphExec_t chunk[2] = {nullptr, nullptr};
+  cudaStream_t capture = nullptr;
 };
+
+// steps per captured graph chunk (even, so that a chunk returns the lattices
+// and the boundary planes to the parity it started from)
+constexpr int kGraphSteps = 32;
 
 namespace {
 
@@ -96,8 +103,8 @@ int validate(const Inputval* in, const lbm_options* opt) {
                      in->nx, in->ny, in->nz);
   if (in->ny > 65535 || in->nz > 65535)
     return set_error(LBM_ERR_INVALID, "ny and nz must be <= 65535");
-  if ((long long)in->nx * in->ny * in->nz > (1LL << 40))
-    return set_error(LBM_ERR_INVALID, "domain too large");
+  if (round_up(in->nx, 8) * (long long)in->ny * in->nz >= (1LL << 31) - 1024)
+    return set_error(LBM_ERR_INVALID, "domain too large (px*ny*nz must be < 2^31)");
   if (in->casetype != CAVITY && in->casetype != CHANNEL)
     return set_error(LBM_ERR_INVALID,
                      "casetype %d not supported (CAVITY=1 and CHANNEL=2 are implemented)",
@@ -129,11 +136,17 @@ struct Sizes {
   int px;
 };
 
+// Extra elements between population planes (a multiple of 128); a non-zero
+// value keeps the 19 streams of a node off power-of-two distances.
+#ifndef LBM_PLANE_PAD
+#define LBM_PLANE_PAD 0
+#endif
+
 Sizes sizes_of(const Inputval* in) {
   Sizes s;
   s.px = (int)round_up(in->nx, 8);
   s.N = (long long)in->nx * in->ny * in->nz;
-  s.qs = round_up((long long)s.px * in->nz * in->ny, 128);
+  s.qs = round_up((long long)s.px * in->nz * in->ny, 128) + LBM_PLANE_PAD;
   s.P = (long long)in->ny * in->nz;
   return s;
 }
@@ -163,6 +176,11 @@ StepArgs<S> make_args(const lbm_domain* d, const void* src, void* dst, long long
   a.src = (const S*)src;
   a.dst = (S*)dst;
   a.qs = d->qs;
+  for (int q = 0; q < Q; ++q) {
+    a.srcq[q] = src ? (const S*)src + q * d->qs : nullptr;
+    a.dstq[q] = dst ? (S*)dst + q * d->qs : nullptr;
+    a.off[q] = cx(q) + d->g.px * (cz(q) + d->g.nz * cy(q));
+  }
   a.g = d->g;
   a.tau = R(d->in.m_dTau);
   const double cs = (double)d->in.m_dSmagorinsky;
@@ -199,20 +217,17 @@ int with_model(const lbm_domain* d, F&& f) {
 // for the FP32-arithmetic formats (unless the scalar one is requested),
 // the scalar kernel for the FP64 build
 template <class S, int COLL, bool LES>
-void launch_step(const lbm_domain* d, const StepArgs<S>& a) {
-  if constexpr (std::is_same<S, double>::value) {
-    const dim3 b = block_of(d->g.nx), gr = grid_of(d->g, b);
-    k_step<S, COLL, LES><<<gr, b, 0, d->stream>>>(a);
-  } else {
-    if (d->opt.kernel == LBM_KERNEL_SCALAR) {
-      const dim3 b = block_of(d->g.nx), gr = grid_of(d->g, b);
-      k_step<S, COLL, LES><<<gr, b, 0, d->stream>>>(a);
-    } else {
+void launch_step(const lbm_domain* d, const StepArgs<S>& a, cudaStream_t st) {
+  if constexpr (!std::is_same<S, double>::value) {
+    if (d->opt.kernel == LBM_KERNEL_PACKED) {
       const int pairs = (d->g.nx + 1) / 2;
       const dim3 b(64, 1, 1), gr((pairs + 63) / 64, d->g.nz, d->g.ny);
-      k_step2<S, COLL, LES><<<gr, b, 0, d->stream>>>(a);
+      k_step2<S, COLL, LES><<<gr, b, 0, st>>>(a);
+      return;
     }
   }
+  const dim3 b = block_of(d->g.nx), gr = grid_of(d->g, b);
+  k_step<S, COLL, LES><<<gr, b, 0, st>>>(a);
 }
 
 int ensure_device(const lbm_domain* d) {
@@ -249,6 +264,9 @@ void free_all(lbm_domain* d) {
   if (d->flag) cudaFree(d->flag);
   if (d->partial) cudaFree(d->partial);
   if (d->dout) cudaFree(d->dout);
+  for (int i = 0; i < 2; ++i)
+    if (d->chunk[i]) cudaGraphExecDestroy(d->chunk[i]);
+  if (d->capture) cudaStreamDestroy(d->capture);
   if (d->ev0) cudaEventDestroy(d->ev0);
   if (d->ev1) cudaEventDestroy(d->ev1);
   if (d->own) cudaStreamDestroy(d->own);
@@ -497,20 +515,55 @@ int lbm_run_simulation(lbm_domain* d, int nsteps) {
   rc = with_storage(d->opt.storage, [&](auto tag) -> int {
     using S = typename decltype(tag)::type;
     return with_model<S>(d, [&](auto coll, auto les) -> int {
-      for (int i = 0; i < nsteps; ++i) {
-        const long long k = d->step + 1;
-        StepArgs<S> a = make_args<S>(d, d->lat[d->cur], d->lat[d->cur ^ 1], k);
-        if (i >= nsteps - 2) a.den_out = d->den[k & 1];
-        if (i == nsteps - 1) {
+      constexpr int C = decltype(coll)::value;
+      constexpr bool L = decltype(les)::value;
+      // one plain step (no side outputs unless requested)
+      auto step_args = [&](long long k, bool den, bool vel, int cur) {
+        StepArgs<S> a = make_args<S>(d, d->lat[cur], d->lat[cur ^ 1], k);
+        if (den) a.den_out = d->den[k & 1];
+        if (vel) {
           a.ux_out = d->ux;
           a.uy_out = d->uy;
           a.uz_out = d->uz;
         }
-        launch_step<S, decltype(coll)::value, decltype(les)::value>(d, a);
+        return a;
+      };
+      int plain = nsteps > 2 ? nsteps - 2 : 0;  // the last two steps write rho / u
+      // whole graph chunks of kGraphSteps plain steps
+      if (plain >= 2 * kGraphSteps) {
+        cudaGraphExec_t& g = d->chunk[d->cur];
+        if (!g) {
+          if (!d->capture) CK(cudaStreamCreateWithFlags(&d->capture, cudaStreamNonBlocking));
+          CK(cudaStreamBeginCapture(d->capture, cudaStreamCaptureModeThreadLocal));
+          int cur = d->cur;
+          long long k = d->step;
+          for (int i = 0; i < kGraphSteps; ++i) {
+            ++k;
+            launch_step<S, C, L>(d, step_args(k, false, false, cur), d->capture);
+            cur ^= 1;
+          }
+          cudaGraph_t graph;
+          CK(cudaStreamEndCapture(d->capture, &graph));
+          cudaError_t e = cudaGraphInstantiate(&g, graph, 0);
+          cudaGraphDestroy(graph);
+          if (e != cudaSuccess)
+            return set_error(LBM_ERR_CUDA, "graph instantiation failed: %s",
+                             cudaGetErrorString(e));
+        }
+        while (plain >= kGraphSteps) {
+          CK(cudaGraphLaunch(g, d->stream));
+          d->step += kGraphSteps;  // even: cur and plane parity unchanged
+          plain -= kGraphSteps;
+        }
+      }
+      const int rest = plain + (nsteps > 2 ? 2 : nsteps);
+      for (int i = 0; i < rest; ++i) {
+        const long long k = d->step + 1;
+        launch_step<S, C, L>(d, step_args(k, i >= rest - 2, i == rest - 1, d->cur), d->stream);
         d->cur ^= 1;
         d->step = k;
-        d->post_direct = false;
       }
+      d->post_direct = false;
       CK(cudaGetLastError());
       return LBM_OK;
     });

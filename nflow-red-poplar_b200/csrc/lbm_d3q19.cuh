@@ -156,6 +156,17 @@ __host__ __device__ __forceinline__ float fma_(float a, float b, float c) { retu
 __host__ __device__ __forceinline__ double fma_(double a, double b, double c) { return fma(a, b, c); }
 __device__ __forceinline__ F2 fma_(F2 a, F2 b, F2 c) { return F2{__ffma2_rn(a.v, b.v, c.v)}; }
 
+// 1/x rounded to nearest (one reciprocal instead of a full division)
+__host__ __device__ __forceinline__ float vrcp(float a) {
+#ifdef __CUDA_ARCH__
+  return __frcp_rn(a);
+#else
+  return 1.0f / a;
+#endif
+}
+__host__ __device__ __forceinline__ double vrcp(double a) { return 1.0 / a; }
+__device__ __forceinline__ F2 vrcp(F2 a) { return mk2(__frcp_rn(a.v.x), __frcp_rn(a.v.y)); }
+
 __host__ __device__ __forceinline__ float vsqrt(float a) { return sqrtf(a); }
 __host__ __device__ __forceinline__ double vsqrt(double a) { return sqrt(a); }
 __device__ __forceinline__ F2 vsqrt(F2 a) { return mk2(sqrtf(a.v.x), sqrtf(a.v.y)); }
@@ -475,7 +486,7 @@ __host__ __device__ __forceinline__ void make_pairs(const V (&f)[Q], PairState<V
 // Smagorinsky tau_eddy from the pair sums (same closed form as les_tau_eddy)
 template <class V>
 __host__ __device__ __forceinline__ V les_tau_eddy_pairs(const PairState<V>& ps, V ux, V uy, V uz,
-                                                         V tau, V les_c) {
+                                                         V inv_rho, V tau, V les_c) {
   const V* s = ps.s;
   V pxx = s[0] + s[3];
   pxx = pxx + s[4];
@@ -506,21 +517,25 @@ __host__ __device__ __forceinline__ V les_tau_eddy_pairs(const PairState<V>& ps,
   qq = fma_(tyy, tyy, qq);
   qq = fma_(tzz, tzz, qq);
   qq = fma_(bc<V>(2), off, qq);
-  return fma_(bc<V>(0.5), vsqrt(fma_(tau, tau, les_c * vsqrt(qq) / ps.rho)),
+  return fma_(bc<V>(0.5), vsqrt(fma_(tau, tau, (les_c * vsqrt(qq)) * inv_rho)),
               bc<V>(-0.5) * tau);
 }
 
 // SRT in pair form: feq_a, feq_abar share w rho (1 - 1.5u^2 + 4.5 (c.u)^2)
-// and differ in the sign of 3 w rho c.u.
-template <class V>
-__host__ __device__ __forceinline__ void collide_srt_pairs(V (&f)[Q], const PairState<V>& ps,
-                                                           V ux, V uy, V uz, V inv_tau) {
+// and differ in the sign of 3 w rho c.u.  emit(q, value) receives every
+// post-collision population.  FROM_PAIRS: rebuild f_a, f_abar from s, d
+// (f is not read after make_pairs, which shortens its register lifetime);
+// otherwise f is updated in place.
+template <bool FROM_PAIRS, class V, class Emit>
+__host__ __device__ __forceinline__ void collide_srt_pairs(const V (&f)[Q], const PairState<V>& ps,
+                                                           V ux, V uy, V uz, V inv_tau,
+                                                           Emit&& emit) {
   V usq = ux * ux;
   usq = fma_(uy, uy, usq);
   usq = fma_(uz, uz, usq);
   const V c0 = fma_(bc<V>(-1.5), usq, bc<V>(1));
   const V rho = ps.rho;
-  f[0] = fma_((rho * bc<V>(1.0 / 3.0)) * c0 - f[0], inv_tau, f[0]);
+  emit(0, fma_((rho * bc<V>(1.0 / 3.0)) * c0 - ps.f0, inv_tau, ps.f0));
   const V wr1 = rho * bc<V>(1.0 / 18.0), wr2 = rho * bc<V>(1.0 / 36.0);
   static_for<0, 9>([&](auto pc) {
     constexpr int p = decltype(pc)::value;
@@ -543,18 +558,27 @@ __host__ __device__ __forceinline__ void collide_srt_pairs(V (&f)[Q], const Pair
     const V wr = wclass(a) == 1 ? wr1 : wr2;
     const V even = wr * fma_(bc<V>(4.5) * eu, eu, c0);
     const V odd = (bc<V>(3) * wr) * eu;
-    const V fa = even + odd, fb = even - odd;
-    f[a] = fma_(fa - f[a], inv_tau, f[a]);
-    f[b] = fma_(fb - f[b], inv_tau, f[b]);
+    if constexpr (FROM_PAIRS) {
+      // s* = s + (2 even - s) inv,  d* = d + (2 odd - d) inv
+      const V ss = fma_(fma_(bc<V>(2), even, -ps.s[p]), inv_tau, ps.s[p]);
+      const V dd = fma_(fma_(bc<V>(2), odd, -ps.d[p]), inv_tau, ps.d[p]);
+      emit(a, bc<V>(0.5) * (ss + dd));
+      emit(b, bc<V>(0.5) * (ss - dd));
+    } else {
+      emit(a, fma_((even + odd) - f[a], inv_tau, f[a]));
+      emit(b, fma_((even - odd) - f[b], inv_tau, f[b]));
+    }
   });
 }
 
 // MRT in pair form (Collision_MRT, lbm_codelets.cpp:449-544), moments
 // formed from s/d, relaxation dm'_k = s_k (m_k - meq_k) / |row_k|^2, back
-// transform f_a -= E_p + O_p, f_abar -= E_p - O_p.
-template <class V, class R>
-__host__ __device__ __forceinline__ void collide_mrt_pairs(V (&f)[Q], const PairState<V>& ps,
-                                                           V s_nu, const MrtParams<R>& p) {
+// transform f_a -= E_p + O_p, f_abar -= E_p - O_p (or, FROM_PAIRS, the same
+// rebuilt from s - 2E and d - 2O).  emit(q, value) receives the results.
+template <bool FROM_PAIRS, class V, class R, class Emit>
+__host__ __device__ __forceinline__ void collide_mrt_pairs(const V (&f)[Q], const PairState<V>& ps,
+                                                           V s_nu, const MrtParams<R>& p,
+                                                           Emit&& emit) {
   const V* s = ps.s;
   const V* d = ps.d;
   const V rho = ps.rho, jx = ps.jx, jy = ps.jy, jz = ps.jz;
@@ -609,7 +633,7 @@ __host__ __device__ __forceinline__ void collide_mrt_pairs(V (&f)[Q], const Pair
   const V e17 = bc<V>(1.98 / 8.0) * m17;
   const V e18 = bc<V>(1.98 / 8.0) * m18;
   // ---- back transform, f -= M^T dm' ----
-  f[0] = f[0] - fma_(bc<V>(-30), e1, bc<V>(12) * e2);
+  emit(0, ps.f0 - fma_(bc<V>(-30), e1, bc<V>(12) * e2));
   const V eax = fma_(bc<V>(-11), e1, bc<V>(-4) * e2);  // rows 1,2 on axis directions
   const V edg = fma_(bc<V>(8), e1, e2);                 // rows 1,2 on diagonals
   const V g910 = e9 + e10;
@@ -640,8 +664,15 @@ __host__ __device__ __forceinline__ void collide_mrt_pairs(V (&f)[Q], const Pair
   static_for<0, 9>([&](auto pc) {
     constexpr int q = decltype(pc)::value;
     constexpr int a = pair_a(q), b = opp(a);
-    f[a] = f[a] - (E[q] + O[q]);
-    f[b] = f[b] - (E[q] - O[q]);
+    if constexpr (FROM_PAIRS) {
+      const V ss = fma_(bc<V>(-2), E[q], s[q]);
+      const V dd = fma_(bc<V>(-2), O[q], d[q]);
+      emit(a, bc<V>(0.5) * (ss + dd));
+      emit(b, bc<V>(0.5) * (ss - dd));
+    } else {
+      emit(a, f[a] - (E[q] + O[q]));
+      emit(b, f[b] - (E[q] - O[q]));
+    }
   });
 }
 

@@ -83,6 +83,12 @@ struct StepArgs {
   const S* __restrict__ src;  // f*_{k-1}
   S* __restrict__ dst;        // f*_k
   long long qs;               // population stride (elements)
+  // hot-path addressing: plane of population q and the in-plane offset
+  // c_x + c_z px + c_y px nz of its donor; node indices inside a plane are
+  // 32-bit (px*nz*ny < 2^31 is checked when the domain is created)
+  const S* srcq[Q];
+  S* dstq[Q];
+  int off[Q];
   Geometry g;
   R tau, les_c, rho0;
   R ulx, uly, ulz;            // lid velocity (cavity)
@@ -146,17 +152,17 @@ __device__ __forceinline__ RealOf<S> boundary_value(const StepArgs<S>& a, int t,
   return fo;  // no rule for this node type: plain bounce-back
 }
 
-// Steps 1-2: the post-stream, post-boundary populations f_k at (x,y,z).
+// Steps 1-2: the post-stream, post-boundary populations f_k at (x,y,z);
+// cell is the node's in-plane index.
 template <class S>
 __device__ __forceinline__ void pull(RealOf<S> (&f)[Q], const StepArgs<S>& a, int x, int y, int z,
-                                     long long cell) {
-  const long long sz = a.g.px, sy = (long long)a.g.px * a.g.nz;
+                                     int cell) {
   const bool edge = (x == 0) | (x == a.g.nx - 1) | (y == 0) | (y == a.g.ny - 1) | (z == 0) |
                     (z == a.g.nz - 1);
   if (!edge) {
     static_for<0, Q>([&](auto qc) {
       constexpr int q = decltype(qc)::value;
-      f[q] = ld(a.src + q * a.qs + cell - (cx(q) + cz(q) * sz + cy(q) * sy), q, a.inv_scale);
+      f[q] = ld(a.srcq[q] + (cell - a.off[q]), q, a.inv_scale);
     });
   } else {
     const int t = node_type(a.g, x, y, z);
@@ -166,9 +172,9 @@ __device__ __forceinline__ void pull(RealOf<S> (&f)[Q], const StepArgs<S>& a, in
       const bool inside = (unsigned)xs < (unsigned)a.g.nx && (unsigned)ys < (unsigned)a.g.ny &&
                           (unsigned)zs < (unsigned)a.g.nz;
       if (inside) {
-        f[q] = ld(a.src + q * a.qs + cell - (cx(q) + cz(q) * sz + cy(q) * sy), q, a.inv_scale);
+        f[q] = ld(a.srcq[q] + (cell - a.off[q]), q, a.inv_scale);
       } else {
-        const RealOf<S> fo = ld(a.src + opp(q) * a.qs + cell, opp(q), a.inv_scale);
+        const RealOf<S> fo = ld(a.srcq[opp(q)] + cell, opp(q), a.inv_scale);
         f[q] = boundary_value<S, q>(a, t, fo, y, z);
       }
     });
@@ -179,27 +185,29 @@ enum { COLL_SRT = 0, COLL_MRT = 1 };
 
 // LES + collision of one node (or one F2 pair of nodes) in pair form.  ps
 // holds the pair sums of f and the density / momentum the equilibrium is
-// built from; u = j / rho.
-template <class S, int COLL, bool LES, class V>
-__device__ __forceinline__ void collide_node(V (&f)[Q], const PairState<V>& ps, V ux, V uy,
-                                             V uz, const StepArgs<S>& a) {
+// built from; u = j / rho.  emit(q, value) receives f*_q.
+template <class S, int COLL, bool LES, bool FROM_PAIRS, class V, class Emit>
+__device__ __forceinline__ void collide_node(const V (&f)[Q], const PairState<V>& ps, V ux, V uy,
+                                             V uz, V inv_rho, const StepArgs<S>& a, Emit&& emit) {
   const V tau = bcast_param<V>(a.tau);
   V te = bc<V>(0);
-  if constexpr (LES) te = les_tau_eddy_pairs<V>(ps, ux, uy, uz, tau, bcast_param<V>(a.les_c));
-  const V inv = bc<V>(1) / (tau + te);
+  if constexpr (LES)
+    te = les_tau_eddy_pairs<V>(ps, ux, uy, uz, inv_rho, tau, bcast_param<V>(a.les_c));
+  const V inv = vrcp(tau + te);
   if constexpr (COLL == COLL_SRT)
-    collide_srt_pairs<V>(f, ps, ux, uy, uz, inv);
+    collide_srt_pairs<FROM_PAIRS, V>(f, ps, ux, uy, uz, inv, emit);
   else
-    collide_mrt_pairs<V>(f, ps, inv, a.mp);
+    collide_mrt_pairs<FROM_PAIRS, V>(f, ps, inv, a.mp, emit);
 }
 
-// rho, u of a node from its pair sums (u = j * (1/rho))
+// u = j * (1/rho); returns 1/rho
 template <class V>
-__device__ __forceinline__ void velocity(const PairState<V>& ps, V& ux, V& uy, V& uz) {
-  const V inv = bc<V>(1) / ps.rho;
+__device__ __forceinline__ V velocity(const PairState<V>& ps, V& ux, V& uy, V& uz) {
+  const V inv = vrcp(ps.rho);
   ux = ps.jx * inv;
   uy = ps.jy * inv;
   uz = ps.jz * inv;
+  return inv;
 }
 
 // Side outputs of the macroscopic state of arF_k.
@@ -239,6 +247,18 @@ __device__ __forceinline__ void store_all(const StepArgs<S>& a, const RealOf<S> 
   });
 }
 
+// emit functor storing f*_q of one node into a lattice
+template <class S>
+struct StoreNode {
+  S* base;
+  long long qs;
+  long long cell;
+  float scale;
+  __device__ __forceinline__ void operator()(int q, RealOf<S> v) const {
+    StoreTraits<S>::store(base + q * qs + cell, v, weight<RealOf<S>>(q), scale);
+  }
+};
+
 // The fused step.  grid = (ceil(nx/blockDim.x), nz, ny), one thread per node.
 template <class S, int COLL, bool LES>
 __global__ void __launch_bounds__(128) k_step(const __grid_constant__ StepArgs<S> a) {
@@ -246,16 +266,17 @@ __global__ void __launch_bounds__(128) k_step(const __grid_constant__ StepArgs<S
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int z = blockIdx.y, y = blockIdx.z;
   if (x >= a.g.nx) return;
-  const long long cell = x + (long long)a.g.px * (z + (long long)a.g.nz * y);
+  const int cell = x + a.g.px * (z + a.g.nz * y);
   R f[Q];
   pull<S>(f, a, x, y, z, cell);
   PairState<R> ps;
   make_pairs<R>(f, ps);
   R ux, uy, uz;
-  velocity<R>(ps, ux, uy, uz);
+  const R inv_rho = velocity<R>(ps, ux, uy, uz);
   write_macro<S>(a, x, y, z, ps.rho, ux, uy, uz);
-  collide_node<S, COLL, LES, R>(f, ps, ux, uy, uz, a);
-  store_all<S>(a, f, cell);
+  collide_node<S, COLL, LES, false, R>(f, ps, ux, uy, uz, inv_rho, a, [&](int q, R v) {
+    StoreTraits<S>::store(a.dstq[q] + cell, v, weight<R>(q), a.scale);
+  });
 }
 
 // ------------------------------------------------------------------ //
@@ -332,11 +353,8 @@ __global__ void __launch_bounds__(128)
   ps.jx = rd * ux;
   ps.jy = rd * uy;
   ps.jz = rd * uz;
-  collide_node<S, COLL, LES, R>(f, ps, ux, uy, uz, a);
-  static_for<0, Q>([&](auto qc) {
-    constexpr int q = decltype(qc)::value;
-    StoreTraits<S>::store(collided + q * a.qs + cell, f[q], weight<R>(q), a.scale);
-  });
+  collide_node<S, COLL, LES, false, R>(f, ps, ux, uy, uz, vrcp(rd), a,
+                                       StoreNode<S>{collided, a.qs, cell, a.scale});
 }
 
 // ------------------------------------------------------------------ //
@@ -374,12 +392,9 @@ __global__ void __launch_bounds__(128)
   write_macro<S>(a, x, y, z, rho, ux, uy, uz);
   PairState<R> ps;
   make_pairs<R>(f, ps);
-  velocity<R>(ps, ux, uy, uz);
-  collide_node<S, COLL, LES, R>(f, ps, ux, uy, uz, a);
-  static_for<0, Q>([&](auto qc) {
-    constexpr int q = decltype(qc)::value;
-    StoreTraits<S>::store(collided + q * a.qs + cell, f[q], weight<R>(q), a.scale);
-  });
+  const R inv_rho = velocity<R>(ps, ux, uy, uz);
+  collide_node<S, COLL, LES, false, R>(f, ps, ux, uy, uz, inv_rho, a,
+                                       StoreNode<S>{collided, a.qs, cell, a.scale});
 }
 
 // ------------------------------------------------------------------ //
@@ -404,7 +419,7 @@ __global__ void __launch_bounds__(128)
       f[q] = ld(a.src + q * a.qs + cell, q, a.inv_scale);
     });
   } else {
-    pull<S>(f, a, x, y, z, cell);
+    pull<S>(f, a, x, y, z, (int)cell);
   }
   long long node;
   if (padded)
@@ -464,26 +479,31 @@ __device__ __forceinline__ void st_pair<__nv_bfloat16>(__nv_bfloat16* p, F2 v, i
   *reinterpret_cast<__nv_bfloat162*>(p) = __float22bfloat162_rn(d);
 }
 
+// minimum resident blocks per SM requested for the packed kernel (caps its
+// registers per thread; 0 = no cap)
+#ifndef LBM_PACKED_MIN_BLOCKS
+#define LBM_PACKED_MIN_BLOCKS 0
+#endif
+
 template <class S, int COLL, bool LES>
-__global__ void __launch_bounds__(64) k_step2(const __grid_constant__ StepArgs<S> a) {
+__global__ void __launch_bounds__(64, LBM_PACKED_MIN_BLOCKS) k_step2(const __grid_constant__ StepArgs<S> a) {
   static_assert(std::is_same<RealOf<S>, float>::value, "packed kernel is FP32 arithmetic");
   const int x0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
   const int z = blockIdx.y, y = blockIdx.z;
   if (x0 >= a.g.nx) return;
-  const long long cell = x0 + (long long)a.g.px * (z + (long long)a.g.nz * y);
+  const int cell = x0 + a.g.px * (z + a.g.nz * y);
   const bool two = x0 + 1 < a.g.nx;
   const bool interior = x0 >= 1 && x0 + 1 <= a.g.nx - 2 && y >= 1 && y <= a.g.ny - 2 && z >= 1 &&
                         z <= a.g.nz - 2;
   F2 f[Q];
   if (interior) {
-    const long long sz = a.g.px, sy = (long long)a.g.px * a.g.nz;
     static_for<0, Q>([&](auto qc) {
       constexpr int q = decltype(qc)::value;
-      const S* p = a.src + q * a.qs + cell - (cz(q) * sz + cy(q) * sy);
+      const S* p = a.srcq[q] + (cell - a.off[q]);
       if constexpr (cx(q) == 0) {
         f[q] = ld_pair<S>(p, q, a.inv_scale);
       } else {
-        f[q] = mk2(ld(p - cx(q), q, a.inv_scale), ld(p + 1 - cx(q), q, a.inv_scale));
+        f[q] = mk2(ld(p, q, a.inv_scale), ld(p + 1, q, a.inv_scale));
       }
     });
   } else {
@@ -502,23 +522,17 @@ __global__ void __launch_bounds__(64) k_step2(const __grid_constant__ StepArgs<S
   PairState<F2> ps;
   make_pairs<F2>(f, ps);
   F2 ux, uy, uz;
-  velocity<F2>(ps, ux, uy, uz);
+  const F2 inv_rho = velocity<F2>(ps, ux, uy, uz);
   if (a.den_out || a.ux_out || a.g.casetype == CHANNEL) {
     write_macro<S>(a, x0, y, z, ps.rho.v.x, ux.v.x, uy.v.x, uz.v.x);
     if (two) write_macro<S>(a, x0 + 1, y, z, ps.rho.v.y, ux.v.y, uy.v.y, uz.v.y);
   }
-  collide_node<S, COLL, LES, F2>(f, ps, ux, uy, uz, a);
-  if (two) {
-    static_for<0, Q>([&](auto qc) {
-      constexpr int q = decltype(qc)::value;
-      st_pair<S>(a.dst + q * a.qs + cell, f[q], q, a.scale);
-    });
-  } else {
-    static_for<0, Q>([&](auto qc) {
-      constexpr int q = decltype(qc)::value;
-      StoreTraits<S>::store(a.dst + q * a.qs + cell, f[q].v.x, weight<float>(q), a.scale);
-    });
-  }
+  collide_node<S, COLL, LES, true, F2>(f, ps, ux, uy, uz, inv_rho, a, [&](int q, F2 v) {
+    if (two)
+      st_pair<S>(a.dstq[q] + cell, v, q, a.scale);
+    else
+      StoreTraits<S>::store(a.dstq[q] + cell, v.v.x, weight<float>(q), a.scale);
+  });
 }
 
 // node type and inside mask per node, [ny][nz][nx]
