@@ -307,6 +307,74 @@ int lbm_estimate_bytes(const Inputval* pinput, const lbm_options* opt,
  * stream around the kernel launches (synchronises). */
 int lbm_last_run_ms(lbm_domain* d, float* ms);
 
+/* ------------------------------------------------------------------ */
+/* Batches: many independent domains of uneven size resident on one    */
+/* GPU, stepped together by one persistent kernel per time step over a  */
+/* tile work-list (every tile a run of nodes of one domain).  Steps are */
+/* issued in chunks captured as CUDA graphs; each domain advances to    */
+/* its own step target, so domains can join and leave between chunks   */
+/* (continuous batching).  No reference counterpart: the reference runs */
+/* one domain per program (main.cpp:287-291).                           */
+/* ------------------------------------------------------------------ */
+typedef struct lbm_batch lbm_batch;
+
+typedef struct lbm_batch_options {
+  int device;             /* CUDA device ordinal                              */
+  size_t hbm_budget;      /* bytes of the device pool holding every domain    */
+  int chunk_steps;        /* steps per captured graph chunk (even), 0 = 32    */
+  int block;              /* threads per CTA (128 or 256), 0 = autotuned/256  */
+  int nodes_per_thread;   /* nodes per thread per tile (1, 2, 4), 0 = 2       */
+  int ctas_per_sm;        /* persistent CTAs per SM, 0 = max resident         */
+  int reserved[8];
+} lbm_batch_options;
+
+void lbm_batch_default_options(lbm_batch_options* bo);
+
+/* Create a batch: reserves bo->hbm_budget bytes of device memory. */
+int lbm_batch_create(const lbm_batch_options* bo, lbm_batch** out);
+int lbm_batch_destroy(lbm_batch* b);
+
+/* Admit a domain with a step target.  Its memory comes from the pool;
+ * LBM_ERR_BUDGET when it does not fit.  The initial state is built on the
+ * batch stream.  Storage LBM_STORE_F64 is not supported in batches. */
+int lbm_batch_add(lbm_batch* b, const Inputval* pinput, const lbm_options* opt,
+                  long long target_steps, int* id);
+
+/* Issue `steps` more steps to every admitted domain that has not reached
+ * its target (each stops at its own target).  Asynchronous. */
+int lbm_batch_step(lbm_batch* b, int steps);
+
+/* Ids (up to max) of domains that reached their target and whose last
+ * chunk has completed on the GPU; non-blocking.  *n = count written. */
+int lbm_batch_poll(lbm_batch* b, int* ids, int max, int* n);
+
+/* The domain handle of a batch member: lbm_export_arF, lbm_get_macroscopic,
+ * lbm_diagnostics and lbm_steps_done work on it (they synchronise the batch
+ * stream).  Owned by the batch. */
+int lbm_batch_domain(lbm_batch* b, int id, lbm_domain** d);
+
+/* Release a member's memory back to the pool (waits for its last chunk). */
+int lbm_batch_remove(lbm_batch* b, int id);
+
+int lbm_batch_sync(lbm_batch* b);
+
+/* Bytes of the pool in use, free (largest block), and domains resident. */
+int lbm_batch_usage(lbm_batch* b, size_t* used, size_t* largest_free, int* ndomains);
+
+/* Bytes a domain of this case takes from a batch pool. */
+int lbm_batch_domain_bytes(const Inputval* pinput, const lbm_options* opt, size_t* bytes);
+
+/* Project autotuner: run `trial_steps` real steps of the current batch with
+ * each candidate (block, nodes per thread, CTAs per SM) and keep the
+ * fastest; writes the choice into *chosen (may be NULL).  The trial steps
+ * advance the domains like any other steps. */
+int lbm_batch_autotune(lbm_batch* b, int trial_steps, lbm_batch_options* chosen);
+
+/* Average milliseconds per step of the last lbm_batch_step call, measured
+ * with CUDA events on the batch stream (synchronises); *lups = lattice
+ * updates issued by that call. */
+int lbm_batch_last_step_ms(lbm_batch* b, float* ms, long long* lups);
+
 #ifdef __cplusplus
 }
 #endif

@@ -66,6 +66,14 @@ class Options(C.Structure):
     ]
 
 
+class BatchOptions(C.Structure):
+    _fields_ = [
+        ("device", C.c_int), ("hbm_budget", C.c_size_t), ("chunk_steps", C.c_int),
+        ("block", C.c_int), ("nodes_per_thread", C.c_int), ("ctas_per_sm", C.c_int),
+        ("reserved", C.c_int * 8),
+    ]
+
+
 def make_inputval(nx, ny=None, nz=None, *, casetype=CAVITY, tau=None, re=None, u=0.1,
                   mrt=False, les=False, cs=0.0, rho0=1.0, h=None):
     """Fill an Inputval the way main.cpp:59-85 does.
@@ -136,6 +144,22 @@ def lib():
         L.lbm_estimate_bytes.argtypes = [C.POINTER(Inputval), C.POINTER(Options),
                                          C.POINTER(C.c_size_t)]
         L.lbm_last_run_ms.argtypes = [vp, C.POINTER(C.c_float)]
+        L.lbm_batch_default_options.argtypes = [C.POINTER(BatchOptions)]
+        L.lbm_batch_create.argtypes = [C.POINTER(BatchOptions), C.POINTER(vp)]
+        L.lbm_batch_destroy.argtypes = [vp]
+        L.lbm_batch_add.argtypes = [vp, C.POINTER(Inputval), C.POINTER(Options), C.c_longlong,
+                                    C.POINTER(C.c_int)]
+        L.lbm_batch_step.argtypes = [vp, i32]
+        L.lbm_batch_poll.argtypes = [vp, vp, i32, C.POINTER(C.c_int)]
+        L.lbm_batch_domain.argtypes = [vp, i32, C.POINTER(vp)]
+        L.lbm_batch_remove.argtypes = [vp, i32]
+        L.lbm_batch_sync.argtypes = [vp]
+        L.lbm_batch_usage.argtypes = [vp, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t),
+                                      C.POINTER(C.c_int)]
+        L.lbm_batch_domain_bytes.argtypes = [C.POINTER(Inputval), C.POINTER(Options),
+                                             C.POINTER(C.c_size_t)]
+        L.lbm_batch_autotune.argtypes = [vp, i32, C.POINTER(BatchOptions)]
+        L.lbm_batch_last_step_ms.argtypes = [vp, C.POINTER(C.c_float), C.POINTER(C.c_longlong)]
         _lib = L
     return _lib
 
@@ -272,3 +296,99 @@ def d3q19_tables():
     m = np.zeros((19, 19), np.float32)
     lib().lbm_d3q19_tables(_ptr(d), _ptr(o), _ptr(w), _ptr(m))
     return d, o, w, m
+
+
+class _Member(Domain):
+    """View of a batch member through the single-domain calls (owned by the batch)."""
+
+    def __init__(self, handle, inputval):
+        self.iv = inputval
+        self.h = handle
+        self.shape = (inputval.ny, inputval.nz, inputval.nx)
+
+    def close(self):
+        self.h = None
+
+    def run(self, nsteps):
+        raise RuntimeError("batch members are stepped by Batch.step")
+
+
+class Batch:
+    """Many resident domains stepped together (continuous batching)."""
+
+    def __init__(self, hbm_budget=1 << 30, device=0, chunk_steps=32, block=0,
+                 nodes_per_thread=0, ctas_per_sm=0):
+        o = BatchOptions()
+        lib().lbm_batch_default_options(C.byref(o))
+        o.device, o.hbm_budget, o.chunk_steps = device, hbm_budget, chunk_steps
+        if block:
+            o.block = block
+        if nodes_per_thread:
+            o.nodes_per_thread = nodes_per_thread
+        o.ctas_per_sm = ctas_per_sm
+        h = C.c_void_p()
+        check(lib().lbm_batch_create(C.byref(o), C.byref(h)))
+        self.h = h
+        self.ivs = {}
+
+    def close(self):
+        if self.h:
+            check(lib().lbm_batch_destroy(self.h))
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add(self, inputval, options=None, steps=0):
+        opt = options if options is not None else default_options()
+        i = C.c_int()
+        check(lib().lbm_batch_add(self.h, C.byref(inputval), C.byref(opt), int(steps),
+                                  C.byref(i)))
+        self.ivs[i.value] = inputval
+        return i.value
+
+    def step(self, steps):
+        check(lib().lbm_batch_step(self.h, int(steps)))
+
+    def poll(self, max_ids=4096):
+        ids = np.zeros(max_ids, np.int32)
+        n = C.c_int()
+        check(lib().lbm_batch_poll(self.h, _ptr(ids), max_ids, C.byref(n)))
+        return [int(v) for v in ids[:n.value]]
+
+    def member(self, i):
+        h = C.c_void_p()
+        check(lib().lbm_batch_domain(self.h, int(i), C.byref(h)))
+        return _Member(h, self.ivs[i])
+
+    def remove(self, i):
+        check(lib().lbm_batch_remove(self.h, int(i)))
+        self.ivs.pop(i, None)
+
+    def sync(self):
+        check(lib().lbm_batch_sync(self.h))
+
+    def usage(self):
+        u, f, n = C.c_size_t(), C.c_size_t(), C.c_int()
+        check(lib().lbm_batch_usage(self.h, C.byref(u), C.byref(f), C.byref(n)))
+        return u.value, f.value, n.value
+
+    def autotune(self, trial_steps=32):
+        o = BatchOptions()
+        check(lib().lbm_batch_autotune(self.h, int(trial_steps), C.byref(o)))
+        return dict(block=o.block, nodes_per_thread=o.nodes_per_thread, ctas_per_sm=o.ctas_per_sm)
+
+    def last_step_ms(self):
+        ms, lups = C.c_float(), C.c_longlong()
+        check(lib().lbm_batch_last_step_ms(self.h, C.byref(ms), C.byref(lups)))
+        return ms.value, lups.value
+
+
+def batch_domain_bytes(inputval, options=None):
+    opt = options if options is not None else default_options()
+    b = C.c_size_t()
+    check(lib().lbm_batch_domain_bytes(C.byref(inputval), C.byref(opt), C.byref(b)))
+    return b.value

@@ -1,0 +1,707 @@
+// lbm_batch.cu — many independent domains of uneven size resident on one
+// GPU and stepped together: one persistent kernel per time step over a tile
+// work-list, step chunks captured as CUDA graphs, a device memory pool for
+// admission by HBM budget, per-domain step targets (continuous batching) and
+// an autotuner over the launch shape.
+//
+// Work-list.  Every active domain contributes ceil(nodes / tile) tiles, a
+// tile being block*npt consecutive nodes in the domain's [y][z][x] order.
+// tile_off[] is the prefix sum over the active domains; a CTA walks the
+// global tile index t = blockIdx.x, += gridDim.x, finds its domain by binary
+// search and copies that domain's kernel arguments into shared memory.
+// Each node then runs step_node<S, COLL, LES>() — the very function of the
+// single-domain kernel — so a domain produces the same bits alone and in a
+// batch, whatever else is resident (no cross-domain data, no atomics).
+//
+// Graphs.  All kernel inputs live in device tables, so the graph of a chunk
+// (chunk_steps launches, launch j reading the tables) stays valid while the
+// membership changes; only the tables are re-uploaded before each chunk.
+#include <algorithm>
+#include <map>
+#include <vector>
+
+#include "lbm_domain.cuh"
+
+using namespace lbm;
+
+namespace {
+
+constexpr int kArgsBytes = 768;  // one StepArgs<S> image, 16-byte multiple
+static_assert(sizeof(StepArgs<float>) <= kArgsBytes, "StepArgs too large");
+static_assert(sizeof(StepArgs<__half>) <= kArgsBytes, "StepArgs too large");
+static_assert(sizeof(StepArgs<__nv_bfloat16>) <= kArgsBytes, "StepArgs too large");
+// argument images per domain: lattice parity (2) x output kind (3: none,
+// rho, rho + u)
+constexpr int kImages = 6;
+
+// per active domain, per chunk
+struct SlotMeta {
+  int variant;       // storage*4 + model (model: 0 SRT, 1 SRT+LES, 2 MRT, 3 MRT+LES)
+  int image_base;    // index of the domain's first argument image
+  int nx, nz;
+  unsigned long long mnx, mnz;  // ceil(2^64 / n): exact 32-bit division
+  long long nodes;
+  int active;        // steps the domain takes in this chunk
+  int cur0;          // lattice holding f* at chunk start
+};
+
+struct BatchTables {
+  int nslots;
+  int tile;          // nodes per tile = block * npt
+  long long ntiles;
+  const SlotMeta* meta;
+  const long long* tile_off;     // [nslots + 1]
+  const unsigned char* images;   // [capacity * kImages][kArgsBytes]
+};
+
+__device__ __forceinline__ unsigned fastdiv(unsigned n, unsigned long long m) {
+  return (unsigned)__umul64hi(m, (unsigned long long)n);
+}
+
+template <class S, int COLL, bool LES>
+__device__ __forceinline__ void batch_node(const unsigned char* img, int x, int y, int z) {
+  step_node<S, COLL, LES>(*reinterpret_cast<const StepArgs<S>*>(img), x, y, z);
+}
+
+template <class S>
+__device__ __forceinline__ void batch_model(int model, const unsigned char* img, int x, int y,
+                                            int z) {
+  switch (model) {
+    case 0: batch_node<S, COLL_SRT, false>(img, x, y, z); break;
+    case 1: batch_node<S, COLL_SRT, true>(img, x, y, z); break;
+    case 2: batch_node<S, COLL_MRT, false>(img, x, y, z); break;
+    default: batch_node<S, COLL_MRT, true>(img, x, y, z); break;
+  }
+}
+
+// One time step of every active domain (launch j of a chunk).
+__global__ void __launch_bounds__(256) k_batch_step(const BatchTables* __restrict__ tab, int j,
+                                                    int npt) {
+  __shared__ __align__(16) unsigned char img[kArgsBytes];
+  const BatchTables T = *tab;
+  int cached = -1;
+  for (long long t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
+    int lo = 0, hi = T.nslots;  // tile_off[lo] <= t < tile_off[hi]
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (T.tile_off[mid] <= t)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    const SlotMeta m = T.meta[lo];
+    if (j >= m.active) continue;  // uniform over the CTA
+    const int par = (m.cur0 + j) & 1;
+    const int kind = j >= m.active - 1 ? 2 : (j >= m.active - 2 ? 1 : 0);
+    const int image = m.image_base + par * 3 + kind;
+    if (image != cached) {
+      __syncthreads();
+      const int4* src = reinterpret_cast<const int4*>(T.images + (size_t)image * kArgsBytes);
+      int4* dst = reinterpret_cast<int4*>(img);
+      for (int i = threadIdx.x; i < kArgsBytes / 16; i += blockDim.x) dst[i] = src[i];
+      __syncthreads();
+      cached = image;
+    }
+    const long long base = (t - T.tile_off[lo]) * (long long)T.tile;
+    for (int i = 0; i < npt; ++i) {
+      const long long n = base + (long long)i * blockDim.x + threadIdx.x;
+      if (n >= m.nodes) break;
+      const unsigned r = fastdiv((unsigned)n, m.mnx);
+      const int x = (int)((unsigned)n - r * (unsigned)m.nx);
+      const unsigned y = fastdiv(r, m.mnz);
+      const int z = (int)(r - y * (unsigned)m.nz);
+      switch (m.variant >> 2) {
+        case 0: batch_model<float>(m.variant & 3, img, x, (int)y, z); break;
+        case 1: batch_model<__half>(m.variant & 3, img, x, (int)y, z); break;
+        default: batch_model<__nv_bfloat16>(m.variant & 3, img, x, (int)y, z); break;
+      }
+    }
+  }
+}
+
+// First-fit device pool with coalescing (offsets 256-byte aligned).
+struct Pool {
+  char* base = nullptr;
+  size_t size = 0;
+  std::map<size_t, size_t> free_;  // offset -> size
+  std::map<size_t, size_t> used_;  // offset -> size
+  void reset(char* b, size_t n) {
+    base = b;
+    size = n;
+    free_.clear();
+    used_.clear();
+    if (n) free_[0] = n;
+  }
+  void* alloc(size_t n) {
+    n = (n + 255) / 256 * 256;
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second >= n) {
+        const size_t off = it->first, rest = it->second - n;
+        free_.erase(it);
+        if (rest) free_[off + n] = rest;
+        used_[off] = n;
+        return base + off;
+      }
+    }
+    return nullptr;
+  }
+  void release(void* p) {
+    if (!p) return;
+    const size_t off = (size_t)((char*)p - base);
+    auto u = used_.find(off);
+    if (u == used_.end()) return;
+    size_t n = u->second;
+    used_.erase(u);
+    size_t start = off;
+    auto nx = free_.lower_bound(off);
+    if (nx != free_.begin()) {
+      auto pv = std::prev(nx);
+      if (pv->first + pv->second == off) {
+        start = pv->first;
+        n += pv->second;
+        free_.erase(pv);
+      }
+    }
+    nx = free_.lower_bound(off);
+    if (nx != free_.end() && start + n == nx->first) {
+      n += nx->second;
+      free_.erase(nx);
+    }
+    free_[start] = n;
+  }
+  size_t used() const {
+    size_t s = 0;
+    for (auto& kv : used_) s += kv.second;
+    return s;
+  }
+  size_t largest_free() const {
+    size_t s = 0;
+    for (auto& kv : free_) s = std::max(s, kv.second);
+    return s;
+  }
+};
+
+int model_of(const Inputval& in) { return (in.bEnableMRT ? 2 : 0) + (in.bEnableLES ? 1 : 0); }
+
+int storage_index(int storage) {
+  return storage == LBM_STORE_F16_SHIFT ? 1 : (storage == LBM_STORE_BF16_SHIFT ? 2 : 0);
+}
+
+}  // namespace
+
+struct lbm_batch {
+  lbm_batch_options opt;
+  int sm_count = 0;
+  cudaStream_t stream = nullptr;
+  cudaStream_t capture = nullptr;
+  char* pool_mem = nullptr;
+  Pool pool;
+  struct Member {
+    lbm_domain* d = nullptr;
+    long long target = 0;
+    int image_slot = 0;       // index in the image table
+    long long issued = 0;     // steps issued so far
+    long long done_chunk = -1;  // chunk whose completion makes the result final
+  };
+  std::map<int, Member> members;
+  int next_id = 1;
+  int capacity = 0;               // image slots
+  std::vector<int> free_images;
+  // device tables and their pinned host images
+  BatchTables* d_tab = nullptr;
+  SlotMeta* d_meta = nullptr;
+  long long* d_off = nullptr;
+  unsigned char* d_images = nullptr;
+  BatchTables* h_tab = nullptr;
+  SlotMeta* h_meta = nullptr;
+  long long* h_off = nullptr;
+  cudaEvent_t tables_free = nullptr;  // previous table upload has been consumed
+  // chunk graph
+  cudaGraphExec_t graph = nullptr;
+  int graph_block = 0, graph_grid = 0, graph_npt = 0, graph_steps = 0;
+  // completion tracking
+  long long chunks_issued = 0;
+  std::vector<std::pair<long long, cudaEvent_t>> chunk_events;
+  long long chunks_completed = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  long long last_lups = 0;
+  int last_steps = 0;
+};
+
+namespace {
+
+int chunk_steps(const lbm_batch* b) { return b->opt.chunk_steps > 0 ? b->opt.chunk_steps : 32; }
+
+int launch_shape(lbm_batch* b, int* block, int* grid, int* npt) {
+  *block = b->opt.block == 128 ? 128 : 256;
+  *npt = b->opt.nodes_per_thread > 0 ? b->opt.nodes_per_thread : 2;
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_step, *block, 0));
+  if (per_sm < 1) per_sm = 1;
+  if (b->opt.ctas_per_sm > 0 && b->opt.ctas_per_sm < per_sm) per_sm = b->opt.ctas_per_sm;
+  *grid = per_sm * b->sm_count;
+  return LBM_OK;
+}
+
+// (Re)capture the chunk graph for the current launch shape.
+int ensure_graph(lbm_batch* b) {
+  int block, grid, npt;
+  int rc = launch_shape(b, &block, &grid, &npt);
+  if (rc) return rc;
+  const int steps = chunk_steps(b);
+  if (b->graph && b->graph_block == block && b->graph_grid == grid && b->graph_npt == npt &&
+      b->graph_steps == steps)
+    return LBM_OK;
+  if (b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  CK(cudaStreamBeginCapture(b->capture, cudaStreamCaptureModeThreadLocal));
+  for (int j = 0; j < steps; ++j) k_batch_step<<<grid, block, 0, b->capture>>>(b->d_tab, j, npt);
+  cudaGraph_t g;
+  CK(cudaStreamEndCapture(b->capture, &g));
+  cudaError_t e = cudaGraphInstantiate(&b->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess)
+    return set_error(LBM_ERR_CUDA, "batch graph instantiation failed: %s", cudaGetErrorString(e));
+  b->graph_block = block;
+  b->graph_grid = grid;
+  b->graph_npt = npt;
+  b->graph_steps = steps;
+  return LBM_OK;
+}
+
+// Argument images of a member: parity x {no output, rho, rho + u}.
+int upload_images(lbm_batch* b, lbm_batch::Member& m) {
+  lbm_domain* d = m.d;
+  std::vector<unsigned char> buf((size_t)kImages * kArgsBytes, 0);
+  int rc = with_storage(d->opt.storage, [&](auto tag) -> int {
+    using S = typename decltype(tag)::type;
+    if constexpr (std::is_same<S, double>::value) {
+      return set_error(LBM_ERR_INVALID, "FP64 storage is not supported in batches");
+    } else {
+      for (int par = 0; par < 2; ++par)
+        for (int kind = 0; kind < 3; ++kind) {
+          // a step starting from lattice `par` has step number of parity par^1
+          StepArgs<S> a = make_args<S>(d, d->lat[par], d->lat[par ^ 1], par ^ 1);
+          if (kind >= 1) a.den_out = d->den[par ^ 1];
+          if (kind == 2) {
+            a.ux_out = d->ux;
+            a.uy_out = d->uy;
+            a.uz_out = d->uz;
+          }
+          std::memcpy(&buf[(size_t)(par * 3 + kind) * kArgsBytes], &a, sizeof(a));
+        }
+      return LBM_OK;
+    }
+  });
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(b->d_images + (size_t)m.image_slot * kImages * kArgsBytes, buf.data(),
+                     buf.size(), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaStreamSynchronize(b->stream));  // buf is a local
+  return LBM_OK;
+}
+
+int grow_images(lbm_batch* b) {
+  const int cap = b->capacity ? b->capacity * 2 : 64;
+  unsigned char* nimg = nullptr;
+  SlotMeta *dm = nullptr, *hm = nullptr;
+  long long *doff = nullptr, *hoff = nullptr;
+  CK(cudaMalloc(&nimg, (size_t)cap * kImages * kArgsBytes));
+  CK(cudaMalloc(&dm, (size_t)cap * sizeof(SlotMeta)));
+  CK(cudaMalloc(&doff, (size_t)(cap + 1) * sizeof(long long)));
+  CK(cudaMallocHost(&hm, (size_t)cap * sizeof(SlotMeta)));
+  CK(cudaMallocHost(&hoff, (size_t)(cap + 1) * sizeof(long long)));
+  CK(cudaStreamSynchronize(b->stream));
+  if (b->d_images) {
+    CK(cudaMemcpy(nimg, b->d_images, (size_t)b->capacity * kImages * kArgsBytes,
+                  cudaMemcpyDeviceToDevice));
+    cudaFree(b->d_images);
+    cudaFree(b->d_meta);
+    cudaFree(b->d_off);
+    cudaFreeHost(b->h_meta);
+    cudaFreeHost(b->h_off);
+  }
+  for (int i = cap - 1; i >= b->capacity; --i) b->free_images.push_back(i);
+  b->d_images = nimg;
+  b->d_meta = dm;
+  b->d_off = doff;
+  b->h_meta = hm;
+  b->h_off = hoff;
+  b->capacity = cap;
+  return LBM_OK;
+}
+
+void retire_completed(lbm_batch* b) {
+  while (!b->chunk_events.empty()) {
+    auto& ce = b->chunk_events.front();
+    if (cudaEventQuery(ce.second) != cudaSuccess) break;
+    b->chunks_completed = ce.first;
+    cudaEventDestroy(ce.second);
+    b->chunk_events.erase(b->chunk_events.begin());
+  }
+}
+
+// Build and upload the tables of one chunk; returns the lattice updates.
+int issue_chunk(lbm_batch* b, int steps_offered, long long* lups) {
+  const int S = chunk_steps(b);
+  int n = 0;
+  long long tiles = 0, updates = 0;
+  const int tile = b->graph_block * b->graph_npt;
+  CK(cudaEventSynchronize(b->tables_free));  // the pinned tables may be rewritten
+  for (auto& kv : b->members) {
+    lbm_batch::Member& m = kv.second;
+    const long long left = m.target - m.issued;
+    if (left <= 0) continue;
+    const int active = (int)std::min<long long>(std::min(S, steps_offered), left);
+    lbm_domain* d = m.d;
+    SlotMeta& sm = b->h_meta[n];
+    sm.variant = storage_index(d->opt.storage) * 4 + model_of(d->in);
+    sm.image_base = m.image_slot * kImages;
+    sm.nx = d->g.nx;
+    sm.nz = d->g.nz;
+    sm.mnx = ~0ull / (unsigned long long)d->g.nx + 1;
+    sm.mnz = ~0ull / (unsigned long long)d->g.nz + 1;
+    sm.nodes = d->N;
+    sm.active = active;
+    sm.cur0 = d->cur;
+    b->h_off[n] = tiles;
+    tiles += (d->N + tile - 1) / tile;
+    updates += d->N * active;
+    // host bookkeeping of the steps this chunk takes
+    d->step += active;
+    d->cur ^= (active & 1);
+    d->post_direct = false;
+    m.issued += active;
+    if (m.issued >= m.target) m.done_chunk = b->chunks_issued + 1;
+    ++n;
+  }
+  b->h_off[n] = tiles;
+  if (n == 0) {
+    *lups = 0;
+    return LBM_OK;
+  }
+  b->h_tab->nslots = n;
+  b->h_tab->tile = tile;
+  b->h_tab->ntiles = tiles;
+  b->h_tab->meta = b->d_meta;
+  b->h_tab->tile_off = b->d_off;
+  b->h_tab->images = b->d_images;
+  CK(cudaMemcpyAsync(b->d_meta, b->h_meta, (size_t)n * sizeof(SlotMeta), cudaMemcpyHostToDevice,
+                     b->stream));
+  CK(cudaMemcpyAsync(b->d_off, b->h_off, (size_t)(n + 1) * sizeof(long long),
+                     cudaMemcpyHostToDevice, b->stream));
+  CK(cudaMemcpyAsync(b->d_tab, b->h_tab, sizeof(BatchTables), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaEventRecord(b->tables_free, b->stream));
+  CK(cudaGraphLaunch(b->graph, b->stream));
+  ++b->chunks_issued;
+  cudaEvent_t ev;
+  CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  CK(cudaEventRecord(ev, b->stream));
+  b->chunk_events.push_back({b->chunks_issued, ev});
+  *lups = updates;
+  return LBM_OK;
+}
+
+void destroy_member(lbm_batch* b, lbm_batch::Member& m) {
+  lbm_domain* d = m.d;
+  if (!d) return;
+  void* bufs[] = {d->lat[0], d->lat[1], d->den[0], d->den[1], d->ux,     d->uy,
+                  d->uz,     d->inlet_u, d->prho[0], d->prho[1], d->pu[0], d->pu[1]};
+  for (void* p : bufs) b->pool.release(p);
+  d->stream = nullptr;  // the batch stream is not the domain's to destroy
+  free_all(d);
+  delete d;
+  m.d = nullptr;
+  b->free_images.push_back(m.image_slot);
+}
+
+}  // namespace
+
+extern "C" {
+
+void lbm_batch_default_options(lbm_batch_options* bo) {
+  if (!bo) return;
+  std::memset(bo, 0, sizeof(*bo));
+  bo->hbm_budget = (size_t)8 << 30;
+  bo->chunk_steps = 32;
+  bo->block = 256;
+  bo->nodes_per_thread = 2;
+}
+
+int lbm_batch_domain_bytes(const Inputval* pinput, const lbm_options* opt, size_t* bytes) {
+  int rc = validate(pinput, opt);
+  if (rc) return rc;
+  if (!bytes) return set_error(LBM_ERR_INVALID, "NULL bytes");
+  *bytes = domain_state_bytes(pinput, opt);
+  return LBM_OK;
+}
+
+int lbm_batch_create(const lbm_batch_options* bo, lbm_batch** out) {
+  if (!out) return set_error(LBM_ERR_INVALID, "NULL out");
+  *out = nullptr;
+  lbm_batch_options o;
+  if (bo)
+    o = *bo;
+  else
+    lbm_batch_default_options(&o);
+  if (o.chunk_steps < 0 || (o.chunk_steps & 1))
+    return set_error(LBM_ERR_INVALID, "chunk_steps must be even");
+  if (o.block != 0 && o.block != 128 && o.block != 256)
+    return set_error(LBM_ERR_INVALID, "block must be 128 or 256");
+  if (o.nodes_per_thread < 0 || o.nodes_per_thread > 8)
+    return set_error(LBM_ERR_INVALID, "nodes_per_thread must be 1..8");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return set_error(LBM_ERR_NO_DEVICE, "no CUDA device available");
+  if (o.device < 0 || o.device >= ndev) return set_error(LBM_ERR_INVALID, "bad device");
+  CK(cudaSetDevice(o.device));
+  lbm_batch* b = new lbm_batch();
+  b->opt = o;
+  auto fail = [&](int rc) {
+    lbm_batch_destroy(b);
+    return rc;
+  };
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, o.device) != cudaSuccess || prop.major < 10)
+    return fail(set_error(LBM_ERR_NO_DEVICE, "device %d is not an sm_100 GPU", o.device));
+  b->sm_count = prop.multiProcessorCount;
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&b->capture, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->tables_free, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess)
+    return fail(set_error(LBM_ERR_CUDA, "stream/event creation failed"));
+  CK(cudaEventRecord(b->tables_free, b->stream));
+  if (o.hbm_budget) {
+    cudaError_t e = cudaMalloc(&b->pool_mem, o.hbm_budget);
+    if (e != cudaSuccess)
+      return fail(set_error(LBM_ERR_OOM, "pool of %zu bytes: %s", o.hbm_budget,
+                            cudaGetErrorString(e)));
+  }
+  b->pool.reset(b->pool_mem, o.hbm_budget);
+  int rc;
+  if (cudaMalloc(&b->d_tab, sizeof(BatchTables)) != cudaSuccess ||
+      cudaMallocHost(&b->h_tab, sizeof(BatchTables)) != cudaSuccess)
+    return fail(set_error(LBM_ERR_OOM, "batch tables"));
+  std::memset(b->h_tab, 0, sizeof(BatchTables));
+  if ((rc = grow_images(b))) return fail(rc);
+  if ((rc = ensure_graph(b))) return fail(rc);
+  *out = b;
+  return LBM_OK;
+}
+
+int lbm_batch_destroy(lbm_batch* b) {
+  if (!b) return set_error(LBM_ERR_INVALID, "NULL batch");
+  cudaSetDevice(b->opt.device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  for (auto& kv : b->members) destroy_member(b, kv.second);
+  b->members.clear();
+  for (auto& ce : b->chunk_events) cudaEventDestroy(ce.second);
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  if (b->d_images) cudaFree(b->d_images);
+  if (b->d_meta) cudaFree(b->d_meta);
+  if (b->d_off) cudaFree(b->d_off);
+  if (b->d_tab) cudaFree(b->d_tab);
+  if (b->h_meta) cudaFreeHost(b->h_meta);
+  if (b->h_off) cudaFreeHost(b->h_off);
+  if (b->h_tab) cudaFreeHost(b->h_tab);
+  if (b->pool_mem) cudaFree(b->pool_mem);
+  if (b->tables_free) cudaEventDestroy(b->tables_free);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->capture) cudaStreamDestroy(b->capture);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return LBM_OK;
+}
+
+int lbm_batch_add(lbm_batch* b, const Inputval* pinput, const lbm_options* opt,
+                  long long target_steps, int* id) {
+  if (!b || !id) return set_error(LBM_ERR_INVALID, "NULL argument");
+  int rc = validate(pinput, opt);
+  if (rc) return rc;
+  if (target_steps < 0) return set_error(LBM_ERR_INVALID, "negative step target");
+  if (opt && opt->storage == LBM_STORE_F64)
+    return set_error(LBM_ERR_INVALID, "FP64 storage is not supported in batches");
+  if (opt && opt->kernel == LBM_KERNEL_PACKED)
+    return set_error(LBM_ERR_INVALID, "batches use the one-node-per-thread kernel");
+  CK(cudaSetDevice(b->opt.device));
+  if (b->free_images.empty() && (rc = grow_images(b))) return rc;
+  lbm_domain* d = new lbm_domain();
+  domain_prepare(d, pinput, opt);
+  d->opt.device = b->opt.device;
+  d->pooled = true;
+  d->stream = b->stream;
+  std::vector<void*> taken;
+  auto alloc = [&](void** p, size_t n) -> int {
+    *p = b->pool.alloc(n);
+    if (!*p) return LBM_ERR_BUDGET;
+    taken.push_back(*p);
+    d->bytes += (n + 255) / 256 * 256;
+    return LBM_OK;
+  };
+  if ((rc = domain_alloc_state(d, alloc))) {
+    for (void* p : taken) b->pool.release(p);
+    delete d;
+    return set_error(LBM_ERR_BUDGET, "domain of %zu bytes does not fit the pool (%zu free)",
+                     domain_state_bytes(pinput, opt), b->pool.largest_free());
+  }
+  lbm_batch::Member m;
+  m.d = d;
+  m.target = target_steps;
+  m.image_slot = b->free_images.back();
+  b->free_images.pop_back();
+  const int new_id = b->next_id++;
+  b->members[new_id] = m;
+  auto undo = [&](int code) {
+    destroy_member(b, b->members[new_id]);
+    b->members.erase(new_id);
+    return code;
+  };
+  // the shared diagnostics / staging buffers of a member come from cudaMalloc
+  // on first use (lbm_diagnostics, lbm_export_arF)
+  cudaDeviceProp prop;
+  cudaGetDeviceProperties(&prop, b->opt.device);
+  d->diag_blocks = 4 * prop.multiProcessorCount;
+  if (cudaMalloc((void**)&d->partial, (size_t)d->diag_blocks * 8 * sizeof(double)) !=
+          cudaSuccess ||
+      cudaMalloc((void**)&d->dout, 8 * sizeof(double)) != cudaSuccess ||
+      cudaMalloc((void**)&d->flag, sizeof(int)) != cudaSuccess ||
+      cudaEventCreate(&d->ev0) != cudaSuccess || cudaEventCreate(&d->ev1) != cudaSuccess)
+    return undo(set_error(LBM_ERR_OOM, "member diagnostics buffers"));
+  if ((rc = domain_upload_profile(d, b->stream)) || (rc = domain_launch_init(d, b->stream)) ||
+      (rc = upload_images(b, b->members[new_id])))
+    return undo(rc);
+  if (target_steps == 0) b->members[new_id].done_chunk = b->chunks_issued;
+  *id = new_id;
+  return LBM_OK;
+}
+
+int lbm_batch_step(lbm_batch* b, int steps) {
+  if (!b) return set_error(LBM_ERR_INVALID, "NULL batch");
+  if (steps < 0) return set_error(LBM_ERR_INVALID, "negative steps");
+  CK(cudaSetDevice(b->opt.device));
+  int rc = ensure_graph(b);
+  if (rc) return rc;
+  CK(cudaEventRecord(b->ev0, b->stream));
+  long long total = 0;
+  int left = steps;
+  while (left > 0) {
+    long long lups = 0;
+    if ((rc = issue_chunk(b, left, &lups))) return rc;
+    if (lups == 0) break;
+    total += lups;
+    left -= std::min(left, chunk_steps(b));
+  }
+  CK(cudaEventRecord(b->ev1, b->stream));
+  b->last_lups = total;
+  b->last_steps = steps - left;
+  retire_completed(b);
+  return LBM_OK;
+}
+
+int lbm_batch_last_step_ms(lbm_batch* b, float* ms, long long* lups) {
+  if (!b || !ms) return set_error(LBM_ERR_INVALID, "NULL argument");
+  CK(cudaEventSynchronize(b->ev1));
+  float t = 0;
+  CK(cudaEventElapsedTime(&t, b->ev0, b->ev1));
+  *ms = b->last_steps > 0 ? t / b->last_steps : 0.0f;
+  if (lups) *lups = b->last_lups;
+  return LBM_OK;
+}
+
+int lbm_batch_poll(lbm_batch* b, int* ids, int max, int* n) {
+  if (!b || !n || (max > 0 && !ids)) return set_error(LBM_ERR_INVALID, "NULL argument");
+  retire_completed(b);
+  int k = 0;
+  for (auto& kv : b->members) {
+    const lbm_batch::Member& m = kv.second;
+    if (m.issued >= m.target && m.done_chunk <= b->chunks_completed) {
+      if (k < max) ids[k] = kv.first;
+      ++k;
+    }
+  }
+  *n = std::min(k, max);
+  return LBM_OK;
+}
+
+int lbm_batch_domain(lbm_batch* b, int id, lbm_domain** d) {
+  if (!b || !d) return set_error(LBM_ERR_INVALID, "NULL argument");
+  auto it = b->members.find(id);
+  if (it == b->members.end()) return set_error(LBM_ERR_INVALID, "no member %d", id);
+  *d = it->second.d;
+  return LBM_OK;
+}
+
+int lbm_batch_remove(lbm_batch* b, int id) {
+  if (!b) return set_error(LBM_ERR_INVALID, "NULL batch");
+  auto it = b->members.find(id);
+  if (it == b->members.end()) return set_error(LBM_ERR_INVALID, "no member %d", id);
+  CK(cudaSetDevice(b->opt.device));
+  if (it->second.issued < it->second.target || it->second.done_chunk > b->chunks_completed)
+    CK(cudaStreamSynchronize(b->stream));
+  else
+    CK(cudaEventSynchronize(b->tables_free));
+  destroy_member(b, it->second);
+  b->members.erase(it);
+  return LBM_OK;
+}
+
+int lbm_batch_sync(lbm_batch* b) {
+  if (!b) return set_error(LBM_ERR_INVALID, "NULL batch");
+  CK(cudaSetDevice(b->opt.device));
+  CK(cudaStreamSynchronize(b->stream));
+  retire_completed(b);
+  return LBM_OK;
+}
+
+int lbm_batch_usage(lbm_batch* b, size_t* used, size_t* largest_free, int* ndomains) {
+  if (!b) return set_error(LBM_ERR_INVALID, "NULL batch");
+  if (used) *used = b->pool.used();
+  if (largest_free) *largest_free = b->pool.largest_free();
+  if (ndomains) *ndomains = (int)b->members.size();
+  return LBM_OK;
+}
+
+int lbm_batch_autotune(lbm_batch* b, int trial_steps, lbm_batch_options* chosen) {
+  if (!b) return set_error(LBM_ERR_INVALID, "NULL batch");
+  if (trial_steps <= 0) return set_error(LBM_ERR_INVALID, "trial_steps must be positive");
+  const int blocks[] = {128, 256};
+  const int npts[] = {1, 2, 4};
+  const int ctas[] = {0, 2};
+  float best = 1e30f;
+  lbm_batch_options keep = b->opt, best_opt = b->opt;
+  for (int blk : blocks)
+    for (int np : npts)
+      for (int c : ctas) {
+        b->opt.block = blk;
+        b->opt.nodes_per_thread = np;
+        b->opt.ctas_per_sm = c;
+        int rc = lbm_batch_step(b, trial_steps);
+        if (rc) {
+          b->opt = keep;
+          return rc;
+        }
+        float ms = 0;
+        long long lups = 0;
+        if ((rc = lbm_batch_last_step_ms(b, &ms, &lups))) {
+          b->opt = keep;
+          return rc;
+        }
+        if (lups == 0) {  // nothing left to step: keep the current shape
+          b->opt = keep;
+          if (chosen) *chosen = keep;
+          return LBM_OK;
+        }
+        const float per_update = ms / (float)lups;
+        if (per_update < best) {
+          best = per_update;
+          best_opt = b->opt;
+        }
+      }
+  b->opt = best_opt;
+  if (chosen) *chosen = best_opt;
+  return ensure_graph(b);
+}
+
+}  // extern "C"

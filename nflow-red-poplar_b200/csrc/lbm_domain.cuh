@@ -1,0 +1,385 @@
+// lbm_domain.cuh — internal state of one resident domain and the helpers
+// shared by the single-domain C ABI (lbm_api.cu) and the batch engine
+// (lbm_batch.cu): validation, sizes, buffer allocation, kernel-argument
+// construction and launch selection.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <type_traits>
+#include <vector>
+
+#include "lbm_internal.h"
+#include "lbm_kernels.cuh"
+
+#define CK(call)                                                                          \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      return set_error(e_ == cudaErrorMemoryAllocation ? LBM_ERR_OOM : LBM_ERR_CUDA,      \
+                       "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, \
+                       __LINE__);                                                         \
+  } while (0)
+
+struct lbm_domain {
+  Inputval in;
+  lbm_options opt;
+  lbm::Geometry g;
+  long long N = 0;    // nodes nx*ny*nz
+  long long qs = 0;   // population stride in elements
+  size_t elem = 4;    // bytes per stored population
+  void* lat[2] = {nullptr, nullptr};
+  int cur = 0;               // lattice holding f*_k
+  bool post_direct = false;  // lat[cur^1] holds arF_k itself
+  long long step = 0;
+  bool initialized = false;
+  float* den[2] = {nullptr, nullptr};  // rho_k in den[k&1], rho_{k-1} in den[(k-1)&1]
+  float* ux = nullptr;
+  float* uy = nullptr;
+  float* uz = nullptr;
+  float* inlet_u = nullptr;                // [ny*nz]
+  float* prho[2] = {nullptr, nullptr};     // [ny*nz]
+  float* pu[2] = {nullptr, nullptr};       // [2][3][ny*nz]
+  float* staging = nullptr;                // AoS import/export buffer
+  size_t staging_bytes = 0;
+  int* flag = nullptr;                     // device error flag
+  double* partial = nullptr;
+  double* dout = nullptr;
+  int diag_blocks = 0;
+  cudaStream_t own = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int last_steps = 0;
+  float scale = 1.f, inv_scale = 1.f;
+  size_t bytes = 0;
+  bool pooled = false;  // buffers belong to a batch pool (lbm_batch), not freed here
+  // CUDA graphs of kGraphSteps plain steps, one per starting lattice
+  cudaGraphExec_t chunk[2] = {nullptr, nullptr};
+  cudaStream_t capture = nullptr;
+};
+
+// steps per captured graph chunk (even, so that a chunk returns the lattices
+// and the boundary planes to the parity it started from)
+constexpr int kGraphSteps = 32;
+
+namespace lbm {
+
+template <class T>
+struct Tag {
+  using type = T;
+};
+
+// call f(Tag<S>{}) with the storage type of the domain
+template <class F>
+int with_storage(int storage, F&& f) {
+  switch (storage) {
+    case LBM_STORE_F32: return f(Tag<float>{});
+    case LBM_STORE_F64: return f(Tag<double>{});
+    case LBM_STORE_F16_SHIFT: return f(Tag<__half>{});
+    case LBM_STORE_BF16_SHIFT: return f(Tag<__nv_bfloat16>{});
+  }
+  return set_error(LBM_ERR_INVALID, "unknown storage %d", storage);
+}
+
+inline size_t storage_bytes(int storage) {
+  switch (storage) {
+    case LBM_STORE_F64: return 8;
+    case LBM_STORE_F16_SHIFT:
+    case LBM_STORE_BF16_SHIFT: return 2;
+    default: return 4;
+  }
+}
+
+inline long long round_up(long long v, long long m) { return (v + m - 1) / m * m; }
+
+inline int validate(const Inputval* in, const lbm_options* opt) {
+  if (!in) return set_error(LBM_ERR_INVALID, "NULL Inputval");
+  if (in->nx < 3 || in->ny < 3 || in->nz < 3)
+    return set_error(LBM_ERR_INVALID, "domain %dx%dx%d too small (each extent must be >= 3)",
+                     in->nx, in->ny, in->nz);
+  if (in->ny > 65535 || in->nz > 65535)
+    return set_error(LBM_ERR_INVALID, "ny and nz must be <= 65535");
+  if (round_up(in->nx, 8) * (long long)in->ny * in->nz >= (1LL << 31) - 1024)
+    return set_error(LBM_ERR_INVALID, "domain too large (px*ny*nz must be < 2^31)");
+  if (in->casetype != CAVITY && in->casetype != CHANNEL)
+    return set_error(LBM_ERR_INVALID,
+                     "casetype %d not supported (CAVITY=1 and CHANNEL=2 are implemented)",
+                     in->casetype);
+  if (!(std::isfinite(in->m_dTau) && in->m_dTau > 0.0f))
+    return set_error(LBM_ERR_INVALID, "relaxation time tau=%g must be positive", in->m_dTau);
+  if (!(std::isfinite(in->m_dRefDen) && in->m_dRefDen > 0.0f))
+    return set_error(LBM_ERR_INVALID, "RefDen=%g must be positive", in->m_dRefDen);
+  if (!std::isfinite(in->m_dSmagorinsky) || !std::isfinite(in->m_dRefVelx) ||
+      !std::isfinite(in->m_dRefVely) || !std::isfinite(in->m_dRefVelz) ||
+      !std::isfinite(in->dWeps) || !std::isfinite(in->dWepsj) || !std::isfinite(in->dWXX))
+    return set_error(LBM_ERR_NOT_FINITE, "non-finite parameter in Inputval");
+  if (opt) {
+    if (opt->storage < LBM_STORE_F32 || opt->storage > LBM_STORE_F64)
+      return set_error(LBM_ERR_INVALID, "unknown storage %d", opt->storage);
+    if (opt->init_kind < LBM_INIT_REFERENCE || opt->init_kind > LBM_INIT_CHANNEL)
+      return set_error(LBM_ERR_INVALID, "unknown init_kind %d", opt->init_kind);
+    if (opt->stream_mode != LBM_STREAM_AB)
+      return set_error(LBM_ERR_INVALID, "stream_mode %d not supported", opt->stream_mode);
+    if (!std::isfinite(opt->noise_amp) || !std::isfinite(opt->store_scale) ||
+        opt->store_scale < 0.0f)
+      return set_error(LBM_ERR_INVALID, "bad noise_amp/store_scale");
+  }
+  return LBM_OK;
+}
+
+struct Sizes {
+  long long N, qs, P;
+  int px;
+};
+
+// Extra elements between population planes (a multiple of 128); a non-zero
+// value keeps the 19 streams of a node off power-of-two distances.
+#ifndef LBM_PLANE_PAD
+#define LBM_PLANE_PAD 0
+#endif
+
+inline Sizes sizes_of(const Inputval* in) {
+  Sizes s;
+  s.px = (int)round_up(in->nx, 8);
+  s.N = (long long)in->nx * in->ny * in->nz;
+  s.qs = round_up((long long)s.px * in->nz * in->ny, 128) + LBM_PLANE_PAD;
+  s.P = (long long)in->ny * in->nz;
+  return s;
+}
+
+inline size_t footprint(const Inputval* in, const lbm_options* opt) {
+  const Sizes s = sizes_of(in);
+  const size_t e = storage_bytes(opt ? opt->storage : LBM_STORE_F32);
+  size_t b = 2 * (size_t)Q * s.qs * e;  // lattices
+  b += 5 * (size_t)s.N * sizeof(float);  // den[2], ux, uy, uz
+  b += 15 * (size_t)s.P * sizeof(float); // inlet profile + planes
+  return b;
+}
+
+inline dim3 block_of(int nx) {
+  int bx = (int)round_up(nx < 128 ? nx : 128, 32);
+  return dim3(bx, 1, 1);
+}
+inline dim3 grid_of(const Geometry& g, dim3 b) {
+  return dim3((g.nx + b.x - 1) / b.x, g.nz, g.ny);
+}
+
+template <class S>
+StepArgs<S> make_args(const lbm_domain* d, const void* src, void* dst, long long k) {
+  using R = RealOf<S>;
+  StepArgs<S> a;
+  std::memset(&a, 0, sizeof(a));
+  a.src = (const S*)src;
+  a.dst = (S*)dst;
+  a.qs = d->qs;
+  for (int q = 0; q < Q; ++q) {
+    a.srcq[q] = src ? (const S*)src + q * d->qs : nullptr;
+    a.dstq[q] = dst ? (S*)dst + q * d->qs : nullptr;
+    a.off[q] = cx(q) + d->g.px * (cz(q) + d->g.nz * cy(q));
+  }
+  a.g = d->g;
+  a.tau = R(d->in.m_dTau);
+  const double cs = (double)d->in.m_dSmagorinsky;
+  a.les_c = R((double)(18.0f * 1.41421356237f) * cs * cs);
+  a.rho0 = R(d->in.m_dRefDen);
+  a.ulx = R(d->in.m_dRefVelx);
+  a.uly = R(d->in.m_dRefVely);
+  a.ulz = R(d->in.m_dRefVelz);
+  a.mp.rho0_inv = R(1) / R(d->in.m_dRefDen);
+  a.mp.weps = R(d->in.dWeps);
+  a.mp.wepsj = R(d->in.dWepsj);
+  a.mp.wxx = R(d->in.dWXX);
+  a.scale = d->scale;
+  a.inv_scale = d->inv_scale;
+  a.inlet_u = d->inlet_u;
+  a.prho_in = d->prho[(k + 1) & 1];  // (k-1)&1
+  a.prho_out = d->prho[k & 1];
+  a.pu_in = d->pu[(k + 1) & 1];
+  a.pu_out = d->pu[k & 1];
+  return a;
+}
+
+// kernel selection by (collision, LES) at run time
+template <class S, class F>
+int with_model(const lbm_domain* d, F&& f) {
+  const bool mrt = d->in.bEnableMRT, les = d->in.bEnableLES;
+  if (mrt && les) return f(std::integral_constant<int, COLL_MRT>{}, std::true_type{});
+  if (mrt) return f(std::integral_constant<int, COLL_MRT>{}, std::false_type{});
+  if (les) return f(std::integral_constant<int, COLL_SRT>{}, std::true_type{});
+  return f(std::integral_constant<int, COLL_SRT>{}, std::false_type{});
+}
+
+// the fused step kernel of the domain's storage: the packed two-node kernel
+// for the FP32-arithmetic formats (unless the scalar one is requested),
+// the scalar kernel for the FP64 build
+template <class S, int COLL, bool LES>
+void launch_step(const lbm_domain* d, const StepArgs<S>& a, cudaStream_t st) {
+  if constexpr (!std::is_same<S, double>::value) {
+    if (d->opt.kernel == LBM_KERNEL_PACKED) {
+      const int pairs = (d->g.nx + 1) / 2;
+      const dim3 b(64, 1, 1), gr((pairs + 63) / 64, d->g.nz, d->g.ny);
+      k_step2<S, COLL, LES><<<gr, b, 0, st>>>(a);
+      return;
+    }
+  }
+  const dim3 b = block_of(d->g.nx), gr = grid_of(d->g, b);
+  k_step<S, COLL, LES><<<gr, b, 0, st>>>(a);
+}
+
+inline int ensure_device(const lbm_domain* d) {
+  CK(cudaSetDevice(d->opt.device));
+  return LBM_OK;
+}
+
+inline int ensure_staging(lbm_domain* d, size_t bytes) {
+  if (d->staging_bytes >= bytes) return LBM_OK;
+  if (d->staging) {
+    CK(cudaFree(d->staging));
+    d->bytes -= d->staging_bytes;
+    d->staging = nullptr;
+    d->staging_bytes = 0;
+  }
+  CK(cudaMalloc(&d->staging, bytes));
+  d->staging_bytes = bytes;
+  d->bytes += bytes;
+  return LBM_OK;
+}
+
+inline void free_all(lbm_domain* d) {
+  if (!d->pooled)
+  for (int i = 0; i < 2; ++i) {
+    if (d->lat[i]) cudaFree(d->lat[i]);
+    if (d->den[i]) cudaFree(d->den[i]);
+    if (d->prho[i]) cudaFree(d->prho[i]);
+    if (d->pu[i]) cudaFree(d->pu[i]);
+  }
+  if (!d->pooled) {
+    if (d->ux) cudaFree(d->ux);
+    if (d->uy) cudaFree(d->uy);
+    if (d->uz) cudaFree(d->uz);
+    if (d->inlet_u) cudaFree(d->inlet_u);
+  }
+  if (d->staging) cudaFree(d->staging);
+  if (d->flag) cudaFree(d->flag);
+  if (d->partial) cudaFree(d->partial);
+  if (d->dout) cudaFree(d->dout);
+  for (int i = 0; i < 2; ++i)
+    if (d->chunk[i]) cudaGraphExecDestroy(d->chunk[i]);
+  if (d->capture) cudaStreamDestroy(d->capture);
+  if (d->ev0) cudaEventDestroy(d->ev0);
+  if (d->ev1) cudaEventDestroy(d->ev1);
+  if (d->own) cudaStreamDestroy(d->own);
+}
+
+
+// Fill the geometry, sizes and storage scale of d from the case.
+inline void domain_prepare(lbm_domain* d, const Inputval* pinput, const lbm_options* opt) {
+  d->in = *pinput;
+  if (opt)
+    d->opt = *opt;
+  else
+    lbm_default_options(&d->opt);
+  const Sizes s = sizes_of(pinput);
+  d->g.nx = pinput->nx;
+  d->g.ny = pinput->ny;
+  d->g.nz = pinput->nz;
+  d->g.px = s.px;
+  d->g.casetype = pinput->casetype;
+  d->N = s.N;
+  d->qs = s.qs;
+  d->elem = storage_bytes(d->opt.storage);
+  if (d->opt.storage == LBM_STORE_F16_SHIFT || d->opt.storage == LBM_STORE_BF16_SHIFT) {
+    float sc = d->opt.store_scale;
+    if (sc == 0.0f) sc = d->opt.storage == LBM_STORE_F16_SHIFT ? 1024.0f : 1.0f;
+    d->scale = sc;
+    d->inv_scale = 1.0f / sc;
+  }
+}
+
+// Allocate the state buffers of d (lattices, macroscopic fields, boundary
+// planes) through alloc(void** p, size_t bytes) -> status.
+template <class Alloc>
+int domain_alloc_state(lbm_domain* d, Alloc&& alloc) {
+  const size_t lat_bytes = (size_t)Q * d->qs * d->elem;
+  const size_t nb = (size_t)d->N * sizeof(float);
+  const size_t pb = (size_t)d->g.ny * d->g.nz * sizeof(float);
+  int rc;
+  if ((rc = alloc(&d->lat[0], lat_bytes)) || (rc = alloc(&d->lat[1], lat_bytes)) ||
+      (rc = alloc((void**)&d->den[0], nb)) || (rc = alloc((void**)&d->den[1], nb)) ||
+      (rc = alloc((void**)&d->ux, nb)) || (rc = alloc((void**)&d->uy, nb)) ||
+      (rc = alloc((void**)&d->uz, nb)) || (rc = alloc((void**)&d->inlet_u, pb)) ||
+      (rc = alloc((void**)&d->prho[0], pb)) || (rc = alloc((void**)&d->prho[1], pb)) ||
+      (rc = alloc((void**)&d->pu[0], 6 * pb)) || (rc = alloc((void**)&d->pu[1], 6 * pb)))
+    return rc;
+  return LBM_OK;
+}
+
+// Bytes domain_alloc_state takes (each buffer rounded to 256 bytes).
+inline size_t domain_state_bytes(const Inputval* in, const lbm_options* opt) {
+  const Sizes s = sizes_of(in);
+  auto r = [](size_t b) { return (b + 255) / 256 * 256; };
+  const size_t e = storage_bytes(opt ? opt->storage : LBM_STORE_F32);
+  const size_t nb = (size_t)s.N * sizeof(float), pb = (size_t)s.P * sizeof(float);
+  return 2 * r((size_t)Q * s.qs * e) + 5 * r(nb) + 3 * r(pb) + 2 * r(6 * pb);
+}
+
+// Upload the channel inlet profile u_x(y,z) = u_max 16 eta(1-eta) zeta(1-zeta).
+inline int domain_upload_profile(lbm_domain* d, cudaStream_t st) {
+  if (d->g.casetype != CHANNEL) return LBM_OK;
+  std::vector<float> prof((size_t)d->g.ny * d->g.nz);
+  for (int y = 0; y < d->g.ny; ++y)
+    for (int z = 0; z < d->g.nz; ++z) {
+      const double eta = (double)y / (double)(d->g.ny - 1);
+      const double zeta = (double)z / (double)(d->g.nz - 1);
+      prof[(size_t)y * d->g.nz + z] =
+          (float)((double)d->in.m_dRefVelx * 16.0 * eta * (1.0 - eta) * zeta * (1.0 - zeta));
+    }
+  CK(cudaMemcpyAsync(d->inlet_u, prof.data(), prof.size() * sizeof(float), cudaMemcpyHostToDevice,
+                     st));
+  CK(cudaStreamSynchronize(st));
+  return LBM_OK;
+}
+
+// InitParams of the domain's initial condition.
+inline InitParams init_params(const lbm_domain* d) {
+  InitParams ip;
+  ip.kind = d->opt.init_kind;
+  ip.seed = d->opt.seed;
+  ip.noise_amp = d->opt.noise_amp;
+  ip.rho0 = d->in.m_dRefDen;
+  ip.ulx = d->in.m_dRefVelx;
+  ip.uly = d->in.m_dRefVely;
+  ip.ulz = d->in.m_dRefVelz;
+  return ip;
+}
+
+// Launch the initial-state kernel of d on st (post lattice lat[1], first
+// collision into lat[0]) and reset the step state.
+inline int domain_launch_init(lbm_domain* d, cudaStream_t st) {
+  const InitParams ip = init_params(d);
+  int rc = with_storage(d->opt.storage, [&](auto tag) -> int {
+    using S = typename decltype(tag)::type;
+    return with_model<S>(d, [&](auto coll, auto les) -> int {
+      StepArgs<S> a = make_args<S>(d, nullptr, d->lat[1], 0);
+      a.den_out = d->den[0];
+      a.ux_out = d->ux;
+      a.uy_out = d->uy;
+      a.uz_out = d->uz;
+      const dim3 b = block_of(d->g.nx), gr = grid_of(d->g, b);
+      k_init<S, decltype(coll)::value, decltype(les)::value>
+          <<<gr, b, 0, st>>>(a, (S*)d->lat[0], ip);
+      CK(cudaGetLastError());
+      return LBM_OK;
+    });
+  });
+  if (rc) return rc;
+  d->cur = 0;
+  d->post_direct = true;
+  d->step = 0;
+  d->initialized = true;
+  d->last_steps = 0;
+  return LBM_OK;
+}
+
+}  // namespace lbm

@@ -259,13 +259,12 @@ struct StoreNode {
   }
 };
 
-// The fused step.  grid = (ceil(nx/blockDim.x), nz, ny), one thread per node.
+// One fused step of the node (x, y, z): pull + boundary rules, macroscopic,
+// LES, collision, store.  Shared by the single-domain and batched kernels,
+// so a domain gets the same bits alone and in a batch.
 template <class S, int COLL, bool LES>
-__global__ void __launch_bounds__(128) k_step(const __grid_constant__ StepArgs<S> a) {
+__device__ __forceinline__ void step_node(const StepArgs<S>& a, int x, int y, int z) {
   using R = RealOf<S>;
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int z = blockIdx.y, y = blockIdx.z;
-  if (x >= a.g.nx) return;
   const int cell = x + a.g.px * (z + a.g.nz * y);
   R f[Q];
   pull<S>(f, a, x, y, z, cell);
@@ -277,6 +276,15 @@ __global__ void __launch_bounds__(128) k_step(const __grid_constant__ StepArgs<S
   collide_node<S, COLL, LES, false, R>(f, ps, ux, uy, uz, inv_rho, a, [&](int q, R v) {
     StoreTraits<S>::store(a.dstq[q] + cell, v, weight<R>(q), a.scale);
   });
+}
+
+// The fused step.  grid = (ceil(nx/blockDim.x), nz, ny), one thread per node.
+template <class S, int COLL, bool LES>
+__global__ void __launch_bounds__(128) k_step(const __grid_constant__ StepArgs<S> a) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int z = blockIdx.y, y = blockIdx.z;
+  if (x >= a.g.nx) return;
+  step_node<S, COLL, LES>(a, x, y, z);
 }
 
 // ------------------------------------------------------------------ //

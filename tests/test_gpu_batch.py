@@ -1,0 +1,136 @@
+"""The batched form: many domains in one persistent launch per step.
+
+A domain's result is the same alone and in a mix (same per-node code, no
+cross-domain data), so alone-vs-batch is compared bit for bit; admission is
+by the HBM budget of the batch pool; continuous batching admits domains
+between chunks and retires them at their own step targets.
+"""
+import numpy as np
+import pytest
+
+import oracle_lib as O
+
+pkg = O.pkg
+pytestmark = pytest.mark.gpu
+
+
+def cavity(n, ny=None, nz=None, re=200.0, mrt=True, les=True, cs=0.1):
+    return pkg.make_inputval(n, ny, nz, casetype=pkg.CAVITY, re=re, u=0.1, mrt=mrt, les=les, cs=cs,
+                             h=n)
+
+
+def channel(nx, ny, nz, mrt=True, les=True):
+    return pkg.make_inputval(nx, ny, nz, casetype=pkg.CHANNEL, tau=0.56, u=0.05, mrt=mrt, les=les,
+                             cs=0.1)
+
+
+CASES = [
+    (cavity(24, 20, 18), pkg.STORE_F32, 1, 1e-6),
+    (cavity(32, mrt=False, les=False), pkg.STORE_F32, 1, 1e-6),
+    (cavity(16, 20, 24, mrt=True, les=False), pkg.STORE_F16_SHIFT, 1, 1e-6),
+    (channel(48, 12, 14), pkg.STORE_F32, pkg.INIT_CHANNEL, 0.01),
+    (channel(40, 16, 12, mrt=False, les=True), pkg.STORE_BF16_SHIFT, pkg.INIT_CHANNEL, 0.01),
+    (cavity(40, 24, 28, re=500.0), pkg.STORE_F16_SHIFT, 1, 1e-6),
+]
+
+
+def opts(storage, kind, amp, seed=3):
+    return pkg.default_options(storage=storage, init_kind=kind, noise_amp=amp, seed=seed)
+
+
+def alone(iv, o, steps):
+    d = pkg.Domain(iv, o)
+    d.run(steps)
+    f = d.export_arF()
+    m = d.macroscopic()
+    d.close()
+    return f, m
+
+
+@pytest.mark.parametrize("steps", [1, 37, 100])
+def test_batch_matches_alone_bit_for_bit(steps):
+    b = pkg.Batch(hbm_budget=512 << 20, chunk_steps=16)
+    ids = [b.add(iv, opts(st, k, a), steps) for iv, st, k, a in CASES]
+    b.step(steps)
+    b.sync()
+    assert sorted(b.poll()) == sorted(ids)
+    for i, (iv, st, k, a) in zip(ids, CASES):
+        m = b.member(i)
+        assert m.steps() == steps
+        f_b = m.export_arF()
+        mac_b = m.macroscopic()
+        f_a, mac_a = alone(iv, opts(st, k, a), steps)
+        np.testing.assert_array_equal(f_b, f_a)
+        for x, y in zip(mac_b, mac_a):
+            np.testing.assert_array_equal(x, y)
+    b.close()
+
+
+def test_continuous_batching_targets_and_late_admission():
+    b = pkg.Batch(hbm_budget=512 << 20, chunk_steps=8)
+    iv0, st0, k0, a0 = CASES[0]
+    iv1, st1, k1, a1 = CASES[2]
+    iv2, st2, k2, a2 = CASES[3]
+    i0 = b.add(iv0, opts(st0, k0, a0), 20)
+    i1 = b.add(iv1, opts(st1, k1, a1), 50)
+    b.step(24)  # i0 finishes at 20 inside the third chunk
+    b.sync()
+    assert b.poll() == [i0]
+    i2 = b.add(iv2, opts(st2, k2, a2), 30)  # joins while i1 is running
+    b.step(40)
+    b.sync()
+    assert sorted(b.poll()) == sorted([i0, i1, i2])
+    for i, case, n in ((i0, CASES[0], 20), (i1, CASES[2], 50), (i2, CASES[3], 30)):
+        iv, st, k, a = case
+        f_b = b.member(i).export_arF()
+        f_a, _ = alone(iv, opts(st, k, a), n)
+        np.testing.assert_array_equal(f_b, f_a)
+    b.close()
+
+
+def test_budget_admission_and_release():
+    iv = cavity(32)
+    o = opts(pkg.STORE_F32, 1, 1e-6)
+    per = pkg.batch_domain_bytes(iv, o)
+    b = pkg.Batch(hbm_budget=int(per * 2.5), chunk_steps=8)
+    i0 = b.add(iv, o, 10)
+    i1 = b.add(iv, o, 10)
+    with pytest.raises(pkg.LbmError) as e:
+        b.add(iv, o, 10)
+    assert e.value.code == pkg.LBM_ERR_BUDGET
+    used, free, n = b.usage()
+    assert n == 2 and used >= 2 * per
+    b.step(10)
+    b.sync()
+    b.remove(i0)
+    i2 = b.add(iv, o, 5)  # the released memory is reused
+    b.step(5)
+    b.sync()
+    assert set(b.poll()) == {i1, i2}
+    b.close()
+
+
+def test_autotune_keeps_results():
+    b = pkg.Batch(hbm_budget=512 << 20, chunk_steps=8)
+    ids = [b.add(iv, opts(st, k, a), 10 ** 6) for iv, st, k, a in CASES]
+    cfg = b.autotune(trial_steps=8)
+    assert cfg["block"] in (128, 256) and cfg["nodes_per_thread"] in (1, 2, 4)
+    done = b.member(ids[0]).steps()
+    b.step(8)
+    b.sync()
+    f_b = b.member(ids[0]).export_arF()
+    iv, st, k, a = CASES[0]
+    f_a, _ = alone(iv, opts(st, k, a), done + 8)
+    np.testing.assert_array_equal(f_b, f_a)
+    ms, lups = b.last_step_ms()
+    assert ms > 0 and lups > 0
+    b.close()
+
+
+def test_batch_rejects_fp64_and_bad_options():
+    b = pkg.Batch(hbm_budget=64 << 20)
+    with pytest.raises(pkg.LbmError):
+        b.add(cavity(8), pkg.default_options(storage=pkg.STORE_F64), 4)
+    b.close()
+    with pytest.raises(pkg.LbmError):
+        pkg.Batch(hbm_budget=64 << 20, chunk_steps=7)
