@@ -163,7 +163,8 @@ enum {
 enum {
   LBM_KERNEL_AUTO = 0,    /* the fastest variant for the format             */
   LBM_KERNEL_SCALAR = 1,  /* one node per thread                            */
-  LBM_KERNEL_PACKED = 2   /* two nodes per thread, packed FP32 arithmetic   */
+  LBM_KERNEL_PACKED = 2,  /* two nodes per thread, packed FP32 arithmetic   */
+  LBM_KERNEL_TMA = 3      /* TMA-staged tiles, persistent producer/consumer */
 };
 
 typedef struct lbm_options {

@@ -39,7 +39,7 @@ LBM_ERR_NO_DEVICE = -9
 STORE_F32, STORE_F16_SHIFT, STORE_BF16_SHIFT, STORE_F64 = 0, 1, 2, 3
 INIT_REFERENCE, INIT_DENSITY_NOISE, INIT_CHANNEL = 0, 1, 2
 STREAM_AB, STREAM_AA = 0, 1
-KERNEL_AUTO, KERNEL_SCALAR, KERNEL_PACKED = 0, 1, 2
+KERNEL_AUTO, KERNEL_SCALAR, KERNEL_PACKED, KERNEL_TMA = 0, 1, 2, 3
 
 
 class Inputval(C.Structure):

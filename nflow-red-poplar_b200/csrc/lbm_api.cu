@@ -145,8 +145,15 @@ int lbm_create(const Inputval* pinput, const lbm_options* opt, lbm_domain** out)
     d->bytes += b;
     return LBM_OK;
   };
-  if ((rc = domain_alloc_state(d, alloc)) || (rc = alloc((void**)&d->flag, sizeof(int))))
+  if ((rc = domain_alloc_state(d, alloc)) || (rc = alloc((void**)&d->flag, 2 * sizeof(int))))
     return fail(rc);
+  if (cudaMemset(d->flag, 0, 2 * sizeof(int)) != cudaSuccess)
+    return fail(set_error(LBM_ERR_CUDA, "flag reset failed"));
+  rc = with_storage(d->opt.storage, [&](auto tag) -> int {
+    using S = typename decltype(tag)::type;
+    return domain_tensor_maps<S>(d, prop.multiProcessorCount);
+  });
+  if (rc) return fail(rc);
   d->diag_blocks = 4 * prop.multiProcessorCount;
   if ((rc = alloc((void**)&d->partial, (size_t)d->diag_blocks * 8 * sizeof(double))) ||
       (rc = alloc((void**)&d->dout, 8 * sizeof(double))))
@@ -336,7 +343,7 @@ int lbm_export_arF(lbm_domain* d, float* arF, int padded) {
   if (rc) return rc;
   CK(cudaMemcpyAsync(arF, d->staging, bytes, cudaMemcpyDeviceToHost, d->stream));
   CK(cudaStreamSynchronize(d->stream));
-  return LBM_OK;
+  return check_kernel_error(d);
 }
 
 int lbm_get_macroscopic(lbm_domain* d, float* den, float* velx, float* vely, float* velz) {
@@ -350,7 +357,7 @@ int lbm_get_macroscopic(lbm_domain* d, float* den, float* velx, float* vely, flo
   if (vely) CK(cudaMemcpyAsync(vely, d->uy, nb, cudaMemcpyDeviceToHost, d->stream));
   if (velz) CK(cudaMemcpyAsync(velz, d->uz, nb, cudaMemcpyDeviceToHost, d->stream));
   CK(cudaStreamSynchronize(d->stream));
-  return LBM_OK;
+  return check_kernel_error(d);
 }
 
 int lbm_get_node_info(lbm_domain* d, int* node_type, int* direction_state) {
@@ -391,7 +398,7 @@ int lbm_sync(lbm_domain* d) {
   int rc = ensure_device(d);
   if (rc) return rc;
   CK(cudaStreamSynchronize(d->stream));
-  return LBM_OK;
+  return check_kernel_error(d);
 }
 
 int lbm_device_bytes(const lbm_domain* d, size_t* bytes) {

@@ -566,7 +566,8 @@ int lbm_batch_add(lbm_batch* b, const Inputval* pinput, const lbm_options* opt,
   if (cudaMalloc((void**)&d->partial, (size_t)d->diag_blocks * 8 * sizeof(double)) !=
           cudaSuccess ||
       cudaMalloc((void**)&d->dout, 8 * sizeof(double)) != cudaSuccess ||
-      cudaMalloc((void**)&d->flag, sizeof(int)) != cudaSuccess ||
+      cudaMalloc((void**)&d->flag, 2 * sizeof(int)) != cudaSuccess ||
+      cudaMemset(d->flag, 0, 2 * sizeof(int)) != cudaSuccess ||
       cudaEventCreate(&d->ev0) != cudaSuccess || cudaEventCreate(&d->ev1) != cudaSuccess)
     return undo(set_error(LBM_ERR_OOM, "member diagnostics buffers"));
   if ((rc = domain_upload_profile(d, b->stream)) || (rc = domain_launch_init(d, b->stream)) ||

@@ -12,6 +12,7 @@
 
 #include "lbm_internal.h"
 #include "lbm_kernels.cuh"
+#include "lbm_tma.cuh"
 
 #define CK(call)                                                                          \
   do {                                                                                    \
@@ -43,7 +44,10 @@ struct lbm_domain {
   float* pu[2] = {nullptr, nullptr};       // [2][3][ny*nz]
   float* staging = nullptr;                // AoS import/export buffer
   size_t staging_bytes = 0;
-  int* flag = nullptr;                     // device error flag
+  int* flag = nullptr;                     // device words: [0] input check, [1] kernel error
+  CUtensorMap tmap[2];                     // TMA views of lat[0], lat[1] (16-bit / FP32)
+  bool tmap_ok = false;
+  int tma_grid = 0;                        // persistent CTAs of the TMA kernel
   double* partial = nullptr;
   double* dout = nullptr;
   int diag_blocks = 0;
@@ -222,9 +226,91 @@ void launch_step(const lbm_domain* d, const StepArgs<S>& a, cudaStream_t st) {
       k_step2<S, COLL, LES><<<gr, b, 0, st>>>(a);
       return;
     }
+    if (d->opt.kernel == LBM_KERNEL_TMA && d->tmap_ok) {
+      using Cfg = TmaCfg<S>;
+      const int which = (a.src == (const S*)d->lat[0]) ? 0 : 1;
+      k_step_tma<S, COLL, LES><<<d->tma_grid, Cfg::THREADS, Cfg::SMEM, st>>>(a, d->tmap[which],
+                                                                            d->flag + 1);
+      return;
+    }
   }
   const dim3 b = block_of(d->g.nx), gr = grid_of(d->g, b);
   k_step<S, COLL, LES><<<gr, b, 0, st>>>(a);
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library)
+typedef CUresult (*TensorMapEncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                      const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                      const cuuint32_t*, CUtensorMapInterleave,
+                                      CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                      CUtensorMapFloatOOBfill);
+inline TensorMapEncodeFn tensor_map_encoder() {
+  static TensorMapEncodeFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (TensorMapEncodeFn)p;
+  }
+  return fn;
+}
+
+// 4-D views (x, z, y, q) of both lattices with the TMA box of TmaCfg<S>,
+// and the persistent grid of the TMA kernel.  Leaves tmap_ok false (the
+// kernel option then falls back to the scalar kernel) for FP64 storage.
+template <class S>
+int domain_tensor_maps(lbm_domain* d, int sm_count) {
+  if constexpr (std::is_same<S, double>::value) {
+    d->tmap_ok = false;
+    return LBM_OK;
+  } else {
+    using Cfg = TmaCfg<S>;
+    TensorMapEncodeFn enc = tensor_map_encoder();
+    if (!enc) return set_error(LBM_ERR_CUDA, "cuTensorMapEncodeTiled not available");
+    const CUtensorMapDataType dt = std::is_same<S, float>::value ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                   : std::is_same<S, __half>::value
+                                       ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+                                       : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+    const cuuint64_t es = sizeof(S);
+    const cuuint64_t dims[4] = {(cuuint64_t)d->g.nx, (cuuint64_t)d->g.nz, (cuuint64_t)d->g.ny,
+                                (cuuint64_t)Q};
+    const cuuint64_t strides[3] = {(cuuint64_t)d->g.px * es,
+                                   (cuuint64_t)d->g.px * d->g.nz * es, (cuuint64_t)d->qs * es};
+    const cuuint32_t box[4] = {(cuuint32_t)Cfg::TXB, (cuuint32_t)Cfg::TZ, 1, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    for (int i = 0; i < 2; ++i) {
+      CUresult r = enc(&d->tmap[i], dt, 4, d->lat[i], dims, strides, box, estr,
+                       CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                       CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (r != CUDA_SUCCESS) return set_error(LBM_ERR_CUDA, "tensor map encoding failed (%d)", (int)r);
+    }
+    int rc = with_model<S>(d, [&](auto coll, auto les) -> int {
+      auto kern = k_step_tma<S, decltype(coll)::value, decltype(les)::value>;
+      CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM));
+      int per_sm = 0;
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Cfg::THREADS, Cfg::SMEM));
+      if (per_sm < 1) return set_error(LBM_ERR_CUDA, "TMA kernel does not fit an SM");
+      const long long ntiles = (long long)((d->g.nx + Cfg::TX - 1) / Cfg::TX) *
+                               ((d->g.nz + Cfg::TZ - 1) / Cfg::TZ) * d->g.ny;
+      d->tma_grid = (int)std::min<long long>(ntiles, (long long)per_sm * sm_count);
+      return LBM_OK;
+    });
+    if (rc) return rc;
+    d->tmap_ok = true;
+    return LBM_OK;
+  }
+}
+
+// LBM_ERR_TIMEOUT if a kernel of the domain reported a failed bounded wait
+inline int check_kernel_error(lbm_domain* d) {
+  int e = 0;
+  CK(cudaMemcpyAsync(&e, d->flag + 1, sizeof(int), cudaMemcpyDeviceToHost, d->stream));
+  CK(cudaStreamSynchronize(d->stream));
+  if (e) return set_error(LBM_ERR_TIMEOUT, "a step kernel gave up a bounded wait (code %d)", e);
+  return LBM_OK;
 }
 
 inline int ensure_device(const lbm_domain* d) {

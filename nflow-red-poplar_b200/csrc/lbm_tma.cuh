@@ -1,0 +1,223 @@
+// lbm_tma.cuh — the fused step with TMA-staged populations (sm_100a).
+//
+// Persistent CTAs: one producer warp and CONSUMER_WARPS consumer warps.  A
+// tile is TX x TZ nodes of one y plane (x fastest).  For population q of a
+// tile the producer issues one cp.async.bulk.tensor.4d load of the box of
+// donors x - c_q into a shared-memory stage: the box starts at
+// (x0 - HX, z0 - c_z, y - c_y, q) and is TX + 2 HX wide so that every x
+// coordinate stays 16-byte aligned (HX = 16 bytes of elements) and the
+// c_x = +-1 shifts are read from the halo; coordinates outside the domain
+// are zero-filled by the TMA unit and belong to boundary nodes, which take
+// the per-node boundary path.  Stages form a ring guarded by mbarriers
+// (full: TMA bytes landed; empty: every consumer warp is done with it).
+// Consumers take x-pairs, read their 19 populations from shared memory,
+// evaluate the node arithmetic on packed FP32 lanes (F2) and store f*
+// straight to global memory.
+//
+// The loads never occupy registers or load slots, so the memory
+// parallelism is set by the stage count, not by occupancy: this is what
+// lets the 16-bit storage formats run at their own bandwidth roofline.
+//
+// Every mbarrier wait is bounded; a wait that gives up writes a code into
+// the domain's error word and the thread stops (the host reports
+// LBM_ERR_TIMEOUT at its next synchronising call).  The producer issues
+// loads only for stages the consumers will drain, so in normal operation
+// the CTA (and its shared memory) outlives every load it issued.
+#pragma once
+#include <cuda.h>
+
+#include "lbm_kernels.cuh"
+
+namespace lbm {
+
+template <class S>
+struct TmaCfg {
+  static constexpr int TX = 128;                       // tile nodes along x
+  static constexpr int TZ = 4;                         // tile rows along z
+  static constexpr int HX = 16 / (int)sizeof(S);       // 16-byte x halo
+  static constexpr int TXB = TX + 2 * HX;              // box width
+  static constexpr int BOX_BYTES = TXB * TZ * (int)sizeof(S);
+  static constexpr int BOX_STRIDE = (BOX_BYTES + 127) / 128 * 128;
+  static constexpr int STAGE_BYTES = Q * BOX_STRIDE;
+  static constexpr int STAGES = sizeof(S) == 4 ? 3 : 4;
+  static constexpr int CONSUMER_WARPS = TX / 2 * TZ / 32;  // one x-pair per thread
+  static constexpr int THREADS = (CONSUMER_WARPS + 1) * 32;
+  static constexpr int SMEM = STAGES * STAGE_BYTES + 2 * STAGES * 8 + 128;
+  static_assert(BOX_BYTES % 16 == 0, "TMA box row must be a multiple of 16 bytes");
+  static_assert(TXB <= 256 && TZ <= 256, "TMA box dimension limit");
+};
+
+// bounded mbarrier waits: about a second of try_wait before giving up
+constexpr int kWaitIters = 1 << 20;
+constexpr int kErrProducerWait = 1;
+constexpr int kErrConsumerWait = 2;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (int i = 0; i < kWaitIters; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map, int c0, int c1,
+                                            int c2, int c3, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(dst),
+      "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
+      : "memory");
+}
+
+// a pair of populations from shared memory as packed FP32 (aligned: c_x = 0)
+template <class S>
+__device__ __forceinline__ F2 lds_pair(const S* p, int q, float inv_scale);
+template <>
+__device__ __forceinline__ F2 lds_pair<float>(const float* p, int, float) {
+  return F2{*reinterpret_cast<const float2*>(p)};
+}
+template <>
+__device__ __forceinline__ F2 lds_pair<__half>(const __half* p, int q, float inv_scale) {
+  const float2 h = __half22float2(*reinterpret_cast<const __half2*>(p));
+  const float w = weight<float>(q);
+  return F2{__ffma2_rn(h, make_float2(inv_scale, inv_scale), make_float2(w, w))};
+}
+template <>
+__device__ __forceinline__ F2 lds_pair<__nv_bfloat16>(const __nv_bfloat16* p, int q,
+                                                      float inv_scale) {
+  const float2 h = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(p));
+  const float w = weight<float>(q);
+  return F2{__ffma2_rn(h, make_float2(inv_scale, inv_scale), make_float2(w, w))};
+}
+
+template <class S, int COLL, bool LES>
+__global__ void __launch_bounds__(TmaCfg<S>::THREADS, 1)
+    k_step_tma(const __grid_constant__ StepArgs<S> a, const __grid_constant__ CUtensorMap src_map,
+               int* __restrict__ err) {
+  using C = TmaCfg<S>;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* smem =
+      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::STAGES * C::STAGE_BYTES);
+  uint64_t* empty = full + C::STAGES;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nx = a.g.nx, ny = a.g.ny, nz = a.g.nz;
+  const int ntx = (nx + C::TX - 1) / C::TX, nzb = (nz + C::TZ - 1) / C::TZ;
+  const long long ntiles = (long long)ntx * nzb * ny;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < C::STAGES; ++s) {
+      mbar_init(smem_addr(&full[s]), 1);
+      mbar_init(smem_addr(&empty[s]), C::CONSUMER_WARPS);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+
+  if (warp == C::CONSUMER_WARPS) {
+    // ---------------- producer: one elected lane ----------------
+    if (lane != 0) return;
+    int i = 0;
+    for (long long t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
+      const int s = i % C::STAGES;
+      const uint32_t ph = (uint32_t)(i / C::STAGES) & 1u;
+      if (!mbar_wait(smem_addr(&empty[s]), ph ^ 1u)) {
+        atomicExch(err, kErrProducerWait);
+        break;
+      }
+      const int xt = (int)(t % ntx);
+      const long long rest = t / ntx;
+      const int zb = (int)(rest % nzb);
+      const int y = (int)(rest / nzb);
+      const int x0 = xt * C::TX, z0 = zb * C::TZ;
+      const uint32_t bar = smem_addr(&full[s]);
+      mbar_expect_tx(bar, (uint32_t)(Q * C::BOX_BYTES));
+      unsigned char* stage = smem + s * C::STAGE_BYTES;
+      static_for<0, Q>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        tma_load_4d(smem_addr(stage + q * C::BOX_STRIDE), &src_map, x0 - C::HX, z0 - cz(q),
+                    y - cy(q), q, bar);
+      });
+    }
+    return;
+  }
+
+  // ---------------- consumers ----------------
+  const int r = threadIdx.x / (C::TX / 2);
+  const int xl = 2 * (threadIdx.x % (C::TX / 2));
+  int i = 0;
+  for (long long t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
+    const int s = i % C::STAGES;
+    const uint32_t ph = (uint32_t)(i / C::STAGES) & 1u;
+    if (!mbar_wait(smem_addr(&full[s]), ph)) {
+      atomicExch(err, kErrConsumerWait);
+      return;
+    }
+    const int xt = (int)(t % ntx);
+    const long long rest = t / ntx;
+    const int zb = (int)(rest % nzb);
+    const int y = (int)(rest / nzb);
+    const int x = xt * C::TX + xl, z = zb * C::TZ + r;
+    if (x < nx && z < nz) {
+      const bool two = x + 1 < nx;
+      const bool interior = x >= 1 && x + 1 <= nx - 2 && y >= 1 && y <= ny - 2 && z >= 1 &&
+                            z <= nz - 2;
+      if (interior) {
+        const S* stage = reinterpret_cast<const S*>(smem + s * C::STAGE_BYTES);
+        const int cell = x + a.g.px * (z + nz * y);
+        F2 f[Q];
+        static_for<0, Q>([&](auto qc) {
+          constexpr int q = decltype(qc)::value;
+          const S* p = stage + q * (C::BOX_STRIDE / (int)sizeof(S)) + r * C::TXB + xl + C::HX -
+                       cx(q);
+          if constexpr (cx(q) == 0) {
+            f[q] = lds_pair<S>(p, q, a.inv_scale);
+          } else {
+            f[q] = mk2(StoreTraits<S>::load(p, weight<float>(q), a.inv_scale),
+                       StoreTraits<S>::load(p + 1, weight<float>(q), a.inv_scale));
+          }
+        });
+        PairState<F2> ps;
+        make_pairs<F2>(f, ps);
+        F2 ux, uy, uz;
+        const F2 inv_rho = velocity<F2>(ps, ux, uy, uz);
+        if (a.den_out || a.ux_out || a.g.casetype == CHANNEL) {
+          write_macro<S>(a, x, y, z, ps.rho.v.x, ux.v.x, uy.v.x, uz.v.x);
+          write_macro<S>(a, x + 1, y, z, ps.rho.v.y, ux.v.y, uy.v.y, uz.v.y);
+        }
+        collide_node<S, COLL, LES, true, F2>(f, ps, ux, uy, uz, inv_rho, a, [&](int q, F2 v) {
+          st_pair<S>(a.dstq[q] + cell, v, q, a.scale);
+        });
+      } else {
+        // boundary nodes: the per-node path with the boundary rules (global loads)
+        step_node<S, COLL, LES>(a, x, y, z);
+        if (two) step_node<S, COLL, LES>(a, x + 1, y, z);
+      }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(smem_addr(&empty[s]));
+  }
+}
+
+}  // namespace lbm
