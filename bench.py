@@ -236,7 +236,7 @@ def main():
     ap.add_argument("--workload", default="cavity256_mrt_les", choices=sorted(WORKLOADS))
     ap.add_argument("--storage", default="f32", choices=["f32", "f16_shift", "bf16_shift", "f64"])
     ap.add_argument("--size", type=int, default=0, help="scale the workload to this nx (profiling)")
-    ap.add_argument("--kernel", default="auto", choices=["auto", "scalar", "packed"])
+    ap.add_argument("--kernel", default="auto", choices=["auto", "scalar", "packed", "tma"])
     ap.add_argument("--no-extras", action="store_true",
                     help="skip cpu baseline, e2e and storage forms (profiling runs)")
     args = ap.parse_args()
@@ -283,7 +283,8 @@ def main():
         opt = pkg.default_options(storage=storage_id[storage], init_kind=w["init"],
                                   noise_amp=w["amp"], seed=1, device=local,
                                   kernel={"auto": pkg.KERNEL_AUTO, "scalar": pkg.KERNEL_SCALAR,
-                                          "packed": pkg.KERNEL_PACKED}[args.kernel])
+                                          "packed": pkg.KERNEL_PACKED,
+                                          "tma": pkg.KERNEL_TMA}[args.kernel])
         dom = pkg.Domain(iv, opt)
         dom.set_stream(stream.cuda_stream)
         dom.run(warm)
