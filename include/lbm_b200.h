@@ -293,6 +293,25 @@ int lbm_get_node_info(lbm_domain* d, int* node_type, int* direction_state);
  * Synchronises the handle's stream. */
 int lbm_diagnostics(lbm_domain* d, double out[8]);
 
+/* No counterpart in the reference.  The diagnostics of lbm_diagnostics
+ * (same 8 values, same order, FP64) over caller-owned device arrays of n
+ * nodes, for callers that cannot allocate device memory when they need them:
+ * a serving loop whose device memory is all handed to resident domains, code
+ * that must not synchronise the device the way cudaMalloc/cudaFree may, or
+ * fields whose memory belongs to another runtime.  It allocates nothing:
+ * the per-block partial sums live in a file-scope __device__ array of the
+ * library sized for at most 67,108,864 nodes (264 KB, held by every GPU that
+ * loads the library until exit); larger n returns LBM_ERR_INVALID.
+ * den_prev may be NULL (out[4] is then 0).  Work is ordered on `stream`
+ * (a cudaStream_t, NULL = default stream) and the call synchronises it.
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls on a device share the array: calls that overlap on the GPU race
+ * and must be serialised by the caller. */
+int lbm_field_diagnostics_static(const float* den, const float* den_prev, const float* velx,
+                                 const float* vely, const float* velz, long long n,
+                                 double out[8], void* stream);
+
 /* Block until all work of the handle is done. */
 int lbm_sync(lbm_domain* d);
 

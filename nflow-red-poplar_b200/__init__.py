@@ -144,6 +144,7 @@ def lib():
         L.lbm_estimate_bytes.argtypes = [C.POINTER(Inputval), C.POINTER(Options),
                                          C.POINTER(C.c_size_t)]
         L.lbm_last_run_ms.argtypes = [vp, C.POINTER(C.c_float)]
+        L.lbm_field_diagnostics_static.argtypes = [vp, vp, vp, vp, vp, C.c_longlong, vp, vp]
         L.lbm_batch_default_options.argtypes = [C.POINTER(BatchOptions)]
         L.lbm_batch_create.argtypes = [C.POINTER(BatchOptions), C.POINTER(vp)]
         L.lbm_batch_destroy.argtypes = [vp]
