@@ -27,6 +27,8 @@ import subprocess
 import sys
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 BYTES = {"f32": 4, "f16_shift": 2, "bf16_shift": 2, "f64": 8}
 
@@ -227,6 +229,234 @@ def run_reference_arm(args, pkg, w):
     print(json.dumps(line), flush=True)
 
 
+# --------------------------------------------------------------------------
+# Further forms (run with --report): precision, batched
+# (configs[3]) and serving.  Each prints one JSON line.
+# --------------------------------------------------------------------------
+def _enstrophy(ux, uy, uz):
+    """0.5 * sum |curl u|^2 over the interior, central differences, FP64.
+    Arrays are [y][z][x]."""
+    ux, uy, uz = (np.asarray(a, np.float64) for a in (ux, uy, uz))
+
+    def d(a, axis):
+        return 0.5 * (np.roll(a, -1, axis) - np.roll(a, 1, axis))
+    wx = d(uz, 0) - d(uy, 1)   # dw/dy - dv/dz
+    wy = d(ux, 1) - d(uz, 2)   # du/dz - dw/dx
+    wz = d(uy, 2) - d(ux, 0)   # dv/dx - du/dy
+    w2 = (wx * wx + wy * wy + wz * wz)[1:-1, 1:-1, 1:-1]
+    return 0.5 * float(w2.sum())
+
+
+def report_precision(args, pkg):
+    """channel 512x128x128 MRT+LES, parabolic inlet u_max=0.05,
+    outlet rho=1, walls, 1 % seeded velocity perturbation, Re = u_max ny / nu
+    = 1000; the same run with FP16-shift, BF16-shift and FP32 storage against
+    the FP64 build."""
+    import torch
+    w = WORKLOADS["channel512x128x128_mrt_les"]
+    iv = make_case(pkg, w, args.size or None)
+    steps = args.steps
+    out = {"report": "precision", "workload": "channel512x128x128_mrt_les", "steps": steps,
+           "nx": iv.nx, "ny": iv.ny, "nz": iv.nz, "re": w["re_ch"], "tau": float(iv.m_dTau),
+           "data": "synthetic", "forms": {}}
+    kern = {"auto": pkg.KERNEL_AUTO, "scalar": pkg.KERNEL_SCALAR, "packed": pkg.KERNEL_PACKED,
+            "tma": pkg.KERNEL_TMA}[args.kernel]
+
+    def run(storage, kernel):
+        o = pkg.default_options(storage=storage, init_kind=w["init"], noise_amp=w["amp"], seed=1,
+                                kernel=kernel)
+        d = pkg.Domain(iv, o)
+        d.run(args.warmup)
+        d.sync()
+        t0 = time.perf_counter()
+        d.run(steps - args.warmup)
+        d.sync()
+        dt = time.perf_counter() - t0
+        den, ux, uy, uz = d.macroscopic()
+        diag = d.diagnostics()
+        d.close()
+        torch.cuda.synchronize()
+        return dict(den=den, ux=ux, uy=uy, uz=uz, ke=float(diag[5]),
+                    mlups=iv.nx * iv.ny * iv.nz * (steps - args.warmup) / dt / 1e6,
+                    nonfinite=int(diag[7]))
+
+    ref = run(pkg.STORE_F64, pkg.KERNEL_SCALAR)
+    ens_ref = _enstrophy(ref["ux"], ref["uy"], ref["uz"])
+    umax = float(np.sqrt(ref["ux"].astype(np.float64) ** 2 + ref["uy"] ** 2 + ref["uz"] ** 2).max())
+    out["fp64"] = {"MLUPS": ref["mlups"], "kinetic_energy": ref["ke"], "enstrophy": ens_ref,
+                   "max_u": umax}
+    for name, st in (("f32", pkg.STORE_F32), ("f16_shift", pkg.STORE_F16_SHIFT),
+                     ("bf16_shift", pkg.STORE_BF16_SHIFT)):
+        r = run(st, kern)
+        du = max(float(np.abs(r[k].astype(np.float64) - ref[k]).max()) for k in ("ux", "uy", "uz"))
+        ens = _enstrophy(r["ux"], r["uy"], r["uz"])
+        out["forms"][name] = {
+            "MLUPS": r["mlups"],
+            "rho_max_abs_err": float(np.abs(r["den"].astype(np.float64) - ref["den"]).max()),
+            "u_max_err_rel_umax": du / umax,
+            "u_rms_err_rel_umax": float(np.sqrt(np.mean(
+                (r["ux"].astype(np.float64) - ref["ux"]) ** 2 +
+                (r["uy"].astype(np.float64) - ref["uy"]) ** 2 +
+                (r["uz"].astype(np.float64) - ref["uz"]) ** 2))) / umax,
+            "kinetic_energy_rel_err": abs(r["ke"] - ref["ke"]) / abs(ref["ke"]),
+            "enstrophy_rel_err": abs(ens - ens_ref) / abs(ens_ref),
+            "nonfinite_nodes": r["nonfinite"]}
+    f32 = out["forms"]["f32"]["MLUPS"]
+    for name in ("f16_shift", "bf16_shift"):
+        out["forms"][name]["speedup_vs_f32"] = out["forms"][name]["MLUPS"] / f32
+    print(json.dumps(out), flush=True)
+
+
+def _c4_domains(seed, n, storage):
+    """edge from {32,48,64,96,128}; 50 % cavities e^3 (lid 0.1),
+    50 % channels 4e x e x e (u_max 0.05); Re log-uniform in [100, 5000]
+    (nu = u e / Re, tau = 3 nu + 0.5); 50 % SRT, 50 % MRT+LES (Cs 0.1)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        e = int(rng.choice([32, 48, 64, 96, 128]))
+        cav = bool(rng.random() < 0.5)
+        re = float(np.exp(rng.uniform(np.log(100.0), np.log(5000.0))))
+        mrt = bool(rng.random() < 0.5)
+        out.append(dict(e=e, cavity=cav, re=re, mrt=mrt, storage=storage))
+    return out
+
+
+def _case_iv(pkg, c):
+    e = c["e"]
+    if c["cavity"]:
+        u = 0.1
+        tau = 3.0 * u * e / c["re"] + 0.5
+        return pkg.make_inputval(e, casetype=pkg.CAVITY, tau=tau, u=u, mrt=c["mrt"], les=c["mrt"],
+                                 cs=0.1, h=e), 1, 1e-6
+    u = 0.05
+    tau = 3.0 * u * e / c["re"] + 0.5
+    return (pkg.make_inputval(4 * e, e, e, casetype=pkg.CHANNEL, tau=tau, u=u, mrt=c["mrt"],
+                              les=c["mrt"], cs=0.1), pkg.INIT_CHANNEL, 0.01)
+
+
+def report_batch(args, pkg):
+    """256 independent domains in one persistent launch per step
+    (CUDA-graph chunks, autotuned launch shape) vs each domain launched
+    alone, for FP32 and FP16-shift storage."""
+    ndom = 256
+    res = {"report": "batch", "domains": ndom, "steps": args.steps, "data": "synthetic (seeded)",
+           "forms": {}}
+    for sname, st in (("f32", pkg.STORE_F32), ("f16_shift", pkg.STORE_F16_SHIFT)):
+        cases = _c4_domains(7, ndom, st)
+        ivs = [_case_iv(pkg, c) for c in cases]
+        opts = [pkg.default_options(storage=st, init_kind=k, noise_amp=a, seed=i + 1)
+                for i, (iv, k, a) in enumerate(ivs)]
+        need = sum(pkg.batch_domain_bytes(iv, o) for (iv, _, _), o in zip(ivs, opts))
+        b = pkg.Batch(hbm_budget=int(need * 1.02) + (64 << 20), chunk_steps=32)
+        t0 = time.perf_counter()
+        for (iv, _, _), o in zip(ivs, opts):
+            b.add(iv, o, 10 ** 9)
+        b.sync()
+        t_admit = time.perf_counter() - t0
+        cfg = b.autotune(trial_steps=32)
+        b.step(args.warmup)
+        b.sync()
+        b.step(args.steps)
+        ms, lups = b.last_step_ms()
+        nodes = sum(iv.nx * iv.ny * iv.nz for iv, _, _ in ivs)
+        batched = lups / (ms * args.steps / 1e3) / 1e6
+        nonfinite = 0
+        for i in list(b.ivs):
+            nonfinite += int(b.member(i).diagnostics()[7] > 0)
+        b.close()
+        # each domain alone (same kernels, one launch per step, graph chunks)
+        t_alone = 0.0
+        for (iv, _, _), o in zip(ivs, opts):
+            d = pkg.Domain(iv, o)
+            d.run(args.warmup)
+            d.run(args.steps)
+            t_alone += d.last_run_ms() * args.steps / 1e3
+            d.close()
+        alone = nodes * args.steps / t_alone / 1e6
+        bpl = 2 * 19 * BYTES[sname]
+        res["forms"][sname] = {"batched_MLUPS": batched, "alone_MLUPS": alone,
+                               "batched_over_alone": batched / alone, "nodes": nodes,
+                               "pool_GB": need / 1e9, "admit_s": t_admit, "autotuned": cfg,
+                               "batched_GB_s": batched * 1e6 * bpl / 1e9,
+                               "domains_nonfinite": nonfinite}
+    print(json.dumps(res), flush=True)
+
+
+def report_serving(args, pkg):
+    """seeded Poisson arrivals, cavity/channel solves with edge
+    32-192, steps U[500, 5000], Re log-U[100, 5000], FP16-shift or FP32 per
+    request (MRT+LES), admitted by an HBM budget and stepped by continuous
+    batching; time-to-solution (arrival -> result on the host) and service
+    time (admission -> result) over a bounded wall-clock window."""
+    rate = args.rate
+    window = args.window
+    budget = int(min(150e9, args.budget_gb * 1e9))
+    rng = np.random.default_rng(11)
+    nreq = 20000
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, nreq))
+    reqs = []
+    for i in range(nreq):
+        e = int(rng.integers(32, 193))
+        cav = bool(rng.random() < 0.5)
+        re = float(np.exp(rng.uniform(np.log(100.0), np.log(5000.0))))
+        steps = int(rng.integers(500, 5001))
+        st = pkg.STORE_F16_SHIFT if rng.random() < 0.5 else pkg.STORE_F32
+        reqs.append(dict(t=float(arrivals[i]), e=e, cavity=cav, re=re, steps=steps, storage=st))
+    b = pkg.Batch(hbm_budget=budget, chunk_steps=32)
+    queue, active, tts, service, done_lups = [], {}, [], [], 0
+    nxt = 0
+    t0 = time.perf_counter()
+    admitted = 0
+    while True:
+        now = time.perf_counter() - t0
+        if now > window:
+            break
+        while nxt < nreq and reqs[nxt]["t"] <= now:
+            queue.append(reqs[nxt])
+            nxt += 1
+        while queue:  # FIFO admission while the head fits the budget
+            r = queue[0]
+            iv, k, a = _case_iv(pkg, dict(e=r["e"], cavity=r["cavity"], re=r["re"], mrt=True))
+            o = pkg.default_options(storage=r["storage"], init_kind=k, noise_amp=a, seed=nxt + 1)
+            try:
+                i = b.add(iv, o, r["steps"])
+            except pkg.LbmError as ex:
+                if ex.code == pkg.LBM_ERR_BUDGET:
+                    break
+                raise
+            queue.pop(0)
+            active[i] = (r, time.perf_counter() - t0, iv.nx * iv.ny * iv.nz)
+            admitted += 1
+        if not active:
+            if nxt < nreq:
+                time.sleep(max(0.0, min(reqs[nxt]["t"] - now, window - now)))
+            continue
+        b.step(32)
+        for i in b.poll():
+            r, t_adm, nodes = active.pop(i)
+            den, ux, uy, uz = b.member(i).macroscopic()  # the result reaches the host
+            t_done = time.perf_counter() - t0
+            tts.append(t_done - r["t"])
+            service.append(t_done - t_adm)
+            done_lups += nodes * r["steps"]
+            b.remove(i)
+    elapsed = time.perf_counter() - t0
+    b.close()
+
+    def pct(v, p):
+        return float(np.percentile(v, p)) if v else None
+    print(json.dumps({
+        "report": "serving", "rate_req_s": rate, "window_s": window, "budget_GB": budget / 1e9,
+        "arrived": nxt, "admitted": admitted, "completed": len(tts), "queued_at_end": len(queue),
+        "tts_p50_s": pct(tts, 50), "tts_p99_s": pct(tts, 99),
+        "service_p50_s": pct(service, 50), "service_p99_s": pct(service, 99),
+        "completed_MLUPS": done_lups / elapsed / 1e6,
+        "offered_LUPS": float(np.mean([(r["e"] ** 3 if r["cavity"] else 4 * r["e"] ** 3) *
+                                       r["steps"] for r in reqs]) * rate),
+        "data": "synthetic (seeded Poisson stream)"}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -237,6 +467,10 @@ def main():
     ap.add_argument("--storage", default="f32", choices=["f32", "f16_shift", "bf16_shift", "f64"])
     ap.add_argument("--size", type=int, default=0, help="scale the workload to this nx (profiling)")
     ap.add_argument("--kernel", default="auto", choices=["auto", "scalar", "packed", "tma"])
+    ap.add_argument("--report", default="", choices=["", "precision", "batch", "serving"])
+    ap.add_argument("--rate", type=float, default=200.0, help="serving: arrivals per second")
+    ap.add_argument("--window", type=float, default=60.0, help="serving: wall-clock window (s)")
+    ap.add_argument("--budget-gb", type=float, default=150.0, help="serving: HBM budget")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip cpu baseline, e2e and storage forms (profiling runs)")
     args = ap.parse_args()
@@ -246,6 +480,10 @@ def main():
     w = WORKLOADS[args.workload]
     if args.impl == "reference":
         run_reference_arm(args, pkg, w)
+        return
+    if args.report:
+        {"precision": report_precision, "batch": report_batch,
+         "serving": report_serving}[args.report](args, pkg)
         return
 
     import torch
