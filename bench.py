@@ -77,6 +77,27 @@ def make_case(pkg, w, size=None):
     return iv
 
 
+def max_over_ranks(value, world):
+    """max of a float over all ranks (the timing rule: the slowest rank).
+
+    Uses the process group's backend: NCCL on a CUDA tensor for GPU runs,
+    gloo on a CPU tensor otherwise."""
+    if world <= 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(value)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_mlups(nodes_per_rank, steps, max_ms, world):
+    """Whole-job MLUPS of `world` independent replicas (weak scaling): all
+    lattice updates over the slowest rank's time."""
+    return world * nodes_per_rank * steps / (max_ms / 1e3) / 1e6
+
+
 def measured_peak():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -503,11 +524,7 @@ def main():
             dist.barrier()
 
     def allmax(v):
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks(v, world)
 
     storage_id = {"f32": pkg.STORE_F32, "f16_shift": pkg.STORE_F16_SHIFT,
                   "bf16_shift": pkg.STORE_BF16_SHIFT, "f64": pkg.STORE_F64}
@@ -550,7 +567,7 @@ def main():
     clocks = sampler.stop() if sampler is not None else None
     ms_max = allmax(ms)
     per_launch_ms = ms / args.steps
-    value = world * cells * args.steps / (ms_max / 1e3) / 1e6
+    value = aggregate_mlups(cells, args.steps, ms_max, world)
 
     peak, peak_kind = measured_peak()
     bpl = 2 * 19 * BYTES[args.storage]
