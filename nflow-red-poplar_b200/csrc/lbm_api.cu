@@ -289,6 +289,7 @@ int lbm_import_arF(lbm_domain* d, const float* arF, int padded) {
   const size_t bytes = (size_t)nodes * Q * sizeof(float);
   if ((rc = ensure_staging(d, bytes))) return rc;
   CK(cudaMemcpyAsync(d->staging, arF, bytes, cudaMemcpyHostToDevice, d->stream));
+  CK(cudaMemsetAsync(d->den[1], 0, (size_t)d->N * sizeof(float), d->stream));
   CK(cudaMemsetAsync(d->flag, 0, sizeof(int), d->stream));
   k_check_finite<<<4 * 148, 256, 0, d->stream>>>(d->staging, nodes * Q, d->flag);
   int hflag = 0;

@@ -106,9 +106,9 @@ inline int validate(const Inputval* in, const lbm_options* opt) {
     return set_error(LBM_ERR_INVALID, "ny and nz must be <= 65535");
   if (round_up(in->nx, 8) * (long long)in->ny * in->nz >= (1LL << 31) - 1024)
     return set_error(LBM_ERR_INVALID, "domain too large (px*ny*nz must be < 2^31)");
-  if (in->casetype != CAVITY && in->casetype != CHANNEL)
+  if (in->casetype != CAVITY && in->casetype != CHANNEL && in->casetype != POISEUILLE)
     return set_error(LBM_ERR_INVALID,
-                     "casetype %d not supported (CAVITY=1 and CHANNEL=2 are implemented)",
+                     "casetype %d not supported (POISEUILLE=0, CAVITY=1, CHANNEL=2)",
                      in->casetype);
   if (!(std::isfinite(in->m_dTau) && in->m_dTau > 0.0f))
     return set_error(LBM_ERR_INVALID, "relaxation time tau=%g must be positive", in->m_dTau);
@@ -197,6 +197,9 @@ StepArgs<S> make_args(const lbm_domain* d, const void* src, void* dst, long long
   a.scale = d->scale;
   a.inv_scale = d->inv_scale;
   a.inlet_u = d->inlet_u;
+  a.init_kind = d->opt.init_kind;
+  a.noise_amp = d->opt.noise_amp;
+  a.seed = d->opt.seed;
   a.prho_in = d->prho[(k + 1) & 1];  // (k-1)&1
   a.prho_out = d->prho[k & 1];
   a.pu_in = d->pu[(k + 1) & 1];
@@ -220,13 +223,15 @@ int with_model(const lbm_domain* d, F&& f) {
 template <class S, int COLL, bool LES>
 void launch_step(const lbm_domain* d, const StepArgs<S>& a, cudaStream_t st) {
   if constexpr (!std::is_same<S, double>::value) {
-    if (d->opt.kernel == LBM_KERNEL_PACKED) {
+    if (d->g.casetype == POISEUILLE) {
+      // struct geometry: the per-node kernel (its pull checks every donor)
+    } else if (d->opt.kernel == LBM_KERNEL_PACKED) {
       const int pairs = (d->g.nx + 1) / 2;
       const dim3 b(64, 1, 1), gr((pairs + 63) / 64, d->g.nz, d->g.ny);
       k_step2<S, COLL, LES><<<gr, b, 0, st>>>(a);
       return;
     }
-    if (d->opt.kernel == LBM_KERNEL_TMA && d->tmap_ok) {
+    else if (d->opt.kernel == LBM_KERNEL_TMA && d->tmap_ok) {
       using Cfg = TmaCfg<S>;
       const int which = (a.src == (const S*)d->lat[0]) ? 0 : 1;
       k_step_tma<S, COLL, LES><<<d->tma_grid, Cfg::THREADS, Cfg::SMEM, st>>>(a, d->tmap[which],
@@ -295,6 +300,7 @@ int domain_tensor_maps(lbm_domain* d, int sm_count) {
       if (per_sm < 1) return set_error(LBM_ERR_CUDA, "TMA kernel does not fit an SM");
       const long long ntiles = (long long)((d->g.nx + Cfg::TX - 1) / Cfg::TX) *
                                ((d->g.nz + Cfg::TZ - 1) / Cfg::TZ) * d->g.ny;
+      if (ntiles >= (1LL << 31)) return set_error(LBM_ERR_INVALID, "too many TMA tiles");
       d->tma_grid = (int)std::min<long long>(ntiles, (long long)per_sm * sm_count);
       return LBM_OK;
     });
@@ -444,6 +450,9 @@ inline InitParams init_params(const lbm_domain* d) {
 // collision into lat[0]) and reset the step state.
 inline int domain_launch_init(lbm_domain* d, cudaStream_t st) {
   const InitParams ip = init_params(d);
+  const size_t nb = (size_t)d->N * sizeof(float);
+  CK(cudaMemsetAsync(d->den[0], 0, nb, st));
+  CK(cudaMemsetAsync(d->den[1], 0, nb, st));
   int rc = with_storage(d->opt.storage, [&](auto tag) -> int {
     using S = typename decltype(tag)::type;
     return with_model<S>(d, [&](auto coll, auto les) -> int {

@@ -48,15 +48,21 @@ struct Geometry {
   int casetype;
 };
 
-// node type of keSetNodeType (kernel.cu:1061-1077) / the Initialize codelet
-// (lbm_codelets.cpp:183-201) for CAVITY; CHANNEL: inlet x=0, outlet
-// x=nx-1, the four side faces are fixed walls and override inlet/outlet.
+// node type of keSetNodeType (kernel.cu:1061-1097) / the Initialize codelet
+// (lbm_codelets.cpp:183-201): CAVITY walls and lid; POISEUILLE inlet x=0,
+// outlet x=nx-1, STRUCT outside the circle of radius 20 about (y,z)=(25,25);
+// CHANNEL: inlet x=0, outlet x=nx-1, the four side faces are fixed walls and
+// override inlet/outlet.
 __device__ __forceinline__ int node_type(const Geometry& g, int x, int y, int z) {
   int t = NODE_FLUID;
   if (g.casetype == CAVITY) {
     if (y == 0) t = NODE_FIXEDWALL;
     if (y == g.ny - 1) t = NODE_MOVINGWALL;
     if (x == 0 || x == g.nx - 1 || z == 0 || z == g.nz - 1) t = NODE_FIXEDWALL;
+  } else if (g.casetype == POISEUILLE) {
+    if (x == 0) t = NODE_INLET;
+    if (x == g.nx - 1) t = NODE_OUTLET;
+    if ((y - 25) * (y - 25) + (z - 25) * (z - 25) > 400) t = NODE_STRUCT;
   } else {  // CHANNEL
     if (x == 0) t = NODE_INLET;
     if (x == g.nx - 1) t = NODE_OUTLET;
@@ -103,6 +109,11 @@ struct StepArgs {
   float* ux_out;
   float* uy_out;
   float* uz_out;
+  // initial condition (POISEUILLE: populations no rule ever writes keep
+  // their initial value, as in the reference)
+  int init_kind;
+  float noise_amp;
+  unsigned long long seed;
 };
 
 template <class S>
@@ -128,9 +139,15 @@ __device__ __forceinline__ RealOf<S> boundary_value(const StepArgs<S>& a, int t,
   }
   const int yz = y * a.g.nz + z;
   if (t == NODE_INLET) {
-    // keBoundaryInlet: ftemp[d] - 6.0 w_d rho(x+1) (c_d . u_in), FP64 literal
-    const R uin = R(a.inlet_u[yz]);
-    const R eu = mul_rn(R(cx(d)), uin);
+    // keBoundaryInlet: ftemp[d] - 6.0 w_d rho(x+1) (c_d . u_in), FP64 literal;
+    // u_in = RefVel (POISEUILLE) or the parabolic profile (CHANNEL)
+    R eu;
+    if (a.g.casetype == CHANNEL) {
+      eu = mul_rn(R(cx(d)), R(a.inlet_u[yz]));
+    } else {
+      eu = add_rn(add_rn(mul_rn(R(cx(d)), a.ulx), mul_rn(R(cy(d)), a.uly)),
+                  mul_rn(R(cz(d)), a.ulz));
+    }
     const double v = (double)fo - 6.0 * (double)weight<R>(d) * (double)a.prho_in[yz] * (double)eu;
     return R(v);
   }
@@ -152,6 +169,90 @@ __device__ __forceinline__ RealOf<S> boundary_value(const StepArgs<S>& a, int t,
   return fo;  // no rule for this node type: plain bounce-back
 }
 
+__device__ __forceinline__ uint64_t splitmix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+// uniform in [-1, 1) from 24 hash bits; exact in double on any IEEE machine
+__device__ __forceinline__ double unit_noise(uint64_t seed, uint64_t node, uint64_t comp) {
+  const uint64_t r = splitmix64(seed * 0x9E3779B97F4A7C15ull + node * 4ull + comp);
+  return __dadd_rn(__dmul_rn(__dmul_rn((double)(r >> 40), 1.0 / 16777216.0), 2.0), -1.0);
+}
+
+// Initial density / velocity of a node (Initialize codelet,
+// lbm_codelets.cpp:207-235, plus the seeded perturbations of LBM_INIT_*).
+struct InitState {
+  float den, ux, uy, uz;
+};
+__device__ __forceinline__ InitState initial_state(const Geometry& g, int kind, uint64_t seed,
+                                                   float amp, float rho0, float ulx, float uly,
+                                                   float ulz, const float* inlet_u, int x, int y,
+                                                   int z, int t) {
+  const long long n = x + (long long)g.nx * (z + (long long)g.nz * y);
+  InitState s{rho0, 0.f, 0.f, 0.f};
+  if (t == NODE_MOVINGWALL) {
+    s.ux = ulx;
+    s.uy = uly;
+    s.uz = ulz;
+  }
+  // separately rounded products and sums (no FMA), as in the CPU oracle
+  if (kind == LBM_INIT_DENSITY_NOISE) {
+    s.den = (float)__dadd_rn((double)rho0, __dmul_rn((double)amp, unit_noise(seed, (uint64_t)n, 0)));
+  } else if (kind == LBM_INIT_CHANNEL &&
+             (t == NODE_FLUID || t == NODE_INLET || t == NODE_OUTLET)) {
+    const double au = __dmul_rn((double)amp, (double)ulx);
+    const float prof = g.casetype == CHANNEL ? inlet_u[y * g.nz + z] : 0.0f;
+    s.ux = (float)__dadd_rn((double)prof, __dmul_rn(au, unit_noise(seed, (uint64_t)n, 0)));
+    s.uy = (float)__dmul_rn(au, unit_noise(seed, (uint64_t)n, 1));
+    s.uz = (float)__dmul_rn(au, unit_noise(seed, (uint64_t)n, 2));
+  }
+  return s;
+}
+
+// feq of lbm_codelets.cpp:225-230 in the codelet's rounding order
+template <class R, int q>
+__device__ __forceinline__ R initial_feq(R rd, R ux, R uy, R uz) {
+  const R eu = add_rn(add_rn(mul_rn(R(cx(q)), ux), mul_rn(R(cy(q)), uy)), mul_rn(R(cz(q)), uz));
+  const R usq = add_rn(add_rn(mul_rn(ux, ux), mul_rn(uy, uy)), mul_rn(uz, uz));
+  const R br = sub_rn(add_rn(add_rn(R(1), mul_rn(R(3), eu)), mul_rn(mul_rn(R(4.5), eu), eu)),
+                      mul_rn(R(1.5), usq));
+  return mul_rn(mul_rn(weight<R>(q), rd), br);
+}
+
+// POISEUILLE streaming + boundaries (kernel.cu:489-516, 659-697, 566-657):
+// a donor that is STRUCT does not stream (keStreaming skips it); a FLUID node
+// takes half-way bounce-back from its own f*_{opp q} (keBoundaryStruct);
+// inlet/outlet nodes apply their rule to donors outside the domain; every
+// other population is never written in the reference and keeps its
+// initial value.
+template <class S>
+__device__ __forceinline__ void pull_struct(RealOf<S> (&f)[Q], const StepArgs<S>& a, int x, int y,
+                                            int z, int cell) {
+  using R = RealOf<S>;
+  const int t = node_type(a.g, x, y, z);
+  const InitState is = initial_state(a.g, a.init_kind, a.seed, a.noise_amp, (float)a.rho0,
+                                     (float)a.ulx, (float)a.uly, (float)a.ulz, a.inlet_u, x, y,
+                                     z, t);
+  static_for<0, Q>([&](auto qc) {
+    constexpr int q = decltype(qc)::value;
+    const int xs = x - cx(q), ys = y - cy(q), zs = z - cz(q);
+    const bool inside = (unsigned)xs < (unsigned)a.g.nx && (unsigned)ys < (unsigned)a.g.ny &&
+                        (unsigned)zs < (unsigned)a.g.nz;
+    if (inside && node_type(a.g, xs, ys, zs) != NODE_STRUCT) {
+      f[q] = ld(a.srcq[q] + (cell - a.off[q]), q, a.inv_scale);
+    } else if (inside && t == NODE_FLUID) {
+      f[q] = ld(a.srcq[opp(q)] + cell, opp(q), a.inv_scale);
+    } else if (!inside && (t == NODE_INLET || t == NODE_OUTLET)) {
+      const R fo = ld(a.srcq[opp(q)] + cell, opp(q), a.inv_scale);
+      f[q] = boundary_value<S, q>(a, t, fo, y, z);
+    } else {
+      f[q] = initial_feq<R, q>(R(is.den), R(is.ux), R(is.uy), R(is.uz));
+    }
+  });
+}
+
 // Steps 1-2: the post-stream, post-boundary populations f_k at (x,y,z);
 // cell is the node's in-plane index.
 template <class S>
@@ -159,7 +260,9 @@ __device__ __forceinline__ void pull(RealOf<S> (&f)[Q], const StepArgs<S>& a, in
                                      int cell) {
   const bool edge = (x == 0) | (x == a.g.nx - 1) | (y == 0) | (y == a.g.ny - 1) | (z == 0) |
                     (z == a.g.nz - 1);
-  if (!edge) {
+  if (a.g.casetype == POISEUILLE) {
+    pull_struct<S>(f, a, x, y, z, cell);
+  } else if (!edge) {
     static_for<0, Q>([&](auto qc) {
       constexpr int q = decltype(qc)::value;
       f[q] = ld(a.srcq[q] + (cell - a.off[q]), q, a.inv_scale);
@@ -222,7 +325,7 @@ __device__ __forceinline__ void write_macro(const StepArgs<S>& a, int x, int y, 
     a.uy_out[n] = (float)uy;
     a.uz_out[n] = (float)uz;
   }
-  if (a.g.casetype == CHANNEL) {
+  if (a.g.casetype == CHANNEL || a.g.casetype == POISEUILLE) {
     const int P = a.g.ny * a.g.nz, yz = y * a.g.nz + z;
     if (x == 1) a.prho_out[yz] = (float)rho;
     if (x == a.g.nx - 1) {
@@ -265,6 +368,9 @@ struct StoreNode {
 template <class S, int COLL, bool LES>
 __device__ __forceinline__ void step_node(const StepArgs<S>& a, int x, int y, int z) {
   using R = RealOf<S>;
+  // STRUCT nodes are never streamed, collided or measured (kernel.cu:294,
+  // 323, 362, 464, 495, 1105)
+  if (a.g.casetype == POISEUILLE && node_type(a.g, x, y, z) == NODE_STRUCT) return;
   const int cell = x + a.g.px * (z + a.g.nz * y);
   R f[Q];
   pull<S>(f, a, x, y, z, cell);
@@ -301,18 +407,6 @@ struct InitParams {
   float rho0, ulx, uly, ulz;  // RefDen, RefVel*
 };
 
-__device__ __forceinline__ uint64_t splitmix64(uint64_t z) {
-  z += 0x9E3779B97F4A7C15ull;
-  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-  return z ^ (z >> 31);
-}
-// uniform in [-1, 1) from 24 hash bits; exact in double on any IEEE machine
-__device__ __forceinline__ double unit_noise(uint64_t seed, uint64_t node, uint64_t comp) {
-  const uint64_t r = splitmix64(seed * 0x9E3779B97F4A7C15ull + node * 4ull + comp);
-  return __dadd_rn(__dmul_rn(__dmul_rn((double)(r >> 40), 1.0 / 16777216.0), 2.0), -1.0);
-}
-
 template <class S, int COLL, bool LES>
 __global__ void __launch_bounds__(128)
     k_init(const __grid_constant__ StepArgs<S> a, S* __restrict__ collided, InitParams ip) {
@@ -321,36 +415,21 @@ __global__ void __launch_bounds__(128)
   const int z = blockIdx.y, y = blockIdx.z;
   if (x >= a.g.nx) return;
   const long long cell = x + (long long)a.g.px * (z + (long long)a.g.nz * y);
-  const long long n = x + (long long)a.g.nx * (z + (long long)a.g.nz * y);
   const int t = node_type(a.g, x, y, z);
-  float den = ip.rho0, velx = 0.f, vely = 0.f, velz = 0.f;
-  if (t == NODE_MOVINGWALL) {
-    velx = ip.ulx;
-    vely = ip.uly;
-    velz = ip.ulz;
-  }
-  // separately rounded products and sums (no FMA), as in the CPU oracle
-  if (ip.kind == LBM_INIT_DENSITY_NOISE) {
-    den = (float)__dadd_rn((double)ip.rho0,
-                           __dmul_rn((double)ip.noise_amp, unit_noise(ip.seed, (uint64_t)n, 0)));
-  } else if (ip.kind == LBM_INIT_CHANNEL &&
-             (t == NODE_FLUID || t == NODE_INLET || t == NODE_OUTLET)) {
-    const double au = __dmul_rn((double)ip.noise_amp, (double)ip.ulx);
-    const float prof = a.g.casetype == CHANNEL ? a.inlet_u[y * a.g.nz + z] : 0.0f;
-    velx = (float)__dadd_rn((double)prof, __dmul_rn(au, unit_noise(ip.seed, (uint64_t)n, 0)));
-    vely = (float)__dmul_rn(au, unit_noise(ip.seed, (uint64_t)n, 1));
-    velz = (float)__dmul_rn(au, unit_noise(ip.seed, (uint64_t)n, 2));
-  }
   R f[Q];
-  const R rd = R(den), ux = R(velx), uy = R(vely), uz = R(velz);
-  // feq of lbm_codelets.cpp:225-230, in the codelet's rounding order
+  if (t == NODE_STRUCT) {
+    // keInitialize leaves STRUCT nodes at the zeros of cudaMemset
+    static_for<0, Q>([&](auto qc) { f[decltype(qc)::value] = R(0); });
+    store_all<S>(a, f, cell);
+    write_macro<S>(a, x, y, z, R(0), R(0), R(0), R(0));
+    return;
+  }
+  const InitState is = initial_state(a.g, ip.kind, ip.seed, ip.noise_amp, ip.rho0, ip.ulx, ip.uly,
+                                     ip.ulz, a.inlet_u, x, y, z, t);
+  const R rd = R(is.den), ux = R(is.ux), uy = R(is.uy), uz = R(is.uz);
   static_for<0, Q>([&](auto qc) {
     constexpr int q = decltype(qc)::value;
-    const R eu = add_rn(add_rn(mul_rn(R(cx(q)), ux), mul_rn(R(cy(q)), uy)), mul_rn(R(cz(q)), uz));
-    const R usq = add_rn(add_rn(mul_rn(ux, ux), mul_rn(uy, uy)), mul_rn(uz, uz));
-    const R br = sub_rn(add_rn(add_rn(R(1), mul_rn(R(3), eu)), mul_rn(mul_rn(R(4.5), eu), eu)),
-                        mul_rn(R(1.5), usq));
-    f[q] = mul_rn(mul_rn(weight<R>(q), rd), br);
+    f[q] = initial_feq<R, q>(rd, ux, uy, uz);
   });
   store_all<S>(a, f, cell);  // post-stream lattice
   write_macro<S>(a, x, y, z, rd, ux, uy, uz);
@@ -395,6 +474,10 @@ __global__ void __launch_bounds__(128)
     constexpr int q = decltype(qc)::value;
     f[q] = ld(a.dst + q * a.qs + cell, q, a.inv_scale);
   });
+  if (a.g.casetype == POISEUILLE && node_type(a.g, x, y, z) == NODE_STRUCT) {
+    write_macro<S>(a, x, y, z, R(0), R(0), R(0), R(0));
+    return;
+  }
   R rho, ux, uy, uz;
   macroscopic<R>(f, rho, ux, uy, uz);  // CurrDen / CurrVel in the codelet's order
   write_macro<S>(a, x, y, z, rho, ux, uy, uz);
@@ -421,7 +504,9 @@ __global__ void __launch_bounds__(128)
   if (x >= a.g.nx) return;
   const long long cell = x + (long long)a.g.px * (z + (long long)a.g.nz * y);
   R f[Q];
-  if (post_direct) {
+  if (a.g.casetype == POISEUILLE && node_type(a.g, x, y, z) == NODE_STRUCT) {
+    static_for<0, Q>([&](auto qc) { f[decltype(qc)::value] = R(0); });
+  } else if (post_direct) {
     static_for<0, Q>([&](auto qc) {
       constexpr int q = decltype(qc)::value;
       f[q] = ld(a.src + q * a.qs + cell, q, a.inv_scale);

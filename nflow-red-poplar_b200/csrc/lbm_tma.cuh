@@ -33,13 +33,13 @@ namespace lbm {
 template <class S>
 struct TmaCfg {
   static constexpr int TX = 128;                       // tile nodes along x
-  static constexpr int TZ = 4;                         // tile rows along z
+  static constexpr int TZ = 8;                         // tile rows along z
   static constexpr int HX = 16 / (int)sizeof(S);       // 16-byte x halo
   static constexpr int TXB = TX + 2 * HX;              // box width
   static constexpr int BOX_BYTES = TXB * TZ * (int)sizeof(S);
   static constexpr int BOX_STRIDE = (BOX_BYTES + 127) / 128 * 128;
   static constexpr int STAGE_BYTES = Q * BOX_STRIDE;
-  static constexpr int STAGES = sizeof(S) == 4 ? 3 : 4;
+  static constexpr int STAGES = sizeof(S) == 4 ? 2 : 4;
   static constexpr int CONSUMER_WARPS = TX / 2 * TZ / 32;  // one x-pair per thread
   static constexpr int THREADS = (CONSUMER_WARPS + 1) * 32;
   static constexpr int SMEM = STAGES * STAGE_BYTES + 2 * STAGES * 8 + 128;
@@ -47,7 +47,10 @@ struct TmaCfg {
   static_assert(TXB <= 256 && TZ <= 256, "TMA box dimension limit");
 };
 
-// bounded mbarrier waits: about a second of try_wait before giving up
+// bounded mbarrier waits: try_wait suspends the thread for up to
+// kSuspendNs per call (it returns as soon as the phase completes), and
+// kWaitIters calls bound a wait to about a second
+constexpr int kSuspendNs = 1000;
 constexpr int kWaitIters = 1 << 20;
 constexpr int kErrProducerWait = 1;
 constexpr int kErrConsumerWait = 2;
@@ -68,10 +71,10 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
 __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n"
       " selp.u32 %0, 1, 0, p;\n}\n"
       : "=r"(ok)
-      : "r"(bar), "r"(parity)
+      : "r"(bar), "r"(parity), "r"(kSuspendNs)
       : "memory");
   return ok != 0;
 }
@@ -123,7 +126,7 @@ __global__ void __launch_bounds__(TmaCfg<S>::THREADS, 1)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nx = a.g.nx, ny = a.g.ny, nz = a.g.nz;
   const int ntx = (nx + C::TX - 1) / C::TX, nzb = (nz + C::TZ - 1) / C::TZ;
-  const long long ntiles = (long long)ntx * nzb * ny;
+  const int ntiles = ntx * nzb * ny;  // < 2^31 (checked when the domain is created)
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < C::STAGES; ++s) {
@@ -139,17 +142,17 @@ __global__ void __launch_bounds__(TmaCfg<S>::THREADS, 1)
     // ---------------- producer: one elected lane ----------------
     if (lane != 0) return;
     int i = 0;
-    for (long long t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
       const int s = i % C::STAGES;
       const uint32_t ph = (uint32_t)(i / C::STAGES) & 1u;
       if (!mbar_wait(smem_addr(&empty[s]), ph ^ 1u)) {
         atomicExch(err, kErrProducerWait);
         break;
       }
-      const int xt = (int)(t % ntx);
-      const long long rest = t / ntx;
-      const int zb = (int)(rest % nzb);
-      const int y = (int)(rest / nzb);
+      const int xt = t % ntx;
+      const int rest = t / ntx;
+      const int zb = rest % nzb;
+      const int y = rest / nzb;
       const int x0 = xt * C::TX, z0 = zb * C::TZ;
       const uint32_t bar = smem_addr(&full[s]);
       mbar_expect_tx(bar, (uint32_t)(Q * C::BOX_BYTES));
@@ -167,17 +170,17 @@ __global__ void __launch_bounds__(TmaCfg<S>::THREADS, 1)
   const int r = threadIdx.x / (C::TX / 2);
   const int xl = 2 * (threadIdx.x % (C::TX / 2));
   int i = 0;
-  for (long long t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
     const int s = i % C::STAGES;
     const uint32_t ph = (uint32_t)(i / C::STAGES) & 1u;
     if (!mbar_wait(smem_addr(&full[s]), ph)) {
       atomicExch(err, kErrConsumerWait);
       return;
     }
-    const int xt = (int)(t % ntx);
-    const long long rest = t / ntx;
-    const int zb = (int)(rest % nzb);
-    const int y = (int)(rest / nzb);
+    const int xt = t % ntx;
+    const int rest = t / ntx;
+    const int zb = rest % nzb;
+    const int y = rest / nzb;
     const int x = xt * C::TX + xl, z = zb * C::TZ + r;
     if (x < nx && z < nz) {
       const bool two = x + 1 < nx;

@@ -127,7 +127,7 @@ def test_argument_errors_are_status_codes():
     assert b"NULL" in L.lbm_last_error()
     iv = pkg.make_inputval(2, 8, 8, tau=0.6)
     assert L.lbm_create(C.byref(iv), None, C.byref(h)) == pkg.LBM_ERR_INVALID
-    iv = pkg.make_inputval(8, tau=0.6, casetype=pkg.POISEUILLE)
+    iv = pkg.make_inputval(8, tau=0.6, casetype=7)
     assert L.lbm_create(C.byref(iv), None, C.byref(h)) == pkg.LBM_ERR_INVALID
     iv = pkg.make_inputval(8, tau=float("nan"))
     assert L.lbm_create(C.byref(iv), None, C.byref(h)) == pkg.LBM_ERR_INVALID
