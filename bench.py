@@ -383,16 +383,23 @@ def report_batch(args, pkg):
         nodes = sum(iv.nx * iv.ny * iv.nz for iv, _, _ in ivs)
         batched = lups / (ms * args.steps / 1e3) / 1e6
         nonfinite = 0
+        steps_done = []
         for i in list(b.ivs):
-            nonfinite += int(b.member(i).diagnostics()[7] > 0)
+            m = b.member(i)
+            nonfinite += int(m.diagnostics()[7] > 0)
+            steps_done.append(m.steps())
         b.close()
         # each domain alone (same kernels, one launch per step, graph chunks)
         t_alone = 0.0
-        for (iv, _, _), o in zip(ivs, opts):
+        nonfinite_alone = 0
+        for ((iv, _, _), o), sd in zip(zip(ivs, opts), steps_done):
             d = pkg.Domain(iv, o)
             d.run(args.warmup)
             d.run(args.steps)
             t_alone += d.last_run_ms() * args.steps / 1e3
+            # the same step count as in the batch (autotuner trials included)
+            d.run(max(0, sd - args.warmup - args.steps))
+            nonfinite_alone += int(d.diagnostics()[7] > 0)
             d.close()
         alone = nodes * args.steps / t_alone / 1e6
         bpl = 2 * 19 * BYTES[sname]
@@ -400,7 +407,8 @@ def report_batch(args, pkg):
                                "batched_over_alone": batched / alone, "nodes": nodes,
                                "pool_GB": need / 1e9, "admit_s": t_admit, "autotuned": cfg,
                                "batched_GB_s": batched * 1e6 * bpl / 1e9,
-                               "domains_nonfinite": nonfinite}
+                               "domains_nonfinite": nonfinite,
+                               "domains_nonfinite_alone": nonfinite_alone}
     print(json.dumps(res), flush=True)
 
 
@@ -427,8 +435,13 @@ def report_serving(args, pkg):
     b = pkg.Batch(hbm_budget=budget, chunk_steps=32)
     queue, active, tts, service, done_lups = [], {}, [], [], 0
     nxt = 0
-    t0 = time.perf_counter()
     admitted = 0
+    executed = 0   # lattice updates issued to the GPU in the window
+    # admission stops while the resident backlog (remaining lattice updates)
+    # exceeds horizon seconds at the nominal rate: requests then finish in
+    # about their own share instead of all sharing the GPU until the end
+    backlog_cap = args.horizon * args.nominal_mlups * 1e6 if args.horizon > 0 else float("inf")
+    t0 = time.perf_counter()
     while True:
         now = time.perf_counter() - t0
         if now > window:
@@ -436,7 +449,8 @@ def report_serving(args, pkg):
         while nxt < nreq and reqs[nxt]["t"] <= now:
             queue.append(reqs[nxt])
             nxt += 1
-        while queue:  # FIFO admission while the head fits the budget
+        backlog = sum(n * left for (_, _, n, left) in active.values())
+        while queue and backlog < backlog_cap:  # FIFO while the head fits the budget
             r = queue[0]
             iv, k, a = _case_iv(pkg, dict(e=r["e"], cavity=r["cavity"], re=r["re"], mrt=True))
             o = pkg.default_options(storage=r["storage"], init_kind=k, noise_amp=a, seed=nxt + 1)
@@ -447,15 +461,21 @@ def report_serving(args, pkg):
                     break
                 raise
             queue.pop(0)
-            active[i] = (r, time.perf_counter() - t0, iv.nx * iv.ny * iv.nz)
+            nodes = iv.nx * iv.ny * iv.nz
+            active[i] = [r, time.perf_counter() - t0, nodes, r["steps"]]
+            backlog += nodes * r["steps"]
             admitted += 1
         if not active:
             if nxt < nreq:
                 time.sleep(max(0.0, min(reqs[nxt]["t"] - now, window - now)))
             continue
         b.step(32)
+        for v in active.values():
+            took = min(32, v[3])
+            executed += v[2] * took
+            v[3] -= took
         for i in b.poll():
-            r, t_adm, nodes = active.pop(i)
+            r, t_adm, nodes, _ = active.pop(i)
             den, ux, uy, uz = b.member(i).macroscopic()  # the result reaches the host
             t_done = time.perf_counter() - t0
             tts.append(t_done - r["t"])
@@ -473,6 +493,9 @@ def report_serving(args, pkg):
         "tts_p50_s": pct(tts, 50), "tts_p99_s": pct(tts, 99),
         "service_p50_s": pct(service, 50), "service_p99_s": pct(service, 99),
         "completed_MLUPS": done_lups / elapsed / 1e6,
+        "aggregate_MLUPS": executed / elapsed / 1e6,
+        "admission": {"hbm_budget_GB": budget / 1e9, "backlog_horizon_s": args.horizon,
+                      "nominal_MLUPS": args.nominal_mlups},
         "offered_LUPS": float(np.mean([(r["e"] ** 3 if r["cavity"] else 4 * r["e"] ** 3) *
                                        r["steps"] for r in reqs]) * rate),
         "data": "synthetic (seeded Poisson stream)"}), flush=True)
@@ -492,6 +515,11 @@ def main():
     ap.add_argument("--rate", type=float, default=200.0, help="serving: arrivals per second")
     ap.add_argument("--window", type=float, default=60.0, help="serving: wall-clock window (s)")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="serving: HBM budget")
+    ap.add_argument("--horizon", type=float, default=4.0,
+                    help="serving: admit while the resident backlog is below this many seconds "
+                         "of work at --nominal-mlups (0 = HBM budget only)")
+    ap.add_argument("--nominal-mlups", type=float, default=30000.0,
+                    help="serving: throughput the backlog horizon is converted with")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip cpu baseline, e2e and storage forms (profiling runs)")
     args = ap.parse_args()

@@ -345,7 +345,10 @@ typedef struct lbm_batch_options {
   int block;              /* threads per CTA (128 or 256), 0 = autotuned/256  */
   int nodes_per_thread;   /* nodes per thread per tile (1, 2, 4), 0 = 2       */
   int ctas_per_sm;        /* persistent CTAs per SM, 0 = max resident         */
-  int reserved[8];
+  int schedule;           /* 0: each CTA a contiguous range of tiles,
+                             1: grid-stride over the tile list                */
+  int regs;               /* kernel build: 0 = 64 registers, 1 = 80           */
+  int reserved[6];
 } lbm_batch_options;
 
 void lbm_batch_default_options(lbm_batch_options* bo);

@@ -70,7 +70,7 @@ class BatchOptions(C.Structure):
     _fields_ = [
         ("device", C.c_int), ("hbm_budget", C.c_size_t), ("chunk_steps", C.c_int),
         ("block", C.c_int), ("nodes_per_thread", C.c_int), ("ctas_per_sm", C.c_int),
-        ("reserved", C.c_int * 8),
+        ("schedule", C.c_int), ("regs", C.c_int), ("reserved", C.c_int * 6),
     ]
 
 
@@ -318,7 +318,7 @@ class Batch:
     """Many resident domains stepped together (continuous batching)."""
 
     def __init__(self, hbm_budget=1 << 30, device=0, chunk_steps=32, block=0,
-                 nodes_per_thread=0, ctas_per_sm=0):
+                 nodes_per_thread=0, ctas_per_sm=0, schedule=0, regs=0):
         o = BatchOptions()
         lib().lbm_batch_default_options(C.byref(o))
         o.device, o.hbm_budget, o.chunk_steps = device, hbm_budget, chunk_steps
@@ -327,6 +327,7 @@ class Batch:
         if nodes_per_thread:
             o.nodes_per_thread = nodes_per_thread
         o.ctas_per_sm = ctas_per_sm
+        o.schedule, o.regs = schedule, regs
         h = C.c_void_p()
         check(lib().lbm_batch_create(C.byref(o), C.byref(h)))
         self.h = h
@@ -380,7 +381,8 @@ class Batch:
     def autotune(self, trial_steps=32):
         o = BatchOptions()
         check(lib().lbm_batch_autotune(self.h, int(trial_steps), C.byref(o)))
-        return dict(block=o.block, nodes_per_thread=o.nodes_per_thread, ctas_per_sm=o.ctas_per_sm)
+        return dict(block=o.block, nodes_per_thread=o.nodes_per_thread, ctas_per_sm=o.ctas_per_sm,
+                    schedule=o.schedule, regs=o.regs)
 
     def last_step_ms(self):
         ms, lups = C.c_float(), C.c_longlong()

@@ -26,7 +26,7 @@ using namespace lbm;
 
 namespace {
 
-constexpr int kArgsBytes = 768;  // one StepArgs<S> image, 16-byte multiple
+constexpr int kArgsBytes = 1024;  // one StepArgs<S> image, 16-byte multiple
 static_assert(sizeof(StepArgs<float>) <= kArgsBytes, "StepArgs too large");
 static_assert(sizeof(StepArgs<__half>) <= kArgsBytes, "StepArgs too large");
 static_assert(sizeof(StepArgs<__nv_bfloat16>) <= kArgsBytes, "StepArgs too large");
@@ -36,21 +36,34 @@ constexpr int kImages = 6;
 
 // per active domain, per chunk
 struct SlotMeta {
-  int variant;       // storage*4 + model (model: 0 SRT, 1 SRT+LES, 2 MRT, 3 MRT+LES)
   int image_base;    // index of the domain's first argument image
   int nx, nz;
+  int active;        // steps the domain takes in this chunk
   unsigned long long mnx, mnz;  // ceil(2^64 / n): exact 32-bit division
   long long nodes;
-  int active;        // steps the domain takes in this chunk
   int cur0;          // lattice holding f* at chunk start
+  int pad;
+};
+
+// model: 0 SRT, 1 SRT+LES, 2 MRT, 3 MRT+LES; variant = storage * 4 + model
+constexpr int kVariants = 12;
+
+// The domains of one variant: meta[slot0 .. slot0 + nslots) and their tile
+// prefix sums tile_off[off0 .. off0 + nslots] (tiles of the variant's list).
+struct VariantList {
+  int nslots;
+  int slot0;
+  int off0;
+  int pad;
+  long long ntiles;
 };
 
 struct BatchTables {
-  int nslots;
   int tile;          // nodes per tile = block * npt
-  long long ntiles;
+  int schedule;      // 0: contiguous tile range per CTA, 1: grid-stride
+  VariantList v[kVariants];
   const SlotMeta* meta;
-  const long long* tile_off;     // [nslots + 1]
+  const long long* tile_off;
   const unsigned char* images;   // [capacity * kImages][kArgsBytes]
 };
 
@@ -58,65 +71,125 @@ __device__ __forceinline__ unsigned fastdiv(unsigned n, unsigned long long m) {
   return (unsigned)__umul64hi(m, (unsigned long long)n);
 }
 
-template <class S, int COLL, bool LES>
-__device__ __forceinline__ void batch_node(const unsigned char* img, int x, int y, int z) {
-  step_node<S, COLL, LES>(*reinterpret_cast<const StepArgs<S>*>(img), x, y, z);
-}
+template <class S> struct StorageIndex;
+template <> struct StorageIndex<float> { static constexpr int value = 0; };
+template <> struct StorageIndex<__half> { static constexpr int value = 1; };
+template <> struct StorageIndex<__nv_bfloat16> { static constexpr int value = 2; };
 
-template <class S>
-__device__ __forceinline__ void batch_model(int model, const unsigned char* img, int x, int y,
-                                            int z) {
-  switch (model) {
-    case 0: batch_node<S, COLL_SRT, false>(img, x, y, z); break;
-    case 1: batch_node<S, COLL_SRT, true>(img, x, y, z); break;
-    case 2: batch_node<S, COLL_MRT, false>(img, x, y, z); break;
-    default: batch_node<S, COLL_MRT, true>(img, x, y, z); break;
+// the nodes of local tile lt of the domain described by m
+template <class S, int COLL, bool LES>
+__device__ __forceinline__ void batch_tile(const StepArgs<S>& a, const SlotMeta& m, long long lt,
+                                           int tile, int npt) {
+  const unsigned base = (unsigned)(lt * tile);
+  const unsigned nodes = (unsigned)m.nodes;
+  for (int i = 0; i < npt; ++i) {
+    const unsigned n = base + (unsigned)i * blockDim.x + threadIdx.x;
+    if (n >= nodes) break;
+    const unsigned r = fastdiv(n, m.mnx);
+    const int x = (int)(n - r * (unsigned)m.nx);
+    const unsigned y = fastdiv(r, m.mnz);
+    const int z = (int)(r - y * (unsigned)m.nz);
+    step_node<S, COLL, LES, IndexAddr>(a, x, (int)y, z);
   }
 }
 
-// One time step of every active domain (launch j of a chunk).
-__global__ void __launch_bounds__(256) k_batch_step(const BatchTables* __restrict__ tab, int j,
-                                                    int npt) {
+// Make slot s (meta and argument image for launch j) the CTA's current
+// domain in shared memory; returns false when the domain takes no step j.
+// All threads of the CTA take the same path.
+__device__ __forceinline__ bool enter_slot(SlotMeta& sm, unsigned char* img,
+                                           const SlotMeta* __restrict__ meta,
+                                           const unsigned char* images, int s, int j, int& cached) {
+  const int active = meta[s].active;
+  if (j >= active) return false;
+  const int image = meta[s].image_base + ((meta[s].cur0 + j) & 1) * 3 +
+                    (j >= active - 1 ? 2 : (j >= active - 2 ? 1 : 0));
+  if (image == cached) return true;
+  __syncthreads();
+  const int4* src = reinterpret_cast<const int4*>(images + (size_t)image * kArgsBytes);
+  int4* dst = reinterpret_cast<int4*>(img);
+  for (int i = threadIdx.x; i < kArgsBytes / 16; i += blockDim.x) dst[i] = src[i];
+  if (threadIdx.x == 0) sm = meta[s];
+  __syncthreads();
+  cached = image;
+  return true;
+}
+
+// One time step (launch j of a chunk) of every active domain of one variant.
+// Schedule 0 gives CTA c the contiguous tiles [c*per, (c+1)*per) of the
+// variant's list, so a CTA looks its domain up once and reloads arguments
+// only where its range crosses into the next domain; schedule 1 walks
+// t = blockIdx.x, += gridDim.x and advances the domain cursor monotonically.
+// The domain's arguments and meta stay in shared memory (uniform over the
+// CTA).  MINB (resident 256-thread CTAs the register budget must allow: 4 ->
+// 64 registers, 3 -> 80) trades spills of the uniform arguments against
+// occupancy; the autotuner picks it.
+template <class S, int COLL, bool LES, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_batch_step(const BatchTables* __restrict__ tab,
+                                                          int j, int npt) {
+  constexpr int V = StorageIndex<S>::value * 4 + (COLL == COLL_MRT ? 2 : 0) + (LES ? 1 : 0);
   __shared__ __align__(16) unsigned char img[kArgsBytes];
-  const BatchTables T = *tab;
+  __shared__ SlotMeta sm;
+  const StepArgs<S>& a = *reinterpret_cast<const StepArgs<S>*>(img);
+  const VariantList L = tab->v[V];
+  if (L.nslots == 0 || L.ntiles == 0) return;
+  const int tile = tab->tile;
+  const SlotMeta* __restrict__ meta = tab->meta + L.slot0;
+  const long long* __restrict__ off = tab->tile_off + L.off0;
+  const unsigned char* images = tab->images;
   int cached = -1;
-  for (long long t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
-    int lo = 0, hi = T.nslots;  // tile_off[lo] <= t < tile_off[hi]
+  if (tab->schedule == 0) {
+    const long long per = (L.ntiles + gridDim.x - 1) / gridDim.x;
+    long long t = (long long)blockIdx.x * per;
+    const long long tend = min(t + per, L.ntiles);
+    if (t >= tend) return;
+    int lo = 0, hi = L.nslots;  // off[lo] <= t < off[hi]
     while (hi - lo > 1) {
       const int mid = (lo + hi) >> 1;
-      if (T.tile_off[mid] <= t)
+      if (off[mid] <= t)
         lo = mid;
       else
         hi = mid;
     }
-    const SlotMeta m = T.meta[lo];
-    if (j >= m.active) continue;  // uniform over the CTA
-    const int par = (m.cur0 + j) & 1;
-    const int kind = j >= m.active - 1 ? 2 : (j >= m.active - 2 ? 1 : 0);
-    const int image = m.image_base + par * 3 + kind;
-    if (image != cached) {
-      __syncthreads();
-      const int4* src = reinterpret_cast<const int4*>(T.images + (size_t)image * kArgsBytes);
-      int4* dst = reinterpret_cast<int4*>(img);
-      for (int i = threadIdx.x; i < kArgsBytes / 16; i += blockDim.x) dst[i] = src[i];
-      __syncthreads();
-      cached = image;
-    }
-    const long long base = (t - T.tile_off[lo]) * (long long)T.tile;
-    for (int i = 0; i < npt; ++i) {
-      const long long n = base + (long long)i * blockDim.x + threadIdx.x;
-      if (n >= m.nodes) break;
-      const unsigned r = fastdiv((unsigned)n, m.mnx);
-      const int x = (int)((unsigned)n - r * (unsigned)m.nx);
-      const unsigned y = fastdiv(r, m.mnz);
-      const int z = (int)(r - y * (unsigned)m.nz);
-      switch (m.variant >> 2) {
-        case 0: batch_model<float>(m.variant & 3, img, x, (int)y, z); break;
-        case 1: batch_model<__half>(m.variant & 3, img, x, (int)y, z); break;
-        default: batch_model<__nv_bfloat16>(m.variant & 3, img, x, (int)y, z); break;
+    for (int s = lo; t < tend; ++s) {
+      const long long s_begin = off[s], s_end = off[s + 1];
+      if (enter_slot(sm, img, meta, images, s, j, cached)) {
+        const long long stop = min(s_end, tend);
+        for (; t < stop; ++t) batch_tile<S, COLL, LES>(a, sm, t - s_begin, tile, npt);
       }
+      t = s_end;
+    }
+  } else {
+    int s = 0;
+    long long s_end = off[1];
+    for (long long t = blockIdx.x; t < L.ntiles; t += gridDim.x) {
+      while (t >= s_end) s_end = off[++s + 1];
+      if (!enter_slot(sm, img, meta, images, s, j, cached)) continue;
+      batch_tile<S, COLL, LES>(a, sm, t - off[s], tile, npt);
     }
   }
+}
+
+using BatchKernel = void (*)(const BatchTables*, int, int);
+
+template <class S, int MINB>
+constexpr BatchKernel batch_kernel_of(int model) {
+  return model == 0   ? k_batch_step<S, COLL_SRT, false, MINB>
+         : model == 1 ? k_batch_step<S, COLL_SRT, true, MINB>
+         : model == 2 ? k_batch_step<S, COLL_MRT, false, MINB>
+                      : k_batch_step<S, COLL_MRT, true, MINB>;
+}
+
+template <int MINB>
+BatchKernel batch_kernel_minb(int variant) {
+  const int st = variant >> 2, model = variant & 3;
+  return st == 0   ? batch_kernel_of<float, MINB>(model)
+         : st == 1 ? batch_kernel_of<__half, MINB>(model)
+                   : batch_kernel_of<__nv_bfloat16, MINB>(model);
+}
+
+// regs: 0 -> the 64-register build, 1 -> the 80-register build
+BatchKernel batch_kernel(int variant, int regs) {
+  return regs == 1 ? batch_kernel_minb<3>(variant) : batch_kernel_minb<4>(variant);
 }
 
 // First-fit device pool with coalescing (offsets 256-byte aligned).
@@ -218,7 +291,9 @@ struct lbm_batch {
   cudaEvent_t tables_free = nullptr;  // previous table upload has been consumed
   // chunk graph
   cudaGraphExec_t graph = nullptr;
-  int graph_block = 0, graph_grid = 0, graph_npt = 0, graph_steps = 0;
+  int graph_block = 0, graph_npt = 0, graph_steps = 0, graph_mask = -1, graph_sched = -1;
+  int graph_ctas = -1, graph_regs = -1;
+  int variant_mask = 0;           // variants with at least one unfinished member
   // completion tracking
   long long chunks_issued = 0;
   std::vector<std::pair<long long, cudaEvent_t>> chunk_events;
@@ -232,32 +307,58 @@ namespace {
 
 int chunk_steps(const lbm_batch* b) { return b->opt.chunk_steps > 0 ? b->opt.chunk_steps : 32; }
 
-int launch_shape(lbm_batch* b, int* block, int* grid, int* npt) {
-  *block = b->opt.block == 128 ? 128 : 256;
-  *npt = b->opt.nodes_per_thread > 0 ? b->opt.nodes_per_thread : 2;
+int launch_block(const lbm_batch* b) { return b->opt.block == 128 ? 128 : 256; }
+int launch_npt(const lbm_batch* b) {
+  return b->opt.nodes_per_thread > 0 ? b->opt.nodes_per_thread : 2;
+}
+
+// persistent grid of one variant's kernel: resident CTAs per SM x SMs
+int launch_grid(lbm_batch* b, int variant, int block, int* grid) {
   int per_sm = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_step, *block, 0));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel(variant, b->opt.regs),
+                                                   block, 0));
   if (per_sm < 1) per_sm = 1;
   if (b->opt.ctas_per_sm > 0 && b->opt.ctas_per_sm < per_sm) per_sm = b->opt.ctas_per_sm;
   *grid = per_sm * b->sm_count;
   return LBM_OK;
 }
 
-// (Re)capture the chunk graph for the current launch shape.
-int ensure_graph(lbm_batch* b) {
-  int block, grid, npt;
-  int rc = launch_shape(b, &block, &grid, &npt);
-  if (rc) return rc;
-  const int steps = chunk_steps(b);
-  if (b->graph && b->graph_block == block && b->graph_grid == grid && b->graph_npt == npt &&
-      b->graph_steps == steps)
+int member_variant(const lbm_domain* d) {
+  return storage_index(d->opt.storage) * 4 + model_of(d->in);
+}
+
+// Variants with a member that still has steps to take.
+int pending_mask(const lbm_batch* b) {
+  int mask = 0;
+  for (auto& kv : b->members)
+    if (kv.second.issued < kv.second.target) mask |= 1 << member_variant(kv.second.d);
+  return mask;
+}
+
+// (Re)capture the chunk graph: chunk_steps steps, each one launch per
+// variant in the mask, for the current launch shape.
+int ensure_graph(lbm_batch* b, int mask) {
+  const int block = launch_block(b), npt = launch_npt(b), steps = chunk_steps(b);
+  const int sched = b->opt.schedule == 1 ? 1 : 0;
+  if (b->graph && b->graph_block == block && b->graph_npt == npt && b->graph_steps == steps &&
+      b->graph_mask == mask && b->graph_sched == sched && b->graph_ctas == b->opt.ctas_per_sm &&
+      b->graph_regs == b->opt.regs)
     return LBM_OK;
   if (b->graph) {
     cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;
   }
+  int grids[kVariants] = {0};
+  for (int v = 0; v < kVariants; ++v)
+    if (mask & (1 << v)) {
+      int rc = launch_grid(b, v, block, &grids[v]);
+      if (rc) return rc;
+    }
   CK(cudaStreamBeginCapture(b->capture, cudaStreamCaptureModeThreadLocal));
-  for (int j = 0; j < steps; ++j) k_batch_step<<<grid, block, 0, b->capture>>>(b->d_tab, j, npt);
+  for (int j = 0; j < steps; ++j)
+    for (int v = 0; v < kVariants; ++v)
+      if (mask & (1 << v))
+        batch_kernel(v, b->opt.regs)<<<grids[v], block, 0, b->capture>>>(b->d_tab, j, npt);
   cudaGraph_t g;
   CK(cudaStreamEndCapture(b->capture, &g));
   cudaError_t e = cudaGraphInstantiate(&b->graph, g, 0);
@@ -265,9 +366,12 @@ int ensure_graph(lbm_batch* b) {
   if (e != cudaSuccess)
     return set_error(LBM_ERR_CUDA, "batch graph instantiation failed: %s", cudaGetErrorString(e));
   b->graph_block = block;
-  b->graph_grid = grid;
   b->graph_npt = npt;
   b->graph_steps = steps;
+  b->graph_mask = mask;
+  b->graph_sched = sched;
+  b->graph_ctas = b->opt.ctas_per_sm;
+  b->graph_regs = b->opt.regs;
   return LBM_OK;
 }
 
@@ -309,9 +413,9 @@ int grow_images(lbm_batch* b) {
   long long *doff = nullptr, *hoff = nullptr;
   CK(cudaMalloc(&nimg, (size_t)cap * kImages * kArgsBytes));
   CK(cudaMalloc(&dm, (size_t)cap * sizeof(SlotMeta)));
-  CK(cudaMalloc(&doff, (size_t)(cap + 1) * sizeof(long long)));
+  CK(cudaMalloc(&doff, (size_t)(cap + kVariants) * sizeof(long long)));
   CK(cudaMallocHost(&hm, (size_t)cap * sizeof(SlotMeta)));
-  CK(cudaMallocHost(&hoff, (size_t)(cap + 1) * sizeof(long long)));
+  CK(cudaMallocHost(&hoff, (size_t)(cap + kVariants) * sizeof(long long)));
   CK(cudaStreamSynchronize(b->stream));
   if (b->d_images) {
     CK(cudaMemcpy(nimg, b->d_images, (size_t)b->capacity * kImages * kArgsBytes,
@@ -342,54 +446,65 @@ void retire_completed(lbm_batch* b) {
   }
 }
 
-// Build and upload the tables of one chunk; returns the lattice updates.
+// Build and upload the tables of one chunk and launch its graph; returns
+// the lattice updates.  Slots are grouped by variant.
 int issue_chunk(lbm_batch* b, int steps_offered, long long* lups) {
   const int S = chunk_steps(b);
-  int n = 0;
-  long long tiles = 0, updates = 0;
+  *lups = 0;
+  const int mask = pending_mask(b);
+  if (mask == 0) return LBM_OK;
+  int rc = ensure_graph(b, mask);
+  if (rc) return rc;
   const int tile = b->graph_block * b->graph_npt;
   CK(cudaEventSynchronize(b->tables_free));  // the pinned tables may be rewritten
-  for (auto& kv : b->members) {
-    lbm_batch::Member& m = kv.second;
-    const long long left = m.target - m.issued;
-    if (left <= 0) continue;
-    const int active = (int)std::min<long long>(std::min(S, steps_offered), left);
-    lbm_domain* d = m.d;
-    SlotMeta& sm = b->h_meta[n];
-    sm.variant = storage_index(d->opt.storage) * 4 + model_of(d->in);
-    sm.image_base = m.image_slot * kImages;
-    sm.nx = d->g.nx;
-    sm.nz = d->g.nz;
-    sm.mnx = ~0ull / (unsigned long long)d->g.nx + 1;
-    sm.mnz = ~0ull / (unsigned long long)d->g.nz + 1;
-    sm.nodes = d->N;
-    sm.active = active;
-    sm.cur0 = d->cur;
-    b->h_off[n] = tiles;
-    tiles += (d->N + tile - 1) / tile;
-    updates += d->N * active;
-    // host bookkeeping of the steps this chunk takes
-    d->step += active;
-    d->cur ^= (active & 1);
-    d->post_direct = false;
-    m.issued += active;
-    if (m.issued >= m.target) m.done_chunk = b->chunks_issued + 1;
-    ++n;
+  std::memset(b->h_tab->v, 0, sizeof(b->h_tab->v));
+  int n = 0, noff = 0;
+  long long updates = 0;
+  for (int v = 0; v < kVariants; ++v) {
+    if (!(mask & (1 << v))) continue;
+    VariantList& L = b->h_tab->v[v];
+    L.slot0 = n;
+    L.off0 = noff;
+    long long tiles = 0;
+    for (auto& kv : b->members) {
+      lbm_batch::Member& m = kv.second;
+      lbm_domain* d = m.d;
+      const long long left = m.target - m.issued;
+      if (left <= 0 || member_variant(d) != v) continue;
+      const int active = (int)std::min<long long>(std::min(S, steps_offered), left);
+      SlotMeta& sm = b->h_meta[n];
+      sm.image_base = m.image_slot * kImages;
+      sm.nx = d->g.nx;
+      sm.nz = d->g.nz;
+      sm.mnx = ~0ull / (unsigned long long)d->g.nx + 1;
+      sm.mnz = ~0ull / (unsigned long long)d->g.nz + 1;
+      sm.nodes = d->N;
+      sm.active = active;
+      sm.cur0 = d->cur;
+      sm.pad = 0;
+      b->h_off[noff++] = tiles;
+      tiles += (d->N + tile - 1) / tile;
+      updates += d->N * active;
+      // host bookkeeping of the steps this chunk takes
+      d->step += active;
+      d->cur ^= (active & 1);
+      d->post_direct = false;
+      m.issued += active;
+      if (m.issued >= m.target) m.done_chunk = b->chunks_issued + 1;
+      ++n;
+    }
+    b->h_off[noff++] = tiles;
+    L.nslots = n - L.slot0;
+    L.ntiles = tiles;
   }
-  b->h_off[n] = tiles;
-  if (n == 0) {
-    *lups = 0;
-    return LBM_OK;
-  }
-  b->h_tab->nslots = n;
   b->h_tab->tile = tile;
-  b->h_tab->ntiles = tiles;
+  b->h_tab->schedule = b->graph_sched;
   b->h_tab->meta = b->d_meta;
   b->h_tab->tile_off = b->d_off;
   b->h_tab->images = b->d_images;
   CK(cudaMemcpyAsync(b->d_meta, b->h_meta, (size_t)n * sizeof(SlotMeta), cudaMemcpyHostToDevice,
                      b->stream));
-  CK(cudaMemcpyAsync(b->d_off, b->h_off, (size_t)(n + 1) * sizeof(long long),
+  CK(cudaMemcpyAsync(b->d_off, b->h_off, (size_t)noff * sizeof(long long),
                      cudaMemcpyHostToDevice, b->stream));
   CK(cudaMemcpyAsync(b->d_tab, b->h_tab, sizeof(BatchTables), cudaMemcpyHostToDevice, b->stream));
   CK(cudaEventRecord(b->tables_free, b->stream));
@@ -451,6 +566,8 @@ int lbm_batch_create(const lbm_batch_options* bo, lbm_batch** out) {
     return set_error(LBM_ERR_INVALID, "block must be 128 or 256");
   if (o.nodes_per_thread < 0 || o.nodes_per_thread > 8)
     return set_error(LBM_ERR_INVALID, "nodes_per_thread must be 1..8");
+  if (o.schedule < 0 || o.schedule > 1) return set_error(LBM_ERR_INVALID, "schedule must be 0 or 1");
+  if (o.regs < 0 || o.regs > 1) return set_error(LBM_ERR_INVALID, "regs must be 0 or 1");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return set_error(LBM_ERR_NO_DEVICE, "no CUDA device available");
@@ -485,7 +602,6 @@ int lbm_batch_create(const lbm_batch_options* bo, lbm_batch** out) {
     return fail(set_error(LBM_ERR_OOM, "batch tables"));
   std::memset(b->h_tab, 0, sizeof(BatchTables));
   if ((rc = grow_images(b))) return fail(rc);
-  if ((rc = ensure_graph(b))) return fail(rc);
   *out = b;
   return LBM_OK;
 }
@@ -529,6 +645,11 @@ int lbm_batch_add(lbm_batch* b, const Inputval* pinput, const lbm_options* opt,
   if (b->free_images.empty() && (rc = grow_images(b))) return rc;
   lbm_domain* d = new lbm_domain();
   domain_prepare(d, pinput, opt);
+  if ((long long)Q * d->qs >= (1LL << 31)) {  // 32-bit population indices (IndexAddr)
+    delete d;
+    return set_error(LBM_ERR_INVALID,
+                     "batch members need 19 x plane size < 2^31 (about 113M nodes)");
+  }
   d->opt.device = b->opt.device;
   d->pooled = true;
   d->stream = b->stream;
@@ -582,7 +703,8 @@ int lbm_batch_step(lbm_batch* b, int steps) {
   if (!b) return set_error(LBM_ERR_INVALID, "NULL batch");
   if (steps < 0) return set_error(LBM_ERR_INVALID, "negative steps");
   CK(cudaSetDevice(b->opt.device));
-  int rc = ensure_graph(b);
+  // capture before the first event so that the timed span holds GPU work only
+  int rc = pending_mask(b) ? ensure_graph(b, pending_mask(b)) : LBM_OK;
   if (rc) return rc;
   CK(cudaEventRecord(b->ev0, b->stream));
   long long total = 0;
@@ -667,42 +789,72 @@ int lbm_batch_usage(lbm_batch* b, size_t* used, size_t* largest_free, int* ndoma
 int lbm_batch_autotune(lbm_batch* b, int trial_steps, lbm_batch_options* chosen) {
   if (!b) return set_error(LBM_ERR_INVALID, "NULL batch");
   if (trial_steps <= 0) return set_error(LBM_ERR_INVALID, "trial_steps must be positive");
-  const int blocks[] = {128, 256};
-  const int npts[] = {1, 2, 4};
-  const int ctas[] = {0, 2};
-  float best = 1e30f;
+  // coordinate search: register build x schedule x block at 2 nodes per
+  // thread, then nodes per thread, then a cap of 2 CTAs per SM
   lbm_batch_options keep = b->opt, best_opt = b->opt;
-  for (int blk : blocks)
-    for (int np : npts)
-      for (int c : ctas) {
-        b->opt.block = blk;
-        b->opt.nodes_per_thread = np;
-        b->opt.ctas_per_sm = c;
-        int rc = lbm_batch_step(b, trial_steps);
-        if (rc) {
-          b->opt = keep;
-          return rc;
-        }
-        float ms = 0;
-        long long lups = 0;
-        if ((rc = lbm_batch_last_step_ms(b, &ms, &lups))) {
-          b->opt = keep;
-          return rc;
-        }
-        if (lups == 0) {  // nothing left to step: keep the current shape
-          b->opt = keep;
-          if (chosen) *chosen = keep;
-          return LBM_OK;
-        }
-        const float per_update = ms / (float)lups;
-        if (per_update < best) {
-          best = per_update;
-          best_opt = b->opt;
-        }
+  float best = 1e30f;
+  bool done = false;
+  auto trial = [&](const lbm_batch_options& o) -> int {
+    b->opt = o;
+    int rc = lbm_batch_step(b, trial_steps);
+    float ms = 0;
+    long long lups = 0;
+    if (!rc) rc = lbm_batch_last_step_ms(b, &ms, &lups);
+    if (rc) return rc;
+    if (lups == 0) {  // nothing left to step
+      done = true;
+      return LBM_OK;
+    }
+    const float per_update = ms / (float)lups;
+    if (per_update < best) {
+      best = per_update;
+      best_opt = o;
+    }
+    return LBM_OK;
+  };
+  std::vector<lbm_batch_options> stage;
+  for (int regs : {0, 1})
+    for (int sc : {0, 1})
+      for (int blk : {128, 256}) {
+        lbm_batch_options o = keep;
+        o.regs = regs;
+        o.schedule = sc;
+        o.block = blk;
+        o.nodes_per_thread = 2;
+        o.ctas_per_sm = 0;
+        stage.push_back(o);
       }
+  for (int phase = 0; phase < 3 && !done; ++phase) {
+    if (phase == 1) {
+      stage.clear();
+      for (int np : {1, 4}) {
+        lbm_batch_options o = best_opt;
+        o.nodes_per_thread = np;
+        stage.push_back(o);
+      }
+    } else if (phase == 2) {
+      stage.clear();
+      lbm_batch_options o = best_opt;
+      o.ctas_per_sm = 2;
+      stage.push_back(o);
+    }
+    for (const lbm_batch_options& o : stage) {
+      int rc = trial(o);
+      if (rc) {
+        b->opt = keep;
+        return rc;
+      }
+      if (done) break;
+    }
+  }
+  if (best >= 1e30f) {
+    b->opt = keep;
+    if (chosen) *chosen = keep;
+    return LBM_OK;
+  }
   b->opt = best_opt;
   if (chosen) *chosen = best_opt;
-  return ensure_graph(b);
+  return LBM_OK;
 }
 
 }  // extern "C"

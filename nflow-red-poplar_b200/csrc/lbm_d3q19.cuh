@@ -92,6 +92,7 @@ struct StoreTraits<float> {
   static constexpr bool shifted = false;
   __device__ static __forceinline__ float load(const float* p, float, float) { return *p; }
   __device__ static __forceinline__ void store(float* p, float v, float, float) { *p = v; }
+  __device__ static __forceinline__ void store_fma(float* p, float v, float, float) { *p = v; }
 };
 template <>
 struct StoreTraits<double> {
@@ -99,6 +100,7 @@ struct StoreTraits<double> {
   static constexpr bool shifted = false;
   __device__ static __forceinline__ double load(const double* p, double, double) { return *p; }
   __device__ static __forceinline__ void store(double* p, double v, double, double) { *p = v; }
+  __device__ static __forceinline__ void store_fma(double* p, double v, float, float) { *p = v; }
 };
 template <>
 struct StoreTraits<__half> {
@@ -110,6 +112,11 @@ struct StoreTraits<__half> {
   __device__ static __forceinline__ void store(__half* p, float v, float w, float scale) {
     *p = __float2half_rn((v - w) * scale);
   }
+  // the same value as store(): (v - w) * scale with scale a power of two is
+  // v * scale - w * scale rounded once; nws = -w * scale
+  __device__ static __forceinline__ void store_fma(__half* p, float v, float scale, float nws) {
+    *p = __float2half_rn(fmaf(v, scale, nws));
+  }
 };
 template <>
 struct StoreTraits<__nv_bfloat16> {
@@ -120,6 +127,10 @@ struct StoreTraits<__nv_bfloat16> {
   }
   __device__ static __forceinline__ void store(__nv_bfloat16* p, float v, float w, float scale) {
     *p = __float2bfloat16_rn((v - w) * scale);
+  }
+  __device__ static __forceinline__ void store_fma(__nv_bfloat16* p, float v, float scale,
+                                                   float nws) {
+    *p = __float2bfloat16_rn(fmaf(v, scale, nws));
   }
 };
 
@@ -156,20 +167,33 @@ __host__ __device__ __forceinline__ float fma_(float a, float b, float c) { retu
 __host__ __device__ __forceinline__ double fma_(double a, double b, double c) { return fma(a, b, c); }
 __device__ __forceinline__ F2 fma_(F2 a, F2 b, F2 c) { return F2{__ffma2_rn(a.v, b.v, c.v)}; }
 
-// 1/x rounded to nearest (one reciprocal instead of a full division)
+// 1/x and sqrt(x) of the FP32 lanes with the single-instruction PTX
+// approximations (rcp.approx: at most 1 ulp; sqrt.approx: relative error
+// below 2^-23) — the node arithmetic needs 2 reciprocals and 2 square roots
+// and is issue-bound; the FP64 build keeps the IEEE operations.
 __host__ __device__ __forceinline__ float vrcp(float a) {
 #ifdef __CUDA_ARCH__
-  return __frcp_rn(a);
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
+  return r;
 #else
   return 1.0f / a;
 #endif
 }
 __host__ __device__ __forceinline__ double vrcp(double a) { return 1.0 / a; }
-__device__ __forceinline__ F2 vrcp(F2 a) { return mk2(__frcp_rn(a.v.x), __frcp_rn(a.v.y)); }
+__device__ __forceinline__ F2 vrcp(F2 a) { return mk2(vrcp(a.v.x), vrcp(a.v.y)); }
 
-__host__ __device__ __forceinline__ float vsqrt(float a) { return sqrtf(a); }
+__host__ __device__ __forceinline__ float vsqrt(float a) {
+#ifdef __CUDA_ARCH__
+  float r;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
+  return r;
+#else
+  return sqrtf(a);
+#endif
+}
 __host__ __device__ __forceinline__ double vsqrt(double a) { return sqrt(a); }
-__device__ __forceinline__ F2 vsqrt(F2 a) { return mk2(sqrtf(a.v.x), sqrtf(a.v.y)); }
+__device__ __forceinline__ F2 vsqrt(F2 a) { return mk2(vsqrt(a.v.x), vsqrt(a.v.y)); }
 
 // broadcast a compile-time constant to a lane value (rounded once to the
 // lane's precision, like a float literal)

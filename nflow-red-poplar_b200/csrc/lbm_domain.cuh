@@ -178,9 +178,10 @@ StepArgs<S> make_args(const lbm_domain* d, const void* src, void* dst, long long
   a.dst = (S*)dst;
   a.qs = d->qs;
   for (int q = 0; q < Q; ++q) {
-    a.srcq[q] = src ? (const S*)src + q * d->qs : nullptr;
-    a.dstq[q] = dst ? (S*)dst + q * d->qs : nullptr;
     a.off[q] = cx(q) + d->g.px * (cz(q) + d->g.nz * cy(q));
+    a.srcq[q] = src ? (const S*)src + q * d->qs : nullptr;
+    a.srcd[q] = src ? (const S*)src + (q * d->qs - a.off[q]) : nullptr;
+    a.dstq[q] = dst ? (S*)dst + q * d->qs : nullptr;
   }
   a.g = d->g;
   a.tau = R(d->in.m_dTau);
@@ -196,6 +197,10 @@ StepArgs<S> make_args(const lbm_domain* d, const void* src, void* dst, long long
   a.mp.wxx = R(d->in.dWXX);
   a.scale = d->scale;
   a.inv_scale = d->inv_scale;
+  for (int c = 0; c < 3; ++c) {
+    const float w = c == 0 ? 1.0f / 3.0f : (c == 1 ? 1.0f / 18.0f : 1.0f / 36.0f);
+    a.nws[c] = -w * d->scale;
+  }
   a.inlet_u = d->inlet_u;
   a.init_kind = d->opt.init_kind;
   a.noise_amp = d->opt.noise_amp;

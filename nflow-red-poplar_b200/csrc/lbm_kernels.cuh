@@ -92,9 +92,11 @@ struct StepArgs {
   // hot-path addressing: plane of population q and the in-plane offset
   // c_x + c_z px + c_y px nz of its donor; node indices inside a plane are
   // 32-bit (px*nz*ny < 2^31 is checked when the domain is created)
-  const S* srcq[Q];
+  const S* srcq[Q];            // plane of population q
+  const S* srcd[Q];            // srcq[q] - off[q]: the donor of a node is srcd[q][cell]
   S* dstq[Q];
   int off[Q];
+  float nws[3];                // -w * scale per weight class (16-bit stores)
   Geometry g;
   R tau, les_c, rho0;
   R ulx, uly, ulz;            // lid velocity (cavity)
@@ -124,6 +126,37 @@ __device__ __forceinline__ RealOf<S> ld(const S* p, int q, float inv_scale) {
 // Boundary value of population q at a node whose donor x - c_q is outside
 // the domain.  d = opp(q) is the reference's "outside" direction; fo is
 // f*_{k-1}[d] at the node itself (arFTemp[d](x) in the reference).
+// Where the populations of a node live (cell = in-plane index of the node).
+// PlaneAddr takes the per-population plane pointers of StepArgs: in the
+// kernel parameter space they are free operands, one address instruction per
+// access.  IndexAddr derives every address from the two lattice bases and
+// the strides: for arguments held in shared memory (the batched kernel),
+// where 38 plane pointers would otherwise be loaded into registers.  It
+// needs Q * qs < 2^31.
+template <class S>
+struct PlaneAddr {
+  const StepArgs<S>& a;
+  int cell;
+  __device__ __forceinline__ PlaneAddr(const StepArgs<S>& args, int c) : a(args), cell(c) {}
+  __device__ __forceinline__ const S* donor(int q) const { return a.srcd[q] + cell; }
+  __device__ __forceinline__ const S* own(int q) const { return a.srcq[q] + cell; }
+  __device__ __forceinline__ S* out(int q) const { return a.dstq[q] + cell; }
+};
+
+template <class S>
+struct IndexAddr {
+  const S* src;
+  S* dst;
+  int cell, qs, px, pxnz;
+  __device__ __forceinline__ IndexAddr(const StepArgs<S>& a, int c)
+      : src(a.src), dst(a.dst), cell(c), qs((int)a.qs), px(a.g.px), pxnz(a.g.px * a.g.nz) {}
+  __device__ __forceinline__ const S* donor(int q) const {
+    return src + (cell + q * qs - (cx(q) + px * cz(q) + pxnz * cy(q)));
+  }
+  __device__ __forceinline__ const S* own(int q) const { return src + (cell + q * qs); }
+  __device__ __forceinline__ S* out(int q) const { return dst + (cell + q * qs); }
+};
+
 template <class S, int q>
 __device__ __forceinline__ RealOf<S> boundary_value(const StepArgs<S>& a, int t, RealOf<S> fo,
                                                     int y, int z) {
@@ -227,9 +260,9 @@ __device__ __forceinline__ R initial_feq(R rd, R ux, R uy, R uz) {
 // inlet/outlet nodes apply their rule to donors outside the domain; every
 // other population is never written in the reference and keeps its
 // initial value.
-template <class S>
-__device__ __forceinline__ void pull_struct(RealOf<S> (&f)[Q], const StepArgs<S>& a, int x, int y,
-                                            int z, int cell) {
+template <class S, class Addr>
+__device__ __forceinline__ void pull_struct(RealOf<S> (&f)[Q], const StepArgs<S>& a, const Addr& ad,
+                                            int x, int y, int z) {
   using R = RealOf<S>;
   const int t = node_type(a.g, x, y, z);
   const InitState is = initial_state(a.g, a.init_kind, a.seed, a.noise_amp, (float)a.rho0,
@@ -241,11 +274,11 @@ __device__ __forceinline__ void pull_struct(RealOf<S> (&f)[Q], const StepArgs<S>
     const bool inside = (unsigned)xs < (unsigned)a.g.nx && (unsigned)ys < (unsigned)a.g.ny &&
                         (unsigned)zs < (unsigned)a.g.nz;
     if (inside && node_type(a.g, xs, ys, zs) != NODE_STRUCT) {
-      f[q] = ld(a.srcq[q] + (cell - a.off[q]), q, a.inv_scale);
+      f[q] = ld(ad.donor(q), q, a.inv_scale);
     } else if (inside && t == NODE_FLUID) {
-      f[q] = ld(a.srcq[opp(q)] + cell, opp(q), a.inv_scale);
+      f[q] = ld(ad.own(opp(q)), opp(q), a.inv_scale);
     } else if (!inside && (t == NODE_INLET || t == NODE_OUTLET)) {
-      const R fo = ld(a.srcq[opp(q)] + cell, opp(q), a.inv_scale);
+      const R fo = ld(ad.own(opp(q)), opp(q), a.inv_scale);
       f[q] = boundary_value<S, q>(a, t, fo, y, z);
     } else {
       f[q] = initial_feq<R, q>(R(is.den), R(is.ux), R(is.uy), R(is.uz));
@@ -255,17 +288,17 @@ __device__ __forceinline__ void pull_struct(RealOf<S> (&f)[Q], const StepArgs<S>
 
 // Steps 1-2: the post-stream, post-boundary populations f_k at (x,y,z);
 // cell is the node's in-plane index.
-template <class S>
-__device__ __forceinline__ void pull(RealOf<S> (&f)[Q], const StepArgs<S>& a, int x, int y, int z,
-                                     int cell) {
+template <class S, class Addr>
+__device__ __forceinline__ void pull(RealOf<S> (&f)[Q], const StepArgs<S>& a, const Addr& ad, int x,
+                                     int y, int z) {
   const bool edge = (x == 0) | (x == a.g.nx - 1) | (y == 0) | (y == a.g.ny - 1) | (z == 0) |
                     (z == a.g.nz - 1);
   if (a.g.casetype == POISEUILLE) {
-    pull_struct<S>(f, a, x, y, z, cell);
+    pull_struct<S>(f, a, ad, x, y, z);
   } else if (!edge) {
     static_for<0, Q>([&](auto qc) {
       constexpr int q = decltype(qc)::value;
-      f[q] = ld(a.srcq[q] + (cell - a.off[q]), q, a.inv_scale);
+      f[q] = ld(ad.donor(q), q, a.inv_scale);
     });
   } else {
     const int t = node_type(a.g, x, y, z);
@@ -275,9 +308,9 @@ __device__ __forceinline__ void pull(RealOf<S> (&f)[Q], const StepArgs<S>& a, in
       const bool inside = (unsigned)xs < (unsigned)a.g.nx && (unsigned)ys < (unsigned)a.g.ny &&
                           (unsigned)zs < (unsigned)a.g.nz;
       if (inside) {
-        f[q] = ld(a.srcq[q] + (cell - a.off[q]), q, a.inv_scale);
+        f[q] = ld(ad.donor(q), q, a.inv_scale);
       } else {
-        const RealOf<S> fo = ld(a.srcq[opp(q)] + cell, opp(q), a.inv_scale);
+        const RealOf<S> fo = ld(ad.own(opp(q)), opp(q), a.inv_scale);
         f[q] = boundary_value<S, q>(a, t, fo, y, z);
       }
     });
@@ -364,23 +397,24 @@ struct StoreNode {
 
 // One fused step of the node (x, y, z): pull + boundary rules, macroscopic,
 // LES, collision, store.  Shared by the single-domain and batched kernels,
-// so a domain gets the same bits alone and in a batch.
-template <class S, int COLL, bool LES>
+// so a domain gets the same bits alone and in a batch (the addressing
+// policy changes where the operands come from, not the arithmetic).
+template <class S, int COLL, bool LES, template <class> class Addr = PlaneAddr>
 __device__ __forceinline__ void step_node(const StepArgs<S>& a, int x, int y, int z) {
   using R = RealOf<S>;
   // STRUCT nodes are never streamed, collided or measured (kernel.cu:294,
   // 323, 362, 464, 495, 1105)
   if (a.g.casetype == POISEUILLE && node_type(a.g, x, y, z) == NODE_STRUCT) return;
-  const int cell = x + a.g.px * (z + a.g.nz * y);
+  const Addr<S> ad(a, x + a.g.px * (z + a.g.nz * y));
   R f[Q];
-  pull<S>(f, a, x, y, z, cell);
+  pull<S>(f, a, ad, x, y, z);
   PairState<R> ps;
   make_pairs<R>(f, ps);
   R ux, uy, uz;
   const R inv_rho = velocity<R>(ps, ux, uy, uz);
   write_macro<S>(a, x, y, z, ps.rho, ux, uy, uz);
   collide_node<S, COLL, LES, false, R>(f, ps, ux, uy, uz, inv_rho, a, [&](int q, R v) {
-    StoreTraits<S>::store(a.dstq[q] + cell, v, weight<R>(q), a.scale);
+    StoreTraits<S>::store_fma(ad.out(q), v, a.scale, a.nws[wclass(q)]);
   });
 }
 
@@ -512,7 +546,7 @@ __global__ void __launch_bounds__(128)
       f[q] = ld(a.src + q * a.qs + cell, q, a.inv_scale);
     });
   } else {
-    pull<S>(f, a, x, y, z, (int)cell);
+    pull<S>(f, a, PlaneAddr<S>(a, (int)cell), x, y, z);
   }
   long long node;
   if (padded)
@@ -592,7 +626,7 @@ __global__ void __launch_bounds__(64, LBM_PACKED_MIN_BLOCKS) k_step2(const __gri
   if (interior) {
     static_for<0, Q>([&](auto qc) {
       constexpr int q = decltype(qc)::value;
-      const S* p = a.srcq[q] + (cell - a.off[q]);
+      const S* p = a.srcd[q] + cell;
       if constexpr (cx(q) == 0) {
         f[q] = ld_pair<S>(p, q, a.inv_scale);
       } else {
@@ -601,9 +635,9 @@ __global__ void __launch_bounds__(64, LBM_PACKED_MIN_BLOCKS) k_step2(const __gri
     });
   } else {
     float fa[Q], fb[Q];
-    pull<S>(fa, a, x0, y, z, cell);
+    pull<S>(fa, a, PlaneAddr<S>(a, cell), x0, y, z);
     if (two) {
-      pull<S>(fb, a, x0 + 1, y, z, cell + 1);
+      pull<S>(fb, a, PlaneAddr<S>(a, cell + 1), x0 + 1, y, z);
     } else {
       static_for<0, Q>([&](auto qc) { fb[decltype(qc)::value] = fa[decltype(qc)::value]; });
     }

@@ -47,9 +47,17 @@ def alone(iv, o, steps):
     return f, m
 
 
+# launch shapes: (schedule, register build, block, nodes per thread)
+SHAPES = [(0, 0, 256, 2), (1, 1, 128, 1), (0, 1, 256, 4), (1, 0, 128, 3)]
+
+
+@pytest.mark.parametrize("shape", SHAPES, ids=["s0r0b256n2", "s1r1b128n1", "s0r1b256n4",
+                                               "s1r0b128n3"])
 @pytest.mark.parametrize("steps", [1, 37, 100])
-def test_batch_matches_alone_bit_for_bit(steps):
-    b = pkg.Batch(hbm_budget=512 << 20, chunk_steps=16)
+def test_batch_matches_alone_bit_for_bit(steps, shape):
+    sched, regs, block, npt = shape
+    b = pkg.Batch(hbm_budget=512 << 20, chunk_steps=16, schedule=sched, regs=regs, block=block,
+                  nodes_per_thread=npt)
     ids = [b.add(iv, opts(st, k, a), steps) for iv, st, k, a in CASES]
     b.step(steps)
     b.sync()
@@ -134,3 +142,7 @@ def test_batch_rejects_fp64_and_bad_options():
     b.close()
     with pytest.raises(pkg.LbmError):
         pkg.Batch(hbm_budget=64 << 20, chunk_steps=7)
+    with pytest.raises(pkg.LbmError):
+        pkg.Batch(hbm_budget=64 << 20, schedule=2)
+    with pytest.raises(pkg.LbmError):
+        pkg.Batch(hbm_budget=64 << 20, regs=2)
