@@ -46,11 +46,13 @@ struct SlotMeta {
 };
 
 // model: 0 SRT, 1 SRT+LES, 2 MRT, 3 MRT+LES; variant = storage * 4 + model
-constexpr int kVariants = 12;
+// A launch group is the domains of one variant with one storage scale; each
+// step launches the group's kernel once, the scale being a kernel parameter.
+constexpr int kGroups = 32;
 
-// The domains of one variant: meta[slot0 .. slot0 + nslots) and their tile
-// prefix sums tile_off[off0 .. off0 + nslots] (tiles of the variant's list).
-struct VariantList {
+// The domains of one group: meta[slot0 .. slot0 + nslots) and their tile
+// prefix sums tile_off[off0 .. off0 + nslots] (tiles of the group's list).
+struct GroupList {
   int nslots;
   int slot0;
   int off0;
@@ -61,7 +63,7 @@ struct VariantList {
 struct BatchTables {
   int tile;          // nodes per tile = block * npt
   int schedule;      // 0: contiguous tile range per CTA, 1: grid-stride
-  VariantList v[kVariants];
+  GroupList v[kGroups];
   const SlotMeta* meta;
   const long long* tile_off;
   const unsigned char* images;   // [capacity * kImages][kArgsBytes]
@@ -71,78 +73,46 @@ __device__ __forceinline__ unsigned fastdiv(unsigned n, unsigned long long m) {
   return (unsigned)__umul64hi(m, (unsigned long long)n);
 }
 
-template <class S> struct StorageIndex;
-template <> struct StorageIndex<float> { static constexpr int value = 0; };
-template <> struct StorageIndex<__half> { static constexpr int value = 1; };
-template <> struct StorageIndex<__nv_bfloat16> { static constexpr int value = 2; };
+// the CTA's current domain, in shared memory: everything the tile loop
+// needs besides the tile index itself, so that little stays live in
+// registers across the node step
+struct CurSlot {
+  SlotMeta m;
+  long long begin, end;  // the domain's tiles [begin, end) in the group list
+  long long ntiles;      // tiles of the group
+  int s;                 // slot index in the group, -1 before the first
+  int ok;                // the domain takes step j
+  int image;             // argument image in img[], -1 = none
+  int fetch;             // image to copy into img[] on entry, -1 = none
+};
 
-// the nodes of local tile lt of the domain described by m
+// the nodes of local tile lt of the current domain
 template <class S, int COLL, bool LES>
-__device__ __forceinline__ void batch_tile(const StepArgs<S>& a, const SlotMeta& m, long long lt,
-                                           int tile, int npt) {
-  const unsigned base = (unsigned)(lt * tile);
-  const unsigned nodes = (unsigned)m.nodes;
+__device__ __forceinline__ void batch_tile(const StepArgs<S>& a, const CurSlot& cur,
+                                           unsigned lt, int npt, const Scales& sc) {
+  const unsigned base = lt * (unsigned)(blockDim.x * npt);
   for (int i = 0; i < npt; ++i) {
     const unsigned n = base + (unsigned)i * blockDim.x + threadIdx.x;
-    if (n >= nodes) break;
-    const unsigned r = fastdiv(n, m.mnx);
-    const int x = (int)(n - r * (unsigned)m.nx);
-    const unsigned y = fastdiv(r, m.mnz);
-    const int z = (int)(r - y * (unsigned)m.nz);
-    step_node<S, COLL, LES, IndexAddr>(a, x, (int)y, z);
+    if (n >= (unsigned)cur.m.nodes) break;
+    const unsigned r = fastdiv(n, cur.m.mnx);
+    const int x = (int)(n - r * (unsigned)cur.m.nx);
+    const unsigned y = fastdiv(r, cur.m.mnz);
+    const int z = (int)(r - y * (unsigned)cur.m.nz);
+    step_node<S, COLL, LES, IndexAddr>(a, x, (int)y, z, sc);
   }
 }
 
-// Make slot s (meta and argument image for launch j) the CTA's current
-// domain in shared memory; returns false when the domain takes no step j.
-// All threads of the CTA take the same path.
-__device__ __forceinline__ bool enter_slot(SlotMeta& sm, unsigned char* img,
-                                           const SlotMeta* __restrict__ meta,
-                                           const unsigned char* images, int s, int j, int& cached) {
-  const int active = meta[s].active;
-  if (j >= active) return false;
-  const int image = meta[s].image_base + ((meta[s].cur0 + j) & 1) * 3 +
-                    (j >= active - 1 ? 2 : (j >= active - 2 ? 1 : 0));
-  if (image == cached) return true;
-  __syncthreads();
-  const int4* src = reinterpret_cast<const int4*>(images + (size_t)image * kArgsBytes);
-  int4* dst = reinterpret_cast<int4*>(img);
-  for (int i = threadIdx.x; i < kArgsBytes / 16; i += blockDim.x) dst[i] = src[i];
-  if (threadIdx.x == 0) sm = meta[s];
-  __syncthreads();
-  cached = image;
-  return true;
-}
-
-// One time step (launch j of a chunk) of every active domain of one variant.
-// Schedule 0 gives CTA c the contiguous tiles [c*per, (c+1)*per) of the
-// variant's list, so a CTA looks its domain up once and reloads arguments
-// only where its range crosses into the next domain; schedule 1 walks
-// t = blockIdx.x, += gridDim.x and advances the domain cursor monotonically.
-// The domain's arguments and meta stay in shared memory (uniform over the
-// CTA).  MINB (resident 256-thread CTAs the register budget must allow: 4 ->
-// 64 registers, 3 -> 80) trades spills of the uniform arguments against
-// occupancy; the autotuner picks it.
-template <class S, int COLL, bool LES, int MINB>
-__global__ void __launch_bounds__(256, MINB) k_batch_step(const BatchTables* __restrict__ tab,
-                                                          int j, int npt) {
-  constexpr int V = StorageIndex<S>::value * 4 + (COLL == COLL_MRT ? 2 : 0) + (LES ? 1 : 0);
-  __shared__ __align__(16) unsigned char img[kArgsBytes];
-  __shared__ SlotMeta sm;
-  const StepArgs<S>& a = *reinterpret_cast<const StepArgs<S>*>(img);
-  const VariantList L = tab->v[V];
-  if (L.nslots == 0 || L.ntiles == 0) return;
-  const int tile = tab->tile;
-  const SlotMeta* __restrict__ meta = tab->meta + L.slot0;
-  const long long* __restrict__ off = tab->tile_off + L.off0;
-  const unsigned char* images = tab->images;
-  int cached = -1;
-  if (tab->schedule == 0) {
-    const long long per = (L.ntiles + gridDim.x - 1) / gridDim.x;
-    long long t = (long long)blockIdx.x * per;
-    const long long tend = min(t + per, L.ntiles);
-    if (t >= tend) return;
-    int lo = 0, hi = L.nslots;  // off[lo] <= t < off[hi]
+// Make the slot holding tile t (at or after the current one) the CTA's
+// current domain: meta, tile range and, when it takes step j, its argument
+// image for launch j.  All threads of the CTA take the same path.
+__device__ __forceinline__ void enter_slot(CurSlot& cur, unsigned char* img,
+                                           const BatchTables* __restrict__ tab, int g, long long t,
+                                           int j) {
+  __syncthreads();  // every thread is done with the previous domain
+  if (threadIdx.x == 0) {
+    const GroupList& L = tab->v[g];
+    const long long* off = tab->tile_off + L.off0;
+    int lo = cur.s < 0 ? 0 : cur.s, hi = L.nslots;  // off[lo] <= t < off[hi]
     while (hi - lo > 1) {
       const int mid = (lo + hi) >> 1;
       if (off[mid] <= t)
@@ -150,26 +120,69 @@ __global__ void __launch_bounds__(256, MINB) k_batch_step(const BatchTables* __r
       else
         hi = mid;
     }
-    for (int s = lo; t < tend; ++s) {
-      const long long s_begin = off[s], s_end = off[s + 1];
-      if (enter_slot(sm, img, meta, images, s, j, cached)) {
-        const long long stop = min(s_end, tend);
-        for (; t < stop; ++t) batch_tile<S, COLL, LES>(a, sm, t - s_begin, tile, npt);
+    const SlotMeta m = tab->meta[L.slot0 + lo];
+    cur.m = m;
+    cur.s = lo;
+    cur.begin = off[lo];
+    cur.end = off[lo + 1];
+    cur.ok = j < m.active;
+    const int image = m.image_base + ((m.cur0 + j) & 1) * 3 +
+                      (j >= m.active - 1 ? 2 : (j >= m.active - 2 ? 1 : 0));
+    cur.fetch = cur.ok && image != cur.image ? image : -1;
+    if (cur.ok) cur.image = image;
+  }
+  __syncthreads();
+  const int fetch = cur.fetch;
+  if (fetch >= 0) {
+    const int4* src = reinterpret_cast<const int4*>(tab->images + (size_t)fetch * kArgsBytes);
+    int4* dst = reinterpret_cast<int4*>(img);
+    for (int i = threadIdx.x; i < kArgsBytes / 16; i += blockDim.x) dst[i] = src[i];
+    __syncthreads();
+  }
+}
+
+// One time step (launch j of a chunk) of every active domain of launch
+// group g (one variant, one storage scale sc).  Schedule 0 gives CTA c the
+// contiguous tiles [c*per, (c+1)*per) of the group's list; schedule 1 walks
+// t = blockIdx.x, += gridDim.x.  Either way the CTA moves forward through the
+// domains and reloads a domain's arguments only when it enters it.  The
+// domain's arguments and meta stay in shared memory (uniform over the CTA).
+// MINB (resident 256-thread CTAs the register budget must allow: 4 -> 64
+// registers, 3 -> 80) trades occupancy against spills; the autotuner picks.
+template <class S, int COLL, bool LES, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_batch_step(const BatchTables* __restrict__ tab,
+                                                          int g, int j, int npt, const Scales sc) {
+  __shared__ __align__(16) unsigned char img[kArgsBytes];
+  __shared__ CurSlot cur;
+  const StepArgs<S>& a = *reinterpret_cast<const StepArgs<S>*>(img);
+  if (threadIdx.x == 0) {
+    cur.s = -1;
+    cur.image = -1;
+    cur.end = 0;
+    cur.ntiles = tab->v[g].ntiles;
+  }
+  __syncthreads();
+  if (tab->schedule == 0) {
+    const long long per = (cur.ntiles + gridDim.x - 1) / gridDim.x;
+    const long long t0 = (long long)blockIdx.x * per;
+    for (long long t = t0; t < min(t0 + per, cur.ntiles); ++t) {
+      if (t >= cur.end) enter_slot(cur, img, tab, g, t, j);
+      if (!cur.ok) {
+        t = cur.end - 1;
+        continue;
       }
-      t = s_end;
+      batch_tile<S, COLL, LES>(a, cur, (unsigned)(t - cur.begin), npt, sc);
     }
   } else {
-    int s = 0;
-    long long s_end = off[1];
-    for (long long t = blockIdx.x; t < L.ntiles; t += gridDim.x) {
-      while (t >= s_end) s_end = off[++s + 1];
-      if (!enter_slot(sm, img, meta, images, s, j, cached)) continue;
-      batch_tile<S, COLL, LES>(a, sm, t - off[s], tile, npt);
+    for (long long t = blockIdx.x; t < cur.ntiles; t += gridDim.x) {
+      if (t >= cur.end) enter_slot(cur, img, tab, g, t, j);
+      if (!cur.ok) continue;
+      batch_tile<S, COLL, LES>(a, cur, (unsigned)(t - cur.begin), npt, sc);
     }
   }
 }
 
-using BatchKernel = void (*)(const BatchTables*, int, int);
+using BatchKernel = void (*)(const BatchTables*, int, int, int, const Scales);
 
 template <class S, int MINB>
 constexpr BatchKernel batch_kernel_of(int model) {
@@ -291,9 +304,9 @@ struct lbm_batch {
   cudaEvent_t tables_free = nullptr;  // previous table upload has been consumed
   // chunk graph
   cudaGraphExec_t graph = nullptr;
-  int graph_block = 0, graph_npt = 0, graph_steps = 0, graph_mask = -1, graph_sched = -1;
+  int graph_block = 0, graph_npt = 0, graph_steps = 0, graph_sched = -1;
+  std::vector<std::pair<int, float>> graph_groups;  // (variant, scale) per launch group
   int graph_ctas = -1, graph_regs = -1;
-  int variant_mask = 0;           // variants with at least one unfinished member
   // completion tracking
   long long chunks_issued = 0;
   std::vector<std::pair<long long, cudaEvent_t>> chunk_events;
@@ -327,48 +340,70 @@ int member_variant(const lbm_domain* d) {
   return storage_index(d->opt.storage) * 4 + model_of(d->in);
 }
 
-// Variants with a member that still has steps to take.
-int pending_mask(const lbm_batch* b) {
-  int mask = 0;
+float member_scale(const lbm_domain* d) {
+  return d->opt.storage == LBM_STORE_F32 ? 1.0f : d->scale;
+}
+
+// Launch groups (variant, storage scale) of the members that still have
+// steps to take, in a fixed order.
+std::vector<std::pair<int, float>> pending_groups(const lbm_batch* b) {
+  std::vector<std::pair<int, float>> gs;
   for (auto& kv : b->members)
-    if (kv.second.issued < kv.second.target) mask |= 1 << member_variant(kv.second.d);
-  return mask;
+    if (kv.second.issued < kv.second.target) {
+      const std::pair<int, float> key(member_variant(kv.second.d), member_scale(kv.second.d));
+      if (std::find(gs.begin(), gs.end(), key) == gs.end()) gs.push_back(key);
+    }
+  std::sort(gs.begin(), gs.end());
+  return gs;
+}
+
+Scales scales_of(float scale) {
+  Scales sc;
+  sc.scale = scale;
+  sc.inv_scale = 1.0f / scale;
+  for (int c = 0; c < 3; ++c) {
+    const float w = c == 0 ? 1.0f / 3.0f : (c == 1 ? 1.0f / 18.0f : 1.0f / 36.0f);
+    sc.nws[c] = -w * scale;
+  }
+  return sc;
 }
 
 // (Re)capture the chunk graph: chunk_steps steps, each one launch per
-// variant in the mask, for the current launch shape.
-int ensure_graph(lbm_batch* b, int mask) {
+// launch group, for the current launch shape.
+int ensure_graph(lbm_batch* b, const std::vector<std::pair<int, float>>& groups) {
   const int block = launch_block(b), npt = launch_npt(b), steps = chunk_steps(b);
   const int sched = b->opt.schedule == 1 ? 1 : 0;
+  if ((int)groups.size() > kGroups)
+    return set_error(LBM_ERR_INVALID, "more than %d (model, storage, scale) groups in a batch",
+                     kGroups);
   if (b->graph && b->graph_block == block && b->graph_npt == npt && b->graph_steps == steps &&
-      b->graph_mask == mask && b->graph_sched == sched && b->graph_ctas == b->opt.ctas_per_sm &&
-      b->graph_regs == b->opt.regs)
+      b->graph_groups == groups && b->graph_sched == sched &&
+      b->graph_ctas == b->opt.ctas_per_sm && b->graph_regs == b->opt.regs)
     return LBM_OK;
   if (b->graph) {
     cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;
   }
-  int grids[kVariants] = {0};
-  for (int v = 0; v < kVariants; ++v)
-    if (mask & (1 << v)) {
-      int rc = launch_grid(b, v, block, &grids[v]);
-      if (rc) return rc;
-    }
+  std::vector<int> grids(groups.size());
+  for (size_t g = 0; g < groups.size(); ++g) {
+    int rc = launch_grid(b, groups[g].first, block, &grids[g]);
+    if (rc) return rc;
+  }
   CK(cudaStreamBeginCapture(b->capture, cudaStreamCaptureModeThreadLocal));
   for (int j = 0; j < steps; ++j)
-    for (int v = 0; v < kVariants; ++v)
-      if (mask & (1 << v))
-        batch_kernel(v, b->opt.regs)<<<grids[v], block, 0, b->capture>>>(b->d_tab, j, npt);
-  cudaGraph_t g;
-  CK(cudaStreamEndCapture(b->capture, &g));
-  cudaError_t e = cudaGraphInstantiate(&b->graph, g, 0);
-  cudaGraphDestroy(g);
+    for (size_t g = 0; g < groups.size(); ++g)
+      batch_kernel(groups[g].first, b->opt.regs)<<<grids[g], block, 0, b->capture>>>(
+          b->d_tab, (int)g, j, npt, scales_of(groups[g].second));
+  cudaGraph_t gr;
+  CK(cudaStreamEndCapture(b->capture, &gr));
+  cudaError_t e = cudaGraphInstantiate(&b->graph, gr, 0);
+  cudaGraphDestroy(gr);
   if (e != cudaSuccess)
     return set_error(LBM_ERR_CUDA, "batch graph instantiation failed: %s", cudaGetErrorString(e));
   b->graph_block = block;
   b->graph_npt = npt;
   b->graph_steps = steps;
-  b->graph_mask = mask;
+  b->graph_groups = groups;
   b->graph_sched = sched;
   b->graph_ctas = b->opt.ctas_per_sm;
   b->graph_regs = b->opt.regs;
@@ -413,9 +448,9 @@ int grow_images(lbm_batch* b) {
   long long *doff = nullptr, *hoff = nullptr;
   CK(cudaMalloc(&nimg, (size_t)cap * kImages * kArgsBytes));
   CK(cudaMalloc(&dm, (size_t)cap * sizeof(SlotMeta)));
-  CK(cudaMalloc(&doff, (size_t)(cap + kVariants) * sizeof(long long)));
+  CK(cudaMalloc(&doff, (size_t)(cap + kGroups) * sizeof(long long)));
   CK(cudaMallocHost(&hm, (size_t)cap * sizeof(SlotMeta)));
-  CK(cudaMallocHost(&hoff, (size_t)(cap + kVariants) * sizeof(long long)));
+  CK(cudaMallocHost(&hoff, (size_t)(cap + kGroups) * sizeof(long long)));
   CK(cudaStreamSynchronize(b->stream));
   if (b->d_images) {
     CK(cudaMemcpy(nimg, b->d_images, (size_t)b->capacity * kImages * kArgsBytes,
@@ -451,18 +486,17 @@ void retire_completed(lbm_batch* b) {
 int issue_chunk(lbm_batch* b, int steps_offered, long long* lups) {
   const int S = chunk_steps(b);
   *lups = 0;
-  const int mask = pending_mask(b);
-  if (mask == 0) return LBM_OK;
-  int rc = ensure_graph(b, mask);
+  const std::vector<std::pair<int, float>> groups = pending_groups(b);
+  if (groups.empty()) return LBM_OK;
+  int rc = ensure_graph(b, groups);
   if (rc) return rc;
   const int tile = b->graph_block * b->graph_npt;
   CK(cudaEventSynchronize(b->tables_free));  // the pinned tables may be rewritten
   std::memset(b->h_tab->v, 0, sizeof(b->h_tab->v));
   int n = 0, noff = 0;
   long long updates = 0;
-  for (int v = 0; v < kVariants; ++v) {
-    if (!(mask & (1 << v))) continue;
-    VariantList& L = b->h_tab->v[v];
+  for (size_t g = 0; g < groups.size(); ++g) {
+    GroupList& L = b->h_tab->v[g];
     L.slot0 = n;
     L.off0 = noff;
     long long tiles = 0;
@@ -470,7 +504,8 @@ int issue_chunk(lbm_batch* b, int steps_offered, long long* lups) {
       lbm_batch::Member& m = kv.second;
       lbm_domain* d = m.d;
       const long long left = m.target - m.issued;
-      if (left <= 0 || member_variant(d) != v) continue;
+      if (left <= 0 || member_variant(d) != groups[g].first || member_scale(d) != groups[g].second)
+        continue;
       const int active = (int)std::min<long long>(std::min(S, steps_offered), left);
       SlotMeta& sm = b->h_meta[n];
       sm.image_base = m.image_slot * kImages;
@@ -704,7 +739,8 @@ int lbm_batch_step(lbm_batch* b, int steps) {
   if (steps < 0) return set_error(LBM_ERR_INVALID, "negative steps");
   CK(cudaSetDevice(b->opt.device));
   // capture before the first event so that the timed span holds GPU work only
-  int rc = pending_mask(b) ? ensure_graph(b, pending_mask(b)) : LBM_OK;
+  const std::vector<std::pair<int, float>> groups = pending_groups(b);
+  int rc = groups.empty() ? LBM_OK : ensure_graph(b, groups);
   if (rc) return rc;
   CK(cudaEventRecord(b->ev0, b->stream));
   long long total = 0;

@@ -126,21 +126,35 @@ __device__ __forceinline__ RealOf<S> ld(const S* p, int q, float inv_scale) {
 // Boundary value of population q at a node whose donor x - c_q is outside
 // the domain.  d = opp(q) is the reference's "outside" direction; fo is
 // f*_{k-1}[d] at the node itself (arFTemp[d](x) in the reference).
-// Where the populations of a node live (cell = in-plane index of the node).
-// PlaneAddr takes the per-population plane pointers of StepArgs: in the
-// kernel parameter space they are free operands, one address instruction per
-// access.  IndexAddr derives every address from the two lattice bases and
-// the strides: for arguments held in shared memory (the batched kernel),
-// where 38 plane pointers would otherwise be loaded into registers.  It
+// Storage scale factors of the shifted 16-bit forms: f = h * inv_scale + w
+// on load, h = f * scale - w * scale on store (nws[c] = -w * scale for the
+// weight class c).
+struct Scales {
+  float scale, inv_scale;
+  float nws[3];
+};
+
+// Where the populations of a node live (cell = in-plane index of the node)
+// and the storage scales.  PlaneAddr takes the per-population plane
+// pointers and scales of StepArgs: in the kernel parameter space they are
+// free operands, one address instruction per access.  IndexAddr derives
+// every address from the two lattice bases and the strides, and takes the
+// scales from a separate Scales value: for arguments held in shared memory
+// (the batched kernel), where 38 plane pointers and the scales would
+// otherwise be loaded into registers or reloaded per access.  IndexAddr
 // needs Q * qs < 2^31.
 template <class S>
 struct PlaneAddr {
   const StepArgs<S>& a;
   int cell;
-  __device__ __forceinline__ PlaneAddr(const StepArgs<S>& args, int c) : a(args), cell(c) {}
+  __device__ __forceinline__ PlaneAddr(const StepArgs<S>& args, int c, const Scales&)
+      : a(args), cell(c) {}
   __device__ __forceinline__ const S* donor(int q) const { return a.srcd[q] + cell; }
   __device__ __forceinline__ const S* own(int q) const { return a.srcq[q] + cell; }
   __device__ __forceinline__ S* out(int q) const { return a.dstq[q] + cell; }
+  __device__ __forceinline__ float inv_scale() const { return a.inv_scale; }
+  __device__ __forceinline__ float scale() const { return a.scale; }
+  __device__ __forceinline__ float nws(int c) const { return a.nws[c]; }
 };
 
 template <class S>
@@ -148,13 +162,18 @@ struct IndexAddr {
   const S* src;
   S* dst;
   int cell, qs, px, pxnz;
-  __device__ __forceinline__ IndexAddr(const StepArgs<S>& a, int c)
-      : src(a.src), dst(a.dst), cell(c), qs((int)a.qs), px(a.g.px), pxnz(a.g.px * a.g.nz) {}
+  const Scales& sc;
+  __device__ __forceinline__ IndexAddr(const StepArgs<S>& a, int c, const Scales& scales)
+      : src(a.src), dst(a.dst), cell(c), qs((int)a.qs), px(a.g.px), pxnz(a.g.px * a.g.nz),
+        sc(scales) {}
   __device__ __forceinline__ const S* donor(int q) const {
     return src + (cell + q * qs - (cx(q) + px * cz(q) + pxnz * cy(q)));
   }
   __device__ __forceinline__ const S* own(int q) const { return src + (cell + q * qs); }
   __device__ __forceinline__ S* out(int q) const { return dst + (cell + q * qs); }
+  __device__ __forceinline__ float inv_scale() const { return sc.inv_scale; }
+  __device__ __forceinline__ float scale() const { return sc.scale; }
+  __device__ __forceinline__ float nws(int c) const { return sc.nws[c]; }
 };
 
 template <class S, int q>
@@ -274,11 +293,11 @@ __device__ __forceinline__ void pull_struct(RealOf<S> (&f)[Q], const StepArgs<S>
     const bool inside = (unsigned)xs < (unsigned)a.g.nx && (unsigned)ys < (unsigned)a.g.ny &&
                         (unsigned)zs < (unsigned)a.g.nz;
     if (inside && node_type(a.g, xs, ys, zs) != NODE_STRUCT) {
-      f[q] = ld(ad.donor(q), q, a.inv_scale);
+      f[q] = ld(ad.donor(q), q, ad.inv_scale());
     } else if (inside && t == NODE_FLUID) {
-      f[q] = ld(ad.own(opp(q)), opp(q), a.inv_scale);
+      f[q] = ld(ad.own(opp(q)), opp(q), ad.inv_scale());
     } else if (!inside && (t == NODE_INLET || t == NODE_OUTLET)) {
-      const R fo = ld(ad.own(opp(q)), opp(q), a.inv_scale);
+      const R fo = ld(ad.own(opp(q)), opp(q), ad.inv_scale());
       f[q] = boundary_value<S, q>(a, t, fo, y, z);
     } else {
       f[q] = initial_feq<R, q>(R(is.den), R(is.ux), R(is.uy), R(is.uz));
@@ -298,7 +317,7 @@ __device__ __forceinline__ void pull(RealOf<S> (&f)[Q], const StepArgs<S>& a, co
   } else if (!edge) {
     static_for<0, Q>([&](auto qc) {
       constexpr int q = decltype(qc)::value;
-      f[q] = ld(ad.donor(q), q, a.inv_scale);
+      f[q] = ld(ad.donor(q), q, ad.inv_scale());
     });
   } else {
     const int t = node_type(a.g, x, y, z);
@@ -308,9 +327,9 @@ __device__ __forceinline__ void pull(RealOf<S> (&f)[Q], const StepArgs<S>& a, co
       const bool inside = (unsigned)xs < (unsigned)a.g.nx && (unsigned)ys < (unsigned)a.g.ny &&
                           (unsigned)zs < (unsigned)a.g.nz;
       if (inside) {
-        f[q] = ld(ad.donor(q), q, a.inv_scale);
+        f[q] = ld(ad.donor(q), q, ad.inv_scale());
       } else {
-        const RealOf<S> fo = ld(ad.own(opp(q)), opp(q), a.inv_scale);
+        const RealOf<S> fo = ld(ad.own(opp(q)), opp(q), ad.inv_scale());
         f[q] = boundary_value<S, q>(a, t, fo, y, z);
       }
     });
@@ -400,12 +419,13 @@ struct StoreNode {
 // so a domain gets the same bits alone and in a batch (the addressing
 // policy changes where the operands come from, not the arithmetic).
 template <class S, int COLL, bool LES, template <class> class Addr = PlaneAddr>
-__device__ __forceinline__ void step_node(const StepArgs<S>& a, int x, int y, int z) {
+__device__ __forceinline__ void step_node(const StepArgs<S>& a, int x, int y, int z,
+                                          const Scales& sc = Scales{}) {
   using R = RealOf<S>;
   // STRUCT nodes are never streamed, collided or measured (kernel.cu:294,
   // 323, 362, 464, 495, 1105)
   if (a.g.casetype == POISEUILLE && node_type(a.g, x, y, z) == NODE_STRUCT) return;
-  const Addr<S> ad(a, x + a.g.px * (z + a.g.nz * y));
+  const Addr<S> ad(a, x + a.g.px * (z + a.g.nz * y), sc);
   R f[Q];
   pull<S>(f, a, ad, x, y, z);
   PairState<R> ps;
@@ -414,7 +434,7 @@ __device__ __forceinline__ void step_node(const StepArgs<S>& a, int x, int y, in
   const R inv_rho = velocity<R>(ps, ux, uy, uz);
   write_macro<S>(a, x, y, z, ps.rho, ux, uy, uz);
   collide_node<S, COLL, LES, false, R>(f, ps, ux, uy, uz, inv_rho, a, [&](int q, R v) {
-    StoreTraits<S>::store_fma(ad.out(q), v, a.scale, a.nws[wclass(q)]);
+    StoreTraits<S>::store_fma(ad.out(q), v, ad.scale(), ad.nws(wclass(q)));
   });
 }
 
@@ -546,7 +566,7 @@ __global__ void __launch_bounds__(128)
       f[q] = ld(a.src + q * a.qs + cell, q, a.inv_scale);
     });
   } else {
-    pull<S>(f, a, PlaneAddr<S>(a, (int)cell), x, y, z);
+    pull<S>(f, a, PlaneAddr<S>(a, (int)cell, Scales{}), x, y, z);
   }
   long long node;
   if (padded)
@@ -635,9 +655,9 @@ __global__ void __launch_bounds__(64, LBM_PACKED_MIN_BLOCKS) k_step2(const __gri
     });
   } else {
     float fa[Q], fb[Q];
-    pull<S>(fa, a, PlaneAddr<S>(a, cell), x0, y, z);
+    pull<S>(fa, a, PlaneAddr<S>(a, cell, Scales{}), x0, y, z);
     if (two) {
-      pull<S>(fb, a, PlaneAddr<S>(a, cell + 1), x0 + 1, y, z);
+      pull<S>(fb, a, PlaneAddr<S>(a, cell + 1, Scales{}), x0 + 1, y, z);
     } else {
       static_for<0, Q>([&](auto qc) { fb[decltype(qc)::value] = fa[decltype(qc)::value]; });
     }
