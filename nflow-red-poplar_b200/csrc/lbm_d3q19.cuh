@@ -90,6 +90,7 @@ template <>
 struct StoreTraits<float> {
   using R = float;
   static constexpr bool shifted = false;
+  __device__ static __forceinline__ float from_raw(float h, float, float) { return h; }
   __device__ static __forceinline__ float load(const float* p, float, float) { return *p; }
   __device__ static __forceinline__ void store(float* p, float v, float, float) { *p = v; }
   __device__ static __forceinline__ void store_fma(float* p, float v, float, float) { *p = v; }
@@ -98,6 +99,7 @@ template <>
 struct StoreTraits<double> {
   using R = double;
   static constexpr bool shifted = false;
+  __device__ static __forceinline__ double from_raw(double h, double, double) { return h; }
   __device__ static __forceinline__ double load(const double* p, double, double) { return *p; }
   __device__ static __forceinline__ void store(double* p, double v, double, double) { *p = v; }
   __device__ static __forceinline__ void store_fma(double* p, double v, float, float) { *p = v; }
@@ -106,8 +108,12 @@ template <>
 struct StoreTraits<__half> {
   using R = float;
   static constexpr bool shifted = true;
+  // f from the stored value h
+  __device__ static __forceinline__ float from_raw(__half h, float w, float inv_scale) {
+    return fmaf(__half2float(h), inv_scale, w);
+  }
   __device__ static __forceinline__ float load(const __half* p, float w, float inv_scale) {
-    return fmaf(__half2float(*p), inv_scale, w);
+    return from_raw(*p, w, inv_scale);
   }
   __device__ static __forceinline__ void store(__half* p, float v, float w, float scale) {
     *p = __float2half_rn((v - w) * scale);
@@ -122,8 +128,11 @@ template <>
 struct StoreTraits<__nv_bfloat16> {
   using R = float;
   static constexpr bool shifted = true;
+  __device__ static __forceinline__ float from_raw(__nv_bfloat16 h, float w, float inv_scale) {
+    return fmaf(__bfloat162float(h), inv_scale, w);
+  }
   __device__ static __forceinline__ float load(const __nv_bfloat16* p, float w, float inv_scale) {
-    return fmaf(__bfloat162float(*p), inv_scale, w);
+    return from_raw(*p, w, inv_scale);
   }
   __device__ static __forceinline__ void store(__nv_bfloat16* p, float v, float w, float scale) {
     *p = __float2bfloat16_rn((v - w) * scale);

@@ -125,6 +125,8 @@ inline int validate(const Inputval* in, const lbm_options* opt) {
       return set_error(LBM_ERR_INVALID, "unknown init_kind %d", opt->init_kind);
     if (opt->stream_mode != LBM_STREAM_AB)
       return set_error(LBM_ERR_INVALID, "stream_mode %d not supported", opt->stream_mode);
+    if (opt->kernel < LBM_KERNEL_AUTO || opt->kernel > LBM_KERNEL_TMA)
+      return set_error(LBM_ERR_INVALID, "unknown kernel %d", opt->kernel);
     if (!std::isfinite(opt->noise_amp) || !std::isfinite(opt->store_scale) ||
         opt->store_scale < 0.0f)
       return set_error(LBM_ERR_INVALID, "bad noise_amp/store_scale");

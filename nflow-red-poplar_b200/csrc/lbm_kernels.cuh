@@ -414,6 +414,22 @@ struct StoreNode {
   }
 };
 
+// Steps 3-6 of a node whose post-stream populations f are known:
+// macroscopic, side outputs, LES, collision, store of f*.
+template <class S, int COLL, bool LES, class Addr>
+__device__ __forceinline__ void finish_node(const RealOf<S> (&f)[Q], const StepArgs<S>& a,
+                                            const Addr& ad, int x, int y, int z) {
+  using R = RealOf<S>;
+  PairState<R> ps;
+  make_pairs<R>(f, ps);
+  R ux, uy, uz;
+  const R inv_rho = velocity<R>(ps, ux, uy, uz);
+  write_macro<S>(a, x, y, z, ps.rho, ux, uy, uz);
+  collide_node<S, COLL, LES, false, R>(f, ps, ux, uy, uz, inv_rho, a, [&](int q, R v) {
+    StoreTraits<S>::store_fma(ad.out(q), v, ad.scale(), ad.nws(wclass(q)));
+  });
+}
+
 // One fused step of the node (x, y, z): pull + boundary rules, macroscopic,
 // LES, collision, store.  Shared by the single-domain and batched kernels,
 // so a domain gets the same bits alone and in a batch (the addressing
@@ -428,14 +444,7 @@ __device__ __forceinline__ void step_node(const StepArgs<S>& a, int x, int y, in
   const Addr<S> ad(a, x + a.g.px * (z + a.g.nz * y), sc);
   R f[Q];
   pull<S>(f, a, ad, x, y, z);
-  PairState<R> ps;
-  make_pairs<R>(f, ps);
-  R ux, uy, uz;
-  const R inv_rho = velocity<R>(ps, ux, uy, uz);
-  write_macro<S>(a, x, y, z, ps.rho, ux, uy, uz);
-  collide_node<S, COLL, LES, false, R>(f, ps, ux, uy, uz, inv_rho, a, [&](int q, R v) {
-    StoreTraits<S>::store_fma(ad.out(q), v, ad.scale(), ad.nws(wclass(q)));
-  });
+  finish_node<S, COLL, LES>(f, a, ad, x, y, z);
 }
 
 // The fused step.  grid = (ceil(nx/blockDim.x), nz, ny), one thread per node.

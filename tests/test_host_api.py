@@ -134,6 +134,9 @@ def test_argument_errors_are_status_codes():
     iv = pkg.make_inputval(8, tau=0.6)
     bad = pkg.default_options(storage=7)
     assert L.lbm_create(C.byref(iv), C.byref(bad), C.byref(h)) == pkg.LBM_ERR_INVALID
+    bad = pkg.default_options(kernel=9)
+    assert L.lbm_create(C.byref(iv), C.byref(bad), C.byref(h)) == pkg.LBM_ERR_INVALID
+    assert b"kernel" in L.lbm_last_error()
     for fn in ("lbm_initialize", "lbm_sync", "lbm_destroy"):
         assert getattr(L, fn)(None) == pkg.LBM_ERR_INVALID
     assert L.lbm_run_simulation(None, 1) == pkg.LBM_ERR_INVALID
