@@ -126,7 +126,8 @@ enum {
   LBM_ERR_TIMEOUT = -6,   /* a bounded device wait gave up                 */
   LBM_ERR_BUDGET = -7,    /* request exceeds the HBM budget                */
   LBM_ERR_NOT_FINITE = -8,/* input data holds NaN/Inf                      */
-  LBM_ERR_NO_DEVICE = -9  /* no CUDA device / extension not usable         */
+  LBM_ERR_NO_DEVICE = -9, /* no CUDA device / extension not usable         */
+  LBM_ERR_IO = -10        /* an output file could not be written          */
 };
 
 /* Population storage of a domain (all arithmetic is done in FP32 except
@@ -292,6 +293,75 @@ int lbm_get_node_info(lbm_domain* d, int* node_type, int* direction_state);
  *   out[7] = number of non-finite populations (0 when healthy)
  * Synchronises the handle's stream. */
 int lbm_diagnostics(lbm_domain* d, double out[8]);
+
+/* ---------------------------------------------------------------------
+ * Convergence stop (kernel.cu:232-248 prints sum |PrevDen - CurrDen| every
+ * 100 steps; here the same residual ends the run).
+ *
+ * Steps in chunks of check_every (>= 1) until the FP64 residual
+ * sum |rho_k - rho_(k-1)| of the last step of a chunk is <= tol, or
+ * max_steps have been taken.  *steps_taken (may be NULL) = steps of this
+ * call, *residual (may be NULL) = the last residual measured.  The residual
+ * check synchronises the stream once per chunk.  Returns LBM_OK whether or
+ * not the tolerance was reached; compare *residual with tol.
+ * --------------------------------------------------------------------- */
+int lbm_run_until_converged(lbm_domain* d, int max_steps, int check_every, double tol,
+                            int* steps_taken, double* residual);
+
+/* ---------------------------------------------------------------------
+ * Checkpoint / restart through the padded arF (the reference's restart
+ * fields irestart / irst, struct.h:84, only name its output files).
+ *
+ * lbm_save_checkpoint writes a 64-byte header ("LBMCKPT1", nx, ny, nz, 19,
+ * steps done, storage, casetype) and the ghost-padded AoS arF
+ * [ny+2][nz+2][nx+2][19] as float32 (what lbm_export_arF(padded = 1)
+ * returns).  lbm_load_checkpoint checks the extents and imports it as
+ * lbm_import_arF does; the handle's step count restarts at 0 and *step (may
+ * be NULL) receives the count stored in the file.  Continuing a cavity after
+ * a load gives the same populations as never stopping.
+ * --------------------------------------------------------------------- */
+int lbm_save_checkpoint(lbm_domain* d, const char* path);
+int lbm_load_checkpoint(lbm_domain* d, const char* path, long long* step);
+
+/* ---------------------------------------------------------------------
+ * Output files: saveFile (kernel.cu:699-1018).
+ *
+ * LBM_SAVE_VTU (BINARYTYPE, common.h:29): VTK XML UnstructuredGrid with
+ *   appended raw data (UInt64 block headers): Float64 point coordinates,
+ *   Int32 hexahedron connectivity / offsets, UInt8 types (12), Float64
+ *   Velocity (3 components) and Density, Int32 flags Fluid, Fixed Wall,
+ *   Moving Wall, Inlet, Outlet, Struct, in kernel.cu's order and names.
+ *   Written as <dir>/Output%06d.vtu (kernel.cu:706 with SAVE_PATH = dir).
+ * LBM_SAVE_CSV (CSVTYPE, common.h:30): <dir>/result.csv
+ *   ("x,y,z,rho,u,v,w", one line per node in [y][z][x] order) and
+ *   <dir>/section.csv ("y/Y,u": u_x*10 along y at x = z = 49), with
+ *   kernel.cu's printf formats, byte for byte.
+ * --------------------------------------------------------------------- */
+enum { LBM_SAVE_VTU = 0, LBM_SAVE_CSV = 1 };
+
+/* Host writers over caller arrays [ny][nz][nx] (no device involved).
+ * lbm_write_csv: either path may be NULL to skip that file. */
+int lbm_write_vtu(const char* path, int nx, int ny, int nz, const float* den, const float* velx,
+                  const float* vely, const float* velz, const int* node_type);
+int lbm_write_csv(const char* result_path, const char* section_path, int nx, int ny, int nz,
+                  const float* den, const float* velx, const float* vely, const float* velz);
+
+/* Capture the macroscopic state after the last step into a snapshot: a
+ * device-side copy on the handle's stream, then an asynchronous copy to
+ * pinned host memory on a side stream, so the next lbm_run_simulation can
+ * start at once and overlaps the transfer.  The first call also reads the
+ * node types (synchronously) and allocates the snapshot buffers. */
+int lbm_snapshot(lbm_domain* d);
+
+/* Write the last snapshot (waits for its host copy) as savetype into dir
+ * (NULL = "./result/", as SAVE_PATH; created if its parent exists) with
+ * file index `index`.  May run on
+ * another host thread while that thread's partner keeps stepping the same
+ * handle; it must not overlap an lbm_snapshot call on the handle. */
+int lbm_save_snapshot(lbm_domain* d, int savetype, const char* dir, int index);
+
+/* lbm_snapshot + lbm_save_snapshot. */
+int lbm_save_file(lbm_domain* d, int savetype, const char* dir, int index);
 
 /* No counterpart in the reference.  The diagnostics of lbm_diagnostics
  * (same 8 values, same order, FP64) over caller-owned device arrays of n

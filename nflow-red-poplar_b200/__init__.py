@@ -35,6 +35,8 @@ LBM_ERR_TIMEOUT = -6
 LBM_ERR_BUDGET = -7
 LBM_ERR_NOT_FINITE = -8
 LBM_ERR_NO_DEVICE = -9
+LBM_ERR_IO = -10
+SAVE_VTU, SAVE_CSV = 0, 1
 
 STORE_F32, STORE_F16_SHIFT, STORE_BF16_SHIFT, STORE_F64 = 0, 1, 2, 3
 INIT_REFERENCE, INIT_DENSITY_NOISE, INIT_CHANNEL = 0, 1, 2
@@ -145,6 +147,15 @@ def lib():
                                          C.POINTER(C.c_size_t)]
         L.lbm_last_run_ms.argtypes = [vp, C.POINTER(C.c_float)]
         L.lbm_field_diagnostics_static.argtypes = [vp, vp, vp, vp, vp, C.c_longlong, vp, vp]
+        L.lbm_run_until_converged.argtypes = [vp, i32, i32, C.c_double, ip,
+                                              C.POINTER(C.c_double)]
+        L.lbm_write_vtu.argtypes = [C.c_char_p, i32, i32, i32, vp, vp, vp, vp, vp]
+        L.lbm_write_csv.argtypes = [C.c_char_p, C.c_char_p, i32, i32, i32, vp, vp, vp, vp]
+        L.lbm_snapshot.argtypes = [vp]
+        L.lbm_save_snapshot.argtypes = [vp, i32, C.c_char_p, i32]
+        L.lbm_save_file.argtypes = [vp, i32, C.c_char_p, i32]
+        L.lbm_save_checkpoint.argtypes = [vp, C.c_char_p]
+        L.lbm_load_checkpoint.argtypes = [vp, C.c_char_p, C.POINTER(C.c_longlong)]
         L.lbm_batch_default_options.argtypes = [C.POINTER(BatchOptions)]
         L.lbm_batch_create.argtypes = [C.POINTER(BatchOptions), C.POINTER(vp)]
         L.lbm_batch_destroy.argtypes = [vp]
@@ -259,6 +270,34 @@ class Domain:
         check(lib().lbm_diagnostics(self.h, _ptr(out)))
         return out
 
+    def run_until_converged(self, max_steps, check_every, tol):
+        """Step until the residual sum|rho_k - rho_(k-1)| <= tol (checked every
+        check_every steps) or max_steps; returns (steps taken, residual)."""
+        n, r = C.c_int(), C.c_double()
+        check(lib().lbm_run_until_converged(self.h, int(max_steps), int(check_every), float(tol),
+                                            C.byref(n), C.byref(r)))
+        return n.value, r.value
+
+    def save_checkpoint(self, path):
+        check(lib().lbm_save_checkpoint(self.h, os.fsencode(path)))
+
+    def load_checkpoint(self, path):
+        """Restart from a checkpoint file; returns the step count stored in it."""
+        k = C.c_longlong()
+        check(lib().lbm_load_checkpoint(self.h, os.fsencode(path), C.byref(k)))
+        return k.value
+
+    def snapshot(self):
+        check(lib().lbm_snapshot(self.h))
+
+    def save_snapshot(self, savetype, directory=None, index=0):
+        d = None if directory is None else os.fsencode(directory)
+        check(lib().lbm_save_snapshot(self.h, int(savetype), d, int(index)))
+
+    def save_file(self, savetype, directory=None, index=0):
+        d = None if directory is None else os.fsencode(directory)
+        check(lib().lbm_save_file(self.h, int(savetype), d, int(index)))
+
     def device_bytes(self):
         b = C.c_size_t()
         check(lib().lbm_device_bytes(self.h, C.byref(b)))
@@ -268,6 +307,27 @@ class Domain:
         v = C.c_float()
         check(lib().lbm_last_run_ms(self.h, C.byref(v)))
         return v.value
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def write_vtu(path, den, ux, uy, uz, node_type):
+    """kernel.cu's BINARYTYPE file from host fields shaped [ny][nz][nx]."""
+    ny, nz, nx = np.shape(den)
+    f = [_f32(a) for a in (den, ux, uy, uz)]
+    t = np.ascontiguousarray(node_type, dtype=np.int32)
+    check(lib().lbm_write_vtu(os.fsencode(path), nx, ny, nz, *[_ptr(a) for a in f], _ptr(t)))
+
+
+def write_csv(result_path, section_path, den, ux, uy, uz):
+    """kernel.cu's CSVTYPE files (result.csv, section.csv); a path may be None."""
+    ny, nz, nx = np.shape(den)
+    f = [_f32(a) for a in (den, ux, uy, uz)]
+    rp = None if result_path is None else os.fsencode(result_path)
+    sp = None if section_path is None else os.fsencode(section_path)
+    check(lib().lbm_write_csv(rp, sp, nx, ny, nz, *[_ptr(a) for a in f]))
 
 
 def decomposition(iv):

@@ -61,6 +61,15 @@ struct lbm_domain {
   // CUDA graphs of kGraphSteps plain steps, one per starting lattice
   cudaGraphExec_t chunk[2] = {nullptr, nullptr};
   cudaStream_t capture = nullptr;
+  // snapshot of the macroscopic state for the output writers
+  // (lbm_snapshot / lbm_save_snapshot)
+  float* snap_dev = nullptr;       // [4][N] rho, ux, uy, uz on the device
+  float* snap_host = nullptr;      // [4][N] pinned host copy
+  int* snap_type = nullptr;        // [N] node types (host)
+  cudaStream_t snap_stream = nullptr;
+  cudaEvent_t snap_taken = nullptr;   // device copy done (handle stream)
+  cudaEvent_t snap_landed = nullptr;  // host copy done (side stream)
+  bool snap_valid = false;
 };
 
 // steps per captured graph chunk (even, so that a chunk returns the lattices
@@ -359,6 +368,13 @@ inline void free_all(lbm_domain* d) {
     if (d->uz) cudaFree(d->uz);
     if (d->inlet_u) cudaFree(d->inlet_u);
   }
+  if (d->snap_stream) cudaStreamSynchronize(d->snap_stream);
+  if (d->snap_dev) cudaFree(d->snap_dev);
+  if (d->snap_host) cudaFreeHost(d->snap_host);
+  delete[] d->snap_type;
+  if (d->snap_taken) cudaEventDestroy(d->snap_taken);
+  if (d->snap_landed) cudaEventDestroy(d->snap_landed);
+  if (d->snap_stream) cudaStreamDestroy(d->snap_stream);
   if (d->staging) cudaFree(d->staging);
   if (d->flag) cudaFree(d->flag);
   if (d->partial) cudaFree(d->partial);

@@ -4,13 +4,20 @@
 // std::chrono around the run (main.cpp:308-314), read arF back
 // (main.cpp:317) and print direction 9 of the plane k=2 (main.cpp:321-347).
 //
-//   lbm_main [h] [maxitr] [Cs] [srt]
+//   lbm_main [h] [maxitr] [Cs] [srt|mrt] [nwrite] [savetype] [outdir]
 // Defaults are main.cpp's: h=10, maxitr=199, MRT+LES, Re=1000, u_lid=0.1,
-// Smagorinsky constant 0 (main.cpp never assigns it).
+// Smagorinsky constant 0 (main.cpp never assigns it), no result files.
+// With nwrite > 0 it also writes the result files of kernel.cu's loop
+// (kernel.cu:203-228, savetype 0 = VTU, 1 = CSV, into outdir, default
+// ./result/) every nwrite steps and prints kernel.cu's residual line every
+// 100 steps (kernel.cu:232-248).  Each file is written by a host thread from
+// a snapshot while the GPU keeps stepping.
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "../../include/lbm_b200.h"
@@ -22,7 +29,7 @@ int main(int argc, char** argv) {
   in.nx = in.ny = in.nz = in.h;
   in.maxitr = argc > 2 ? std::atoi(argv[2]) : 199;
   in.m_dSmagorinsky = argc > 3 ? (float)std::atof(argv[3]) : 0.0f;
-  const bool srt = argc > 4 && std::strcmp(argv[4], "srt") == 0;
+  const bool srt = argc > 4 && std::strcmp(argv[4], "srt") == 0;  // anything else: MRT+LES
   in.bEnableMRT = !srt;
   in.bEnableLES = !srt;
   in.m_dRefDen = 1.0f;
@@ -30,8 +37,9 @@ int main(int argc, char** argv) {
   in.Re = 1000;
   in.length = (float)(in.nx * in.ny * in.nz);
   in.nu = in.m_dRefVelx * in.h / in.Re;
-  in.nwrite = 10000;
-  in.savetype = 1;
+  in.nwrite = argc > 5 ? std::atoi(argv[5]) : 0;
+  in.savetype = argc > 6 ? std::atoi(argv[6]) : 1;
+  const char* outdir = argc > 7 ? argv[7] : nullptr;
   in.casetype = CAVITY;
   in.m_dTau = 3.0f * in.m_dRefVelx * in.h / in.Re + 0.50f;
   in.dWeps = 3.0f;
@@ -51,7 +59,36 @@ int main(int argc, char** argv) {
   lbm_sync(d);
   auto t0 = std::chrono::high_resolution_clock::now();
   std::printf(" - Running program\n");
-  if (lbm_run_simulation(d, in.maxitr) != LBM_OK || lbm_sync(d) != LBM_OK) {
+  bool ok = true;
+  if (in.nwrite <= 0) {
+    ok = lbm_run_simulation(d, in.maxitr) == LBM_OK && lbm_sync(d) == LBM_OK;
+  } else {
+    // kernel.cu's loop: a residual line every 100 steps, a file every nwrite
+    std::thread writer;
+    int write_rc = LBM_OK;
+    for (int icycle = 0; ok && icycle < in.maxitr;) {
+      const int next_print = (icycle / 100 + 1) * 100, next_write = (icycle / in.nwrite + 1) * in.nwrite;
+      int k = std::min(std::min(next_print, next_write), in.maxitr) - icycle;
+      ok = lbm_run_simulation(d, k) == LBM_OK;
+      icycle += k;
+      if (ok && icycle % 100 == 0) {
+        double diag[8];
+        ok = lbm_diagnostics(d, diag) == LBM_OK;
+        if (ok) std::printf("ITER=%d | ERROR=%.5e\n", icycle, diag[4]);
+      }
+      if (ok && icycle % in.nwrite == 0) {
+        if (writer.joinable()) writer.join();
+        ok = write_rc == LBM_OK && lbm_snapshot(d) == LBM_OK;
+        const int index = icycle / in.nwrite, type = in.savetype;
+        if (ok) writer = std::thread([&write_rc, d, type, outdir, index] {
+            write_rc = lbm_save_snapshot(d, type, outdir, index);
+          });
+      }
+    }
+    if (writer.joinable()) writer.join();
+    ok = ok && write_rc == LBM_OK && lbm_sync(d) == LBM_OK;
+  }
+  if (!ok) {
     std::fprintf(stderr, " - Error: %s\n", lbm_last_error());
     lbm_destroy(d);
     return 1;

@@ -16,6 +16,9 @@
  * SRT / inlet / outlet / struct restatement against the reference itself and
  * to generate tests/golden/kernelcu_*.npz.
  */
+#include <sys/stat.h>
+#include <unistd.h>
+
 #include <string>
 #include <vector>
 
@@ -23,6 +26,11 @@
 #include "kernel.cu" /* reference */
 
 #include "orc_common.h"
+
+/* main.cpp:29-33 defines LBMSolver's constructor and destructor empty;
+ * main.cpp is not built here, so the driver supplies the same. */
+LBMSolver::LBMSolver() {}
+LBMSolver::~LBMSolver() {}
 
 namespace {
 const int kCx[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
@@ -230,6 +238,57 @@ int kref_run(const Inputval* pin, const orc_ext* ext, int nsteps, float* arF, fl
   cudaFree(dDS);
   return 0;
 #undef KR
+}
+
+/* The reference's saveFile (kernel.cu:699-1018) on host fields
+ * [ny][nz][nx]: writes result.csv + section.csv (savetype CSVTYPE) or
+ * result/Output%06d.vtu (BINARYTYPE, index = file number) into workdir.
+ * The cell index array is built as kernel.cu:26-57 builds it inside
+ * runSimulation.  Host code only: needs no GPU.  Returns 0, or -1 when
+ * workdir is not usable. */
+int kref_save_file(const Inputval* pin, const float* den, const float* ux, const float* uy,
+                   const float* uz, const int* ntype, int savetype, int index,
+                   const char* workdir) {
+  Inputval in = *pin;
+  const int nx = in.nx, ny = in.ny, nz = in.nz;
+  const int N = nx * ny * nz;
+  in.length = (float)N;
+  in.irestart = 0;
+  in.nwrite = 1;
+  in.icycle = index;
+  LBMSolver* ps = new LBMSolver();
+  HostNodeData& h = ps->m_HostNode;
+  /* saveFile reads 8 bytes from every 4-byte value of these arrays
+   * (kernel.cu:906-916); one spare element keeps the last read inside the
+   * allocation */
+  for (std::vector<float>* v : {&h.m_dCurrDen, &h.m_dCurrVelx, &h.m_dCurrVely, &h.m_dCurrVelz})
+    v->reserve(N + 2);
+  h.m_dCurrDen.assign(den, den + N);
+  h.m_dCurrVelx.assign(ux, ux + N);
+  h.m_dCurrVely.assign(uy, uy + N);
+  h.m_dCurrVelz.assign(uz, uz + N);
+  h.m_nNodeType.assign(ntype, ntype + N);
+  std::vector<int> arIndex((size_t)N * 8, 0);
+  int k = 0;
+  for (int n = 0; n < N; ++n) {
+    const int slave = nx * nz, x = (n % slave) % nx, y = n / slave, z = (n % slave) / nx;
+    if (x >= nx - 1 || y >= ny - 1 || z >= nz - 1) continue;
+    for (int y2 = y; y2 < y + 2; ++y2)
+      for (int c = 0; c < 4; ++c) {
+        const int x2 = x + (c == 1 || c == 2), z2 = z + (c >= 2);
+        arIndex[k++] = nz * nx * y2 + nx * z2 + x2;
+      }
+  }
+  char cwd[4096];
+  if (!getcwd(cwd, sizeof(cwd)) || chdir(workdir) != 0) {
+    delete ps;
+    return -1;
+  }
+  mkdir("result", 0755); /* SAVE_PATH: saveFile exits when it cannot open the file */
+  saveFile(&in, ps, arIndex, savetype); /* reference */
+  const int rc = chdir(cwd) == 0 ? 0 : -1;
+  delete ps;
+  return rc;
 }
 
 }  // extern "C"

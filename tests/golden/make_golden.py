@@ -8,6 +8,7 @@ are committed so that the tests run without it.
 
     python tests/golden/make_golden.py            # cavity fixtures (CPU)
     python tests/golden/make_golden.py --kernelcu # kernel.cu fixtures (GPU)
+    python tests/golden/make_golden.py --savefile # saveFile CSV fixtures (CPU)
 
 Cases
   cavity10_mrtles_cs0   main.cpp:59-85 as shipped: h=10, Re=1000, u_lid=0.1,
@@ -17,6 +18,10 @@ Cases
   cavity16_noise_cs01   16^3, Re=100, Cs=0.1, seeded density noise 1e-6, 50 steps
   kernelcu_srt32        kernel.cu SRT cavity 32^3, tau=0.6, noise 1e-6, 200 steps
   kernelcu_srtles24     kernel.cu SRT+LES cavity 24^3, Re=200, Cs=0.1, 100 steps
+  savefile/<nx>x<ny>x<nz>_result.csv, _section.csv
+                        the reference's saveFile (kernel.cu:973-1018, host
+                        code of the kernel.cu build, no GPU) on the seeded
+                        fields of tests/test_output.py:fields()
 """
 import argparse
 import os
@@ -83,14 +88,34 @@ def kernelcu_cases():
                                       seed=np.int32(1)))
 
 
+def savefile_cases():
+    import shutil
+    import tempfile
+    from test_output import fields, ref_save
+    out = os.path.join(OUTDIR, "savefile")
+    os.makedirs(out, exist_ok=True)
+    for (nx, ny, nz), seed in (((7, 5, 6), 1), ((52, 4, 51), 2)):
+        den, u, t = fields(nx, ny, nz, seed)
+        tmp = tempfile.mkdtemp()
+        ref_save(tmp, nx, ny, nz, den, u, t, pkg.SAVE_CSV)
+        # the 52x4x51 case is kept for its section line only (small files)
+        names = ("result.csv", "section.csv") if nx < 49 else ("section.csv",)
+        for name in names:
+            shutil.copy(os.path.join(tmp, name), os.path.join(out, f"{nx}x{ny}x{nz}_{name}"))
+        shutil.rmtree(tmp)
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--kernelcu", action="store_true")
+    ap.add_argument("--savefile", action="store_true")
     ap.add_argument("--outdir", default=HERE)
     a = ap.parse_args()
     OUTDIR = a.outdir
     os.makedirs(OUTDIR, exist_ok=True)
     if a.kernelcu:
         kernelcu_cases()
+    elif a.savefile:
+        savefile_cases()
     else:
         poplar_cases()

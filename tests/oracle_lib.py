@@ -57,6 +57,8 @@ def _load(path, prefix):
         L.orc_profile.argtypes = [C.c_float, C.c_int, C.c_int, C.c_int, C.c_int]
     if prefix == "kref":
         L.kref_run.argtypes = [C.POINTER(Inputval), C.POINTER(Ext), C.c_int] + [vp] * 5
+        L.kref_save_file.argtypes = ([C.POINTER(Inputval)] + [vp] * 5 +
+                                     [C.c_int, C.c_int, C.c_char_p])
     _libs[path] = L
     return L
 
