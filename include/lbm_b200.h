@@ -294,6 +294,15 @@ int lbm_get_node_info(lbm_domain* d, int* node_type, int* direction_state);
  * Synchronises the handle's stream. */
 int lbm_diagnostics(lbm_domain* d, double out[8]);
 
+/* Solid voxels (general solid masks: keBoundaryStruct, kernel.cu:659-697,
+ * on any geometry).  mask[ny][nz][nx], nonzero = solid: those nodes become
+ * NODE_STRUCT (in addition to POISEUILLE's pipe wall), are never streamed or
+ * collided and export as zeros; a FLUID node next to one takes half-way
+ * bounce-back; donors outside the box keep the case's own rules.  NULL
+ * removes the mask.  Restarts the domain from its initial state (as
+ * lbm_initialize).  Not for batch members. */
+int lbm_set_solid_mask(lbm_domain* d, const unsigned char* mask);
+
 /* ---------------------------------------------------------------------
  * Convergence stop (kernel.cu:232-248 prints sum |PrevDen - CurrDen| every
  * 100 steps; here the same residual ends the run).

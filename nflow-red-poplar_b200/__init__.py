@@ -155,6 +155,7 @@ def lib():
         L.lbm_save_snapshot.argtypes = [vp, i32, C.c_char_p, i32]
         L.lbm_save_file.argtypes = [vp, i32, C.c_char_p, i32]
         L.lbm_save_checkpoint.argtypes = [vp, C.c_char_p]
+        L.lbm_set_solid_mask.argtypes = [vp, vp]
         L.lbm_load_checkpoint.argtypes = [vp, C.c_char_p, C.POINTER(C.c_longlong)]
         L.lbm_batch_default_options.argtypes = [C.POINTER(BatchOptions)]
         L.lbm_batch_create.argtypes = [C.POINTER(BatchOptions), C.POINTER(vp)]
@@ -277,6 +278,16 @@ class Domain:
         check(lib().lbm_run_until_converged(self.h, int(max_steps), int(check_every), float(tol),
                                             C.byref(n), C.byref(r)))
         return n.value, r.value
+
+    def set_solid_mask(self, mask):
+        """Solid voxels [ny][nz][nx] (nonzero = solid), or None; restarts
+        the domain from its initial state."""
+        if mask is None:
+            check(lib().lbm_set_solid_mask(self.h, None))
+            return
+        m = np.ascontiguousarray(np.asarray(mask) != 0, dtype=np.uint8)
+        assert m.shape == (self.iv.ny, self.iv.nz, self.iv.nx), m.shape
+        check(lib().lbm_set_solid_mask(self.h, _ptr(m)))
 
     def save_checkpoint(self, path):
         check(lib().lbm_save_checkpoint(self.h, os.fsencode(path)))

@@ -192,6 +192,30 @@ int lbm_initialize(lbm_domain* d) {
   return domain_launch_init(d, d->stream);
 }
 
+int lbm_set_solid_mask(lbm_domain* d, const unsigned char* mask) {
+  if (!d) return set_error(LBM_ERR_INVALID, "NULL domain");
+  if (d->pooled) return set_error(LBM_ERR_INVALID, "batch members take no solid mask");
+  int rc = ensure_device(d);
+  if (rc) return rc;
+  if (mask) {
+    if (!d->solid && cudaMalloc(&d->solid, (size_t)d->N) != cudaSuccess) {
+      d->solid = nullptr;
+      return set_error(LBM_ERR_OOM, "solid mask of %lld bytes", d->N);
+    }
+    CK(cudaMemcpyAsync(d->solid, mask, (size_t)d->N, cudaMemcpyHostToDevice, d->stream));
+    d->g.solid = d->solid;
+  } else {
+    d->g.solid = nullptr;
+  }
+  // the step kernel and its captured graphs depend on the geometry
+  for (int i = 0; i < 2; ++i)
+    if (d->chunk[i]) {
+      cudaGraphExecDestroy(d->chunk[i]);
+      d->chunk[i] = nullptr;
+    }
+  return domain_launch_init(d, d->stream);
+}
+
 int lbm_run_simulation(lbm_domain* d, int nsteps) {
   if (!d) return set_error(LBM_ERR_INVALID, "NULL domain");
   if (!d->initialized) return set_error(LBM_ERR_STATE, "lbm_run_simulation before lbm_initialize");

@@ -70,6 +70,7 @@ struct lbm_domain {
   cudaEvent_t snap_taken = nullptr;   // device copy done (handle stream)
   cudaEvent_t snap_landed = nullptr;  // host copy done (side stream)
   bool snap_valid = false;
+  unsigned char* solid = nullptr;  // [N] solid mask on the device (lbm_set_solid_mask)
 };
 
 // steps per captured graph chunk (even, so that a chunk returns the lattices
@@ -239,7 +240,7 @@ int with_model(const lbm_domain* d, F&& f) {
 template <class S, int COLL, bool LES>
 void launch_step(const lbm_domain* d, const StepArgs<S>& a, cudaStream_t st) {
   if constexpr (!std::is_same<S, double>::value) {
-    if (d->g.casetype == POISEUILLE) {
+    if (has_struct(d->g)) {
       // struct geometry: the per-node kernel (its pull checks every donor)
     } else if (d->opt.kernel == LBM_KERNEL_PACKED) {
       const int pairs = (d->g.nx + 1) / 2;
@@ -368,6 +369,7 @@ inline void free_all(lbm_domain* d) {
     if (d->uz) cudaFree(d->uz);
     if (d->inlet_u) cudaFree(d->inlet_u);
   }
+  if (d->solid) cudaFree(d->solid);
   if (d->snap_stream) cudaStreamSynchronize(d->snap_stream);
   if (d->snap_dev) cudaFree(d->snap_dev);
   if (d->snap_host) cudaFreeHost(d->snap_host);
@@ -401,6 +403,7 @@ inline void domain_prepare(lbm_domain* d, const Inputval* pinput, const lbm_opti
   d->g.nz = pinput->nz;
   d->g.px = s.px;
   d->g.casetype = pinput->casetype;
+  d->g.solid = nullptr;
   d->N = s.N;
   d->qs = s.qs;
   d->elem = storage_bytes(d->opt.storage);

@@ -46,14 +46,21 @@ __device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(
 struct Geometry {
   int nx, ny, nz, px;
   int casetype;
+  const unsigned char* solid;  // [ny][nz][nx], nonzero = STRUCT; may be null
 };
+
+// the geometry holds STRUCT nodes: POISEUILLE, or any case with a solid mask
+__host__ __device__ __forceinline__ bool has_struct(const Geometry& g) {
+  return g.casetype == POISEUILLE || g.solid != nullptr;
+}
 
 // node type of keSetNodeType (kernel.cu:1061-1097) / the Initialize codelet
 // (lbm_codelets.cpp:183-201): CAVITY walls and lid; POISEUILLE inlet x=0,
 // outlet x=nx-1, STRUCT outside the circle of radius 20 about (y,z)=(25,25);
 // CHANNEL: inlet x=0, outlet x=nx-1, the four side faces are fixed walls and
-// override inlet/outlet.
+// override inlet/outlet.  A solid mask makes its nodes STRUCT in any case.
 __device__ __forceinline__ int node_type(const Geometry& g, int x, int y, int z) {
+  if (g.solid && g.solid[x + (long long)g.nx * (z + (long long)g.nz * y)]) return NODE_STRUCT;
   int t = NODE_FLUID;
   if (g.casetype == CAVITY) {
     if (y == 0) t = NODE_FIXEDWALL;
@@ -273,12 +280,13 @@ __device__ __forceinline__ R initial_feq(R rd, R ux, R uy, R uz) {
   return mul_rn(mul_rn(weight<R>(q), rd), br);
 }
 
-// POISEUILLE streaming + boundaries (kernel.cu:489-516, 659-697, 566-657):
-// a donor that is STRUCT does not stream (keStreaming skips it); a FLUID node
-// takes half-way bounce-back from its own f*_{opp q} (keBoundaryStruct);
-// inlet/outlet nodes apply their rule to donors outside the domain; every
-// other population is never written in the reference and keeps its
-// initial value.
+// Streaming + boundaries with STRUCT nodes (kernel.cu:489-516, 659-697,
+// 566-657): a donor that is STRUCT does not stream (keStreaming skips it); a
+// FLUID node takes half-way bounce-back from its own f*_{opp q}
+// (keBoundaryStruct); donors outside the domain take the case's rule (in
+// POISEUILLE only inlet/outlet nodes have one); every other population is
+// never written in the reference and keeps its initial value.  POISEUILLE,
+// and any case with a solid mask (the same rules on arbitrary voxels).
 template <class S, class Addr>
 __device__ __forceinline__ void pull_struct(RealOf<S> (&f)[Q], const StepArgs<S>& a, const Addr& ad,
                                             int x, int y, int z) {
@@ -296,7 +304,8 @@ __device__ __forceinline__ void pull_struct(RealOf<S> (&f)[Q], const StepArgs<S>
       f[q] = ld(ad.donor(q), q, ad.inv_scale());
     } else if (inside && t == NODE_FLUID) {
       f[q] = ld(ad.own(opp(q)), opp(q), ad.inv_scale());
-    } else if (!inside && (t == NODE_INLET || t == NODE_OUTLET)) {
+    } else if (!inside &&
+               (a.g.casetype != POISEUILLE || t == NODE_INLET || t == NODE_OUTLET)) {
       const R fo = ld(ad.own(opp(q)), opp(q), ad.inv_scale());
       f[q] = boundary_value<S, q>(a, t, fo, y, z);
     } else {
@@ -312,7 +321,7 @@ __device__ __forceinline__ void pull(RealOf<S> (&f)[Q], const StepArgs<S>& a, co
                                      int y, int z) {
   const bool edge = (x == 0) | (x == a.g.nx - 1) | (y == 0) | (y == a.g.ny - 1) | (z == 0) |
                     (z == a.g.nz - 1);
-  if (a.g.casetype == POISEUILLE) {
+  if (has_struct(a.g)) {
     pull_struct<S>(f, a, ad, x, y, z);
   } else if (!edge) {
     static_for<0, Q>([&](auto qc) {
@@ -440,7 +449,7 @@ __device__ __forceinline__ void step_node(const StepArgs<S>& a, int x, int y, in
   using R = RealOf<S>;
   // STRUCT nodes are never streamed, collided or measured (kernel.cu:294,
   // 323, 362, 464, 495, 1105)
-  if (a.g.casetype == POISEUILLE && node_type(a.g, x, y, z) == NODE_STRUCT) return;
+  if (has_struct(a.g) && node_type(a.g, x, y, z) == NODE_STRUCT) return;
   const Addr<S> ad(a, x + a.g.px * (z + a.g.nz * y), sc);
   R f[Q];
   pull<S>(f, a, ad, x, y, z);
@@ -537,7 +546,7 @@ __global__ void __launch_bounds__(128)
     constexpr int q = decltype(qc)::value;
     f[q] = ld(a.dst + q * a.qs + cell, q, a.inv_scale);
   });
-  if (a.g.casetype == POISEUILLE && node_type(a.g, x, y, z) == NODE_STRUCT) {
+  if (has_struct(a.g) && node_type(a.g, x, y, z) == NODE_STRUCT) {
     write_macro<S>(a, x, y, z, R(0), R(0), R(0), R(0));
     return;
   }
@@ -567,7 +576,7 @@ __global__ void __launch_bounds__(128)
   if (x >= a.g.nx) return;
   const long long cell = x + (long long)a.g.px * (z + (long long)a.g.nz * y);
   R f[Q];
-  if (a.g.casetype == POISEUILLE && node_type(a.g, x, y, z) == NODE_STRUCT) {
+  if (has_struct(a.g) && node_type(a.g, x, y, z) == NODE_STRUCT) {
     static_for<0, Q>([&](auto qc) { f[decltype(qc)::value] = R(0); });
   } else if (post_direct) {
     static_for<0, Q>([&](auto qc) {

@@ -36,6 +36,7 @@
  * Build: oracle/Makefile (-O2 -ffp-contract=off so that no FMA contraction
  * changes the rounding relative to the reference build).
  */
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -188,6 +189,7 @@ struct Solver {
   R Mat[19 * 19], Inv[19 * 19];
   std::vector<Tile> tiles;
   bool has_struct = false;
+  std::vector<unsigned char> solid;  // [N] solid voxels (this project's general masks)
 
   long id(int x, int y, int z) const { return x + (long)nx * (z + (long)nz * y); }
   long pid(int x, int y, int z) const {
@@ -279,6 +281,7 @@ struct Solver {
   /* keSetNodeType (kernel.cu:1046-1097) / Initialize codelet
    * (lbm_codelets.cpp:183-201); CHANNEL is this project's extension. */
   int node_type(int x, int y, int z) const {
+    if (!solid.empty() && solid[id(x, y, z)]) return NODE_STRUCT;
     int t = NODE_FLUID;
     if (in.casetype == CAVITY) {
       if (y == 0) t = NODE_FIXEDWALL;
@@ -616,12 +619,14 @@ struct Solver {
     streaming();
     if (in.casetype == CAVITY) {
       boundary_cavity();
+      if (has_struct) boundary_struct();  // solid mask: keBoundaryStruct's rule
     } else if (in.casetype == POISEUILLE) {
       boundary_struct();
       boundary_inlet();
       boundary_outlet();
     } else if (in.casetype == CHANNEL) {
       boundary_cavity();
+      if (has_struct) boundary_struct();
       boundary_inlet();
       boundary_outlet();
     }
@@ -661,6 +666,21 @@ void set_arF(Solver<R>* s, const double* arF) {
   s->macroscopic();
 }
 
+/* Solid voxels mask[ny][nz][nx] (nonzero = STRUCT; NULL removes them):
+ * the lbm_set_solid_mask counterpart.  Restarts from the initial state. */
+template <typename R>
+void set_solid(Solver<R>* s, const unsigned char* mask) {
+  if (mask)
+    s->solid.assign(mask, mask + s->N);
+  else
+    s->solid.clear();
+  std::fill(s->arF.begin(), s->arF.end(), R(0));
+  std::fill(s->arFT.begin(), s->arFT.end(), R(0));
+  for (auto* v : {&s->den, &s->pden, &s->vx, &s->vy, &s->vz, &s->tau_e})
+    std::fill(v->begin(), v->end(), R(0));
+  s->initialize();
+}
+
 }  // namespace
 
 extern "C" {
@@ -689,6 +709,16 @@ void* orc_create(const Inputval* in, const orc_ext* ext) {
     return nullptr;
   }
   return h;
+}
+
+int orc_set_solid(void* hp, const unsigned char* mask) {
+  Handle* h = (Handle*)hp;
+  if (!h) return -1;
+  if (h->dbl)
+    set_solid(h->sd, mask);
+  else
+    set_solid(h->sf, mask);
+  return 0;
 }
 
 int orc_step(void* hp, int nsteps) {

@@ -79,8 +79,24 @@ extern "C" {
  * Outputs: arF AoS [ny][nz][nx][19] (post-stream, post-boundary),
  * den/ux/uy/uz [ny][nz][nx] (CurrDen/CurrVel), any may be NULL.
  * Returns 0, or the CUDA error code. */
+int kref_run_solid(const Inputval* pin, const orc_ext* ext, int nsteps,
+                   const unsigned char* solid, float* arF, float* den, float* ux, float* uy,
+                   float* uz);
+
 int kref_run(const Inputval* pin, const orc_ext* ext, int nsteps, float* arF, float* den,
              float* ux, float* uy, float* uz) {
+  return kref_run_solid(pin, ext, nsteps, nullptr, arF, den, ux, uy, uz);
+}
+
+/* kref_run with solid voxels: nodes with solid[n] != 0 ([ny][nz][nx]) are
+ * made NODE_STRUCT in the NodeType array the reference kernels read (the
+ * geometry of keSetNodeType otherwise), so that the reference's own
+ * keStreaming / keBoundaryStruct run on arbitrary obstacles.  The
+ * reference applies keBoundaryStruct in the POISEUILLE case only
+ * (kernel.cu:202-212), so only that case is comparable. */
+int kref_run_solid(const Inputval* pin, const orc_ext* ext, int nsteps,
+                   const unsigned char* solid, float* arF, float* den, float* ux, float* uy,
+                   float* uz) {
   Inputval in = *pin;
   const int nx = in.nx, ny = in.ny, nz = in.nz;
   const int N = nx * ny * nz;
@@ -115,7 +131,7 @@ int kref_run(const Inputval* pin, const orc_ext* ext, int nsteps, float* arF, fl
     for (int z = 0; z < nz; ++z)
       for (int x = 0; x < nx; ++x) {
         const int n = x + z * nx + y * nSlave;
-        const int t = node_type_host(&in, x, y, z);
+        const int t = (solid && solid[n]) ? NODE_STRUCT : node_type_host(&in, x, y, z);
         t0[n] = t;
         if (t == NODE_STRUCT) continue;
         float dn = in.m_dRefDen, vx = 0.f, vy = 0.f, vz = 0.f;
@@ -177,6 +193,7 @@ int kref_run(const Inputval* pin, const orc_ext* ext, int nsteps, float* arF, fl
   keInitialNodeDirection<<<gridSize, blockSize>>>(dDS, nNodeSize, dDir, N);
   keSetNodeType<<<gridSize, blockSize>>>(dType, nNodeSize, N, in.casetype);
   KR(cudaGetLastError());
+  if (solid) KR(cudaMemcpy(dType, t0.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
   KR(cudaMemcpy(dF, f0.data(), sizeof(float) * N * 19, cudaMemcpyHostToDevice));
   KR(cudaMemcpy(dDen, d0.data(), sizeof(float) * N, cudaMemcpyHostToDevice));
   KR(cudaMemcpy(dVx, x0.data(), sizeof(float) * N, cudaMemcpyHostToDevice));

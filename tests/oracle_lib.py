@@ -44,6 +44,8 @@ def _load(path, prefix):
         getattr(L, prefix + "_step").argtypes = [vp, C.c_int]
         getattr(L, prefix + "_get").argtypes = [vp] + [vp] * 9
         getattr(L, prefix + "_destroy").argtypes = [vp]
+        if prefix == "orc":
+            L.orc_set_solid.argtypes = [vp, vp]
         getattr(L, prefix + "_decomposition").argtypes = [C.POINTER(Inputval), vp]
         getattr(L, prefix + "_set_move_decomp").argtypes = [C.c_int, vp, vp]
         getattr(L, prefix + "_inverse_mrt").argtypes = [vp, vp]
@@ -57,6 +59,8 @@ def _load(path, prefix):
         L.orc_profile.argtypes = [C.c_float, C.c_int, C.c_int, C.c_int, C.c_int]
     if prefix == "kref":
         L.kref_run.argtypes = [C.POINTER(Inputval), C.POINTER(Ext), C.c_int] + [vp] * 5
+        L.kref_run_solid.argtypes = ([C.POINTER(Inputval), C.POINTER(Ext), C.c_int, vp] +
+                                     [vp] * 5)
         L.kref_save_file.argtypes = ([C.POINTER(Inputval)] + [vp] * 5 +
                                      [C.c_int, C.c_int, C.c_char_p])
     _libs[path] = L
@@ -119,6 +123,11 @@ class Run:
         a = np.ascontiguousarray(arF, np.float64)
         assert self.L.orc_set_arF(self.h, _p(a)) == 0
 
+    def set_solid(self, mask):
+        """Solid voxels [ny][nz][nx] (or None); restarts from the initial state."""
+        m = None if mask is None else np.ascontiguousarray(np.asarray(mask) != 0, np.uint8)
+        assert self.L.orc_set_solid(self.h, _p(m)) == 0
+
     def close(self):
         if self.h:
             getattr(self.L, self.p + "_destroy")(self.h)
@@ -131,8 +140,9 @@ class Run:
             pass
 
 
-def kernelcu_run(iv, nsteps, init_kind=0, seed=1, amp=0.0):
-    """Run the reference's kernel.cu on the GPU; returns arF, den, ux, uy, uz."""
+def kernelcu_run(iv, nsteps, init_kind=0, seed=1, amp=0.0, solid=None):
+    """Run the reference's kernel.cu on the GPU; returns arF, den, ux, uy, uz.
+    solid: optional [ny][nz][nx] voxels made NODE_STRUCT."""
     L = kernelcu_ref_lib()
     if L is None:
         raise RuntimeError("oracle/_ref/libkernelcu_ref.so not built")
@@ -140,7 +150,9 @@ def kernelcu_run(iv, nsteps, init_kind=0, seed=1, amp=0.0):
     ny, nz, nx = iv.ny, iv.nz, iv.nx
     arF = np.empty((ny, nz, nx, 19), np.float32)
     out = [np.empty((ny, nz, nx), np.float32) for _ in range(4)]
-    rc = L.kref_run(C.byref(iv), C.byref(ext), int(nsteps), _p(arF), *[_p(a) for a in out])
+    m = None if solid is None else np.ascontiguousarray(np.asarray(solid) != 0, np.uint8)
+    rc = L.kref_run_solid(C.byref(iv), C.byref(ext), int(nsteps), _p(m), _p(arF),
+                          *[_p(a) for a in out])
     if rc != 0:
         raise RuntimeError(f"kref_run failed with CUDA error {rc}")
     return dict(arF=arF, den=out[0], ux=out[1], uy=out[2], uz=out[3])
