@@ -12,7 +12,13 @@
 // (full: TMA bytes landed; empty: every consumer warp is done with it).
 // Consumers take x-pairs, read their 19 populations from shared memory,
 // evaluate the node arithmetic on packed FP32 lanes (F2) and store f*
-// straight to global memory.
+// straight to global memory.  Rows on a y or z face of the box are all
+// boundary nodes and their consumers take the per-node boundary path
+// uniformly.  In the other rows the x-pairs at the two x faces are left to a
+// boundary warp, which runs the per-node path (global loads) for those few
+// nodes alongside the consumers instead of making half of the consumer warps
+// diverge into it; it reads only the source lattice and writes only its own
+// nodes, so it needs no barrier.
 //
 // The loads never occupy registers or load slots, so the memory
 // parallelism is set by the stage count, not by occupancy: this is what
@@ -41,10 +47,12 @@ struct TmaCfg {
   static constexpr int STAGE_BYTES = Q * BOX_STRIDE;
   static constexpr int STAGES = sizeof(S) == 4 ? 2 : 4;
   static constexpr int CONSUMER_WARPS = TX / 2 * TZ / 32;  // one x-pair per thread
-  static constexpr int THREADS = (CONSUMER_WARPS + 1) * 32;
+  // + one producer warp + one boundary warp
+  static constexpr int THREADS = (CONSUMER_WARPS + 2) * 32;
   static constexpr int SMEM = STAGES * STAGE_BYTES + 2 * STAGES * 8 + 128;
   static_assert(BOX_BYTES % 16 == 0, "TMA box row must be a multiple of 16 bytes");
   static_assert(TXB <= 256 && TZ <= 256, "TMA box dimension limit");
+  static_assert(TZ * 4 <= 32, "the boundary warp covers 4 x-edge candidates per tile row");
 };
 
 // bounded mbarrier waits: try_wait suspends the thread for up to
@@ -118,9 +126,10 @@ __global__ void __launch_bounds__(TmaCfg<S>::THREADS, 1)
     k_step_tma(const __grid_constant__ StepArgs<S> a, const __grid_constant__ CUtensorMap src_map,
                int* __restrict__ err) {
   using C = TmaCfg<S>;
-  extern __shared__ unsigned char smem_raw[];
-  unsigned char* smem =
-      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  // 128-byte aligned stage base, derived by pointer arithmetic on the
+  // __shared__ array so that the compiler keeps the shared address space
+  unsigned char* smem = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::STAGES * C::STAGE_BYTES);
   uint64_t* empty = full + C::STAGES;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -166,6 +175,27 @@ __global__ void __launch_bounds__(TmaCfg<S>::THREADS, 1)
     return;
   }
 
+  if (warp == C::CONSUMER_WARPS + 1) {
+    // ---------------- boundary warp ----------------
+    // lane = 4 * row + candidate; candidates x = 0, 1, nx-2, nx-1 of an
+    // interior row, taken when no consumer pair covers them
+    const int r = lane >> 2, c = lane & 3;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+      const int xt = t % ntx;
+      const int rest = t / ntx;
+      const int zb = rest % nzb;
+      const int y = rest / nzb;
+      const int x0 = xt * C::TX, z = zb * C::TZ + r;
+      if (r >= C::TZ || z >= nz || y == 0 || y == ny - 1 || z == 0 || z == nz - 1) continue;
+      const int x = c < 2 ? c : nx - 4 + c;
+      if (x < x0 || x >= x0 + C::TX || x >= nx || (c >= 2 && x < 2)) continue;
+      const int pair = x & ~1;
+      if (pair >= 1 && pair + 1 <= nx - 2) continue;  // a consumer's interior pair
+      step_node<S, COLL, LES>(a, x, y, z);
+    }
+    return;
+  }
+
   // ---------------- consumers ----------------
   const int r = threadIdx.x / (C::TX / 2);
   const int xl = 2 * (threadIdx.x % (C::TX / 2));
@@ -184,8 +214,8 @@ __global__ void __launch_bounds__(TmaCfg<S>::THREADS, 1)
     const int x = xt * C::TX + xl, z = zb * C::TZ + r;
     if (x < nx && z < nz) {
       const bool two = x + 1 < nx;
-      const bool interior = x >= 1 && x + 1 <= nx - 2 && y >= 1 && y <= ny - 2 && z >= 1 &&
-                            z <= nz - 2;
+      const bool face_row = y == 0 || y == ny - 1 || z == 0 || z == nz - 1;
+      const bool interior = !face_row && x >= 1 && x + 1 <= nx - 2;
       if (interior) {
         const S* stage = reinterpret_cast<const S*>(smem + s * C::STAGE_BYTES);
         const int cell = x + a.g.px * (z + nz * y);
@@ -212,11 +242,12 @@ __global__ void __launch_bounds__(TmaCfg<S>::THREADS, 1)
         collide_node<S, COLL, LES, true, F2>(f, ps, ux, uy, uz, inv_rho, a, [&](int q, F2 v) {
           st_pair<S>(a.dstq[q] + cell, v, q, a.scale);
         });
-      } else {
-        // boundary nodes: the per-node path with the boundary rules (global loads)
+      } else if (face_row) {
+        // a row of boundary nodes: the per-node path with the boundary rules
         step_node<S, COLL, LES>(a, x, y, z);
         if (two) step_node<S, COLL, LES>(a, x + 1, y, z);
       }
+      // else: an x-face pair of an interior row, done by the boundary warp
     }
     __syncwarp();
     if (lane == 0) mbar_arrive(smem_addr(&empty[s]));

@@ -22,10 +22,14 @@ def run(iv, steps, storage=pkg.STORE_F32, kernel=pkg.KERNEL_TMA, kind=1, amp=1e-
     return d
 
 
-@pytest.mark.parametrize("shape", [(48, 20, 18), (130, 9, 11), (256, 24, 7)])
+@pytest.mark.parametrize("shape", [(48, 20, 18), (130, 9, 11), (256, 24, 7), (131, 10, 9),
+                                   (5, 6, 7), (3, 4, 5)])
 @pytest.mark.parametrize("mrt,les", [(True, True), (False, False)])
 def test_tma_cavity_vs_oracle(shape, mrt, les):
-    iv = pkg.make_inputval(*shape, casetype=pkg.CAVITY, re=200.0, u=0.1, mrt=mrt, les=les, cs=0.1,
+    # the tiny boxes (every node on a face) run at a lower Re: at tau ~ 0.5045
+    # SRT rounding differences of 1 ulp grow past the tolerance in 120 steps
+    re = 200.0 if min(shape) >= 7 else 20.0
+    iv = pkg.make_inputval(*shape, casetype=pkg.CAVITY, re=re, u=0.1, mrt=mrt, les=les, cs=0.1,
                            h=shape[0])
     d = run(iv, 120)
     ref = O.Run(iv, init_kind=1, amp=1e-6)
