@@ -108,9 +108,10 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def traffic_from_profile(workload, storage):
-    """dram bytes per launch of k_step from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", f"k_step_{storage}_{workload}.txt")
+def traffic_from_profile(workload, storage, streaming="ab"):
+    """dram bytes per launch of the step kernel from the committed ncu summary."""
+    kern = "k_aa_step" if streaming == "aa" else "k_step"
+    path = os.path.join(ROOT, "profiles", f"{kern}_{storage}_{workload}.txt")
     try:
         for line in open(path):
             if line.startswith("dram_bytes_per_launch:"):
@@ -511,6 +512,8 @@ def main():
     ap.add_argument("--storage", default="f32", choices=["f32", "f16_shift", "bf16_shift", "f64"])
     ap.add_argument("--size", type=int, default=0, help="scale the workload to this nx (profiling)")
     ap.add_argument("--kernel", default="auto", choices=["auto", "scalar", "packed", "tma"])
+    ap.add_argument("--streaming", default="ab", choices=["ab", "aa"],
+                    help="ab: pull between two lattices; aa: AA pattern in one lattice (cavity)")
     ap.add_argument("--report", default="", choices=["", "precision", "batch", "serving"])
     ap.add_argument("--rate", type=float, default=200.0, help="serving: arrivals per second")
     ap.add_argument("--window", type=float, default=60.0, help="serving: wall-clock window (s)")
@@ -567,7 +570,9 @@ def main():
                                   noise_amp=w["amp"], seed=1, device=local,
                                   kernel={"auto": pkg.KERNEL_AUTO, "scalar": pkg.KERNEL_SCALAR,
                                           "packed": pkg.KERNEL_PACKED,
-                                          "tma": pkg.KERNEL_TMA}[args.kernel])
+                                          "tma": pkg.KERNEL_TMA}[args.kernel],
+                                  stream_mode=pkg.STREAM_AA if args.streaming == "aa"
+                                  else pkg.STREAM_AB)
         dom = pkg.Domain(iv, opt)
         dom.set_stream(stream.cuda_stream)
         dom.run(warm)
@@ -601,7 +606,7 @@ def main():
     bpl = 2 * 19 * BYTES[args.storage]
     alg_bytes = bpl * cells
     achieved = alg_bytes / (per_launch_ms / 1e3) / 1e9
-    traffic = traffic_from_profile(args.workload, args.storage)
+    traffic = traffic_from_profile(args.workload, args.storage, args.streaming)
 
     line = {
         "metric": "MLUPS", "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
@@ -610,10 +615,13 @@ def main():
         "config": {"workload": args.workload, "nx": iv.nx, "ny": iv.ny, "nz": iv.nz,
                    "collision": "MRT" if iv.bEnableMRT else "SRT", "les": bool(iv.bEnableLES),
                    "cs": round(float(iv.m_dSmagorinsky), 6), "tau": round(float(iv.m_dTau), 6),
-                   "storage": args.storage, "streaming": "pull A/B, fused boundaries",
+                   "storage": args.storage,
+                   "streaming": ("AA pattern, one lattice in place, fused boundaries"
+                                 if args.streaming == "aa" else "pull A/B, fused boundaries"),
                    "kernel": args.kernel,
-                   "l2": "inputs larger than L2 (2 lattices of %.2f GB vs 126 MB)" %
-                         (19 * BYTES[args.storage] * cells / 1e9),
+                   "l2": "inputs larger than L2 (%d lattice(s) of %.2f GB vs 126 MB)" %
+                         (1 if args.streaming == "aa" else 2,
+                          19 * BYTES[args.storage] * cells / 1e9),
                    "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,

@@ -157,7 +157,9 @@ enum {
 /* Streaming schedule of the fused kernel. */
 enum {
   LBM_STREAM_AB = 0,   /* pull, two population lattices (A/B)             */
-  LBM_STREAM_AA = 1    /* in-place AA pattern, one lattice (half memory)   */
+  LBM_STREAM_AA = 1    /* in-place AA pattern, one lattice (half memory);
+                          CAVITY cases, single domains (not batches, not
+                          with a solid mask)                                */
 };
 
 /* Kernel variant of the fused step (FP32-arithmetic storage formats). */

@@ -192,9 +192,92 @@ int lbm_initialize(lbm_domain* d) {
   return domain_launch_init(d, d->stream);
 }
 
+}  // extern "C"
+
+namespace {
+
+// nsteps AA steps (local and neighbour steps alternate with the layout),
+// in graph chunks where possible; the last two steps write the rho of their
+// input arF (the previous-step density of the residual), then k_aa_macro
+// writes rho and u of the final arF.
+int run_aa(lbm_domain* d, int nsteps) {
+  return with_storage(d->opt.storage, [&](auto tag) -> int {
+    using S = typename decltype(tag)::type;
+    return with_model<S>(d, [&](auto coll, auto les) -> int {
+      constexpr int C = decltype(coll)::value;
+      constexpr bool L = decltype(les)::value;
+      const dim3 b = block_of(d->g.nx), gr = grid_of(d->g, b);
+      auto args = [&](long long k, bool den) {
+        StepArgs<S> a = make_args<S>(d, d->lat[0], d->lat[0], k);
+        if (den) a.den_out = d->den[(k - 1) & 1];  // rho of the step's input arF_{k-1}
+        return a;
+      };
+      auto one = [&](bool den) {
+        const long long k = d->step + 1;
+        k_aa_step<S, C, L><<<gr, b, 0, d->stream>>>(args(k, den), d->cur, d->aa_first ? 1 : 0);
+        d->aa_first = false;
+        d->cur ^= 1;
+        d->step = k;
+      };
+      int left = nsteps;
+      if (d->aa_first && left > 0) {  // never inside a graph: it has its own collision
+        one(left <= 2);
+        --left;
+      }
+      int plain = left > 2 ? left - 2 : 0;
+      if (plain >= 2 * kGraphSteps) {
+        cudaGraphExec_t& g = d->chunk[d->cur];
+        if (!g) {
+          if (!d->capture) CK(cudaStreamCreateWithFlags(&d->capture, cudaStreamNonBlocking));
+          CK(cudaStreamBeginCapture(d->capture, cudaStreamCaptureModeThreadLocal));
+          int cur = d->cur;
+          long long k = d->step;
+          for (int i = 0; i < kGraphSteps; ++i) {
+            ++k;
+            k_aa_step<S, C, L><<<gr, b, 0, d->capture>>>(args(k, false), cur, 0);
+            cur ^= 1;
+          }
+          cudaGraph_t graph;
+          CK(cudaStreamEndCapture(d->capture, &graph));
+          cudaError_t e = cudaGraphInstantiate(&g, graph, 0);
+          cudaGraphDestroy(graph);
+          if (e != cudaSuccess)
+            return set_error(LBM_ERR_CUDA, "graph instantiation failed: %s",
+                             cudaGetErrorString(e));
+        }
+        while (plain >= kGraphSteps) {
+          CK(cudaGraphLaunch(g, d->stream));
+          d->step += kGraphSteps;  // even: the layout is unchanged
+          plain -= kGraphSteps;
+          left -= kGraphSteps;
+        }
+      }
+      while (left > 0) {
+        one(left <= 2);
+        --left;
+      }
+      StepArgs<S> m = make_args<S>(d, d->lat[0], d->lat[0], d->step);
+      m.den_out = d->den[d->step & 1];
+      m.ux_out = d->ux;
+      m.uy_out = d->uy;
+      m.uz_out = d->uz;
+      k_aa_macro<S><<<gr, b, 0, d->stream>>>(m, d->cur);
+      d->post_direct = false;
+      CK(cudaGetLastError());
+      return LBM_OK;
+    });
+  });
+}
+
+}  // namespace
+
+extern "C" {
+
 int lbm_set_solid_mask(lbm_domain* d, const unsigned char* mask) {
   if (!d) return set_error(LBM_ERR_INVALID, "NULL domain");
   if (d->pooled) return set_error(LBM_ERR_INVALID, "batch members take no solid mask");
+  if (d->opt.stream_mode == LBM_STREAM_AA && mask)
+    return set_error(LBM_ERR_INVALID, "solid masks need the pull (A/B) streaming");
   int rc = ensure_device(d);
   if (rc) return rc;
   if (mask) {
@@ -224,6 +307,13 @@ int lbm_run_simulation(lbm_domain* d, int nsteps) {
   int rc = ensure_device(d);
   if (rc) return rc;
   CK(cudaEventRecord(d->ev0, d->stream));
+  if (d->opt.stream_mode == LBM_STREAM_AA) {
+    rc = run_aa(d, nsteps);
+    if (rc) return rc;
+    CK(cudaEventRecord(d->ev1, d->stream));
+    d->last_steps = nsteps;
+    return LBM_OK;
+  }
   rc = with_storage(d->opt.storage, [&](auto tag) -> int {
     using S = typename decltype(tag)::type;
     return with_model<S>(d, [&](auto coll, auto les) -> int {
@@ -326,14 +416,15 @@ int lbm_import_arF(lbm_domain* d, const float* arF, int padded) {
   rc = with_storage(d->opt.storage, [&](auto tag) -> int {
     using S = typename decltype(tag)::type;
     return with_model<S>(d, [&](auto coll, auto les) -> int {
-      StepArgs<S> a = make_args<S>(d, nullptr, d->lat[1], 0);
+      const bool aa = d->opt.stream_mode == LBM_STREAM_AA;
+      StepArgs<S> a = make_args<S>(d, nullptr, d->lat[aa ? 0 : 1], 0);
       a.den_out = d->den[0];
       a.ux_out = d->ux;
       a.uy_out = d->uy;
       a.uz_out = d->uz;
       const dim3 b = block_of(d->g.nx), gr = grid_of(d->g, b);
       k_import<S, decltype(coll)::value, decltype(les)::value>
-          <<<gr, b, 0, d->stream>>>(a, d->staging, padded, (S*)d->lat[0]);
+          <<<gr, b, 0, d->stream>>>(a, d->staging, padded, aa ? nullptr : (S*)d->lat[0]);
       CK(cudaGetLastError());
       return LBM_OK;
     });
@@ -341,6 +432,7 @@ int lbm_import_arF(lbm_domain* d, const float* arF, int padded) {
   if (rc) return rc;
   d->cur = 0;
   d->post_direct = true;
+  d->aa_first = false;
   d->step = 0;
   d->initialized = true;
   d->last_steps = 0;
@@ -359,9 +451,12 @@ int lbm_export_arF(lbm_domain* d, float* arF, int padded) {
   if (padded) CK(cudaMemsetAsync(d->staging, 0, bytes, d->stream));
   rc = with_storage(d->opt.storage, [&](auto tag) -> int {
     using S = typename decltype(tag)::type;
-    StepArgs<S> a = make_args<S>(d, d->lat[d->cur ^ 1], nullptr, d->step);
+    const bool aa = d->opt.stream_mode == LBM_STREAM_AA;
+    StepArgs<S> a = make_args<S>(d, d->lat[aa ? 0 : d->cur ^ 1], nullptr, d->step);
+    const int mode = aa ? (d->cur ? kExportAASwapped : kExportDirect)
+                        : (d->post_direct ? kExportDirect : kExportPull);
     const dim3 b = block_of(d->g.nx), gr = grid_of(d->g, b);
-    k_export<S><<<gr, b, 0, d->stream>>>(a, d->staging, padded, d->post_direct ? 1 : 0);
+    k_export<S><<<gr, b, 0, d->stream>>>(a, d->staging, padded, mode);
     CK(cudaGetLastError());
     return LBM_OK;
   });

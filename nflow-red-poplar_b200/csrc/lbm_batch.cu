@@ -676,6 +676,8 @@ int lbm_batch_add(lbm_batch* b, const Inputval* pinput, const lbm_options* opt,
     return set_error(LBM_ERR_INVALID, "FP64 storage is not supported in batches");
   if (opt && opt->kernel == LBM_KERNEL_PACKED)
     return set_error(LBM_ERR_INVALID, "batches use the one-node-per-thread kernel");
+  if (opt && opt->stream_mode == LBM_STREAM_AA)
+    return set_error(LBM_ERR_INVALID, "batches use the pull (A/B) streaming");
   CK(cudaSetDevice(b->opt.device));
   if (b->free_images.empty() && (rc = grow_images(b))) return rc;
   lbm_domain* d = new lbm_domain();

@@ -71,6 +71,9 @@ struct lbm_domain {
   cudaEvent_t snap_landed = nullptr;  // host copy done (side stream)
   bool snap_valid = false;
   unsigned char* solid = nullptr;  // [N] solid mask on the device (lbm_set_solid_mask)
+  // AA streaming: cur is the layout of lat[0] (0 natural, 1 swapped);
+  // aa_first: the next step is the first after the initial state
+  bool aa_first = false;
 };
 
 // steps per captured graph chunk (even, so that a chunk returns the lattices
@@ -133,8 +136,11 @@ inline int validate(const Inputval* in, const lbm_options* opt) {
       return set_error(LBM_ERR_INVALID, "unknown storage %d", opt->storage);
     if (opt->init_kind < LBM_INIT_REFERENCE || opt->init_kind > LBM_INIT_CHANNEL)
       return set_error(LBM_ERR_INVALID, "unknown init_kind %d", opt->init_kind);
-    if (opt->stream_mode != LBM_STREAM_AB)
+    if (opt->stream_mode != LBM_STREAM_AB && opt->stream_mode != LBM_STREAM_AA)
       return set_error(LBM_ERR_INVALID, "stream_mode %d not supported", opt->stream_mode);
+    if (opt->stream_mode == LBM_STREAM_AA && in->casetype != CAVITY)
+      return set_error(LBM_ERR_INVALID,
+                       "AA streaming is implemented for the cavity (casetype %d) only", CAVITY);
     if (opt->kernel < LBM_KERNEL_AUTO || opt->kernel > LBM_KERNEL_TMA)
       return set_error(LBM_ERR_INVALID, "unknown kernel %d", opt->kernel);
     if (!std::isfinite(opt->noise_amp) || !std::isfinite(opt->store_scale) ||
@@ -167,7 +173,8 @@ inline Sizes sizes_of(const Inputval* in) {
 inline size_t footprint(const Inputval* in, const lbm_options* opt) {
   const Sizes s = sizes_of(in);
   const size_t e = storage_bytes(opt ? opt->storage : LBM_STORE_F32);
-  size_t b = 2 * (size_t)Q * s.qs * e;  // lattices
+  const int lattices = opt && opt->stream_mode == LBM_STREAM_AA ? 1 : 2;
+  size_t b = lattices * (size_t)Q * s.qs * e;  // lattices
   b += 5 * (size_t)s.N * sizeof(float);  // den[2], ux, uy, uz
   b += 15 * (size_t)s.P * sizeof(float); // inlet profile + planes
   return b;
@@ -285,6 +292,10 @@ inline TensorMapEncodeFn tensor_map_encoder() {
 // kernel option then falls back to the scalar kernel) for FP64 storage.
 template <class S>
 int domain_tensor_maps(lbm_domain* d, int sm_count) {
+  if (d->opt.stream_mode == LBM_STREAM_AA) {  // the TMA kernel is a pull (A/B) kernel
+    d->tmap_ok = false;
+    return LBM_OK;
+  }
   if constexpr (std::is_same<S, double>::value) {
     d->tmap_ok = false;
     return LBM_OK;
@@ -423,7 +434,8 @@ int domain_alloc_state(lbm_domain* d, Alloc&& alloc) {
   const size_t nb = (size_t)d->N * sizeof(float);
   const size_t pb = (size_t)d->g.ny * d->g.nz * sizeof(float);
   int rc;
-  if ((rc = alloc(&d->lat[0], lat_bytes)) || (rc = alloc(&d->lat[1], lat_bytes)) ||
+  const bool aa = d->opt.stream_mode == LBM_STREAM_AA;  // one lattice, in place
+  if ((rc = alloc(&d->lat[0], lat_bytes)) || (!aa && (rc = alloc(&d->lat[1], lat_bytes))) ||
       (rc = alloc((void**)&d->den[0], nb)) || (rc = alloc((void**)&d->den[1], nb)) ||
       (rc = alloc((void**)&d->ux, nb)) || (rc = alloc((void**)&d->uy, nb)) ||
       (rc = alloc((void**)&d->uz, nb)) || (rc = alloc((void**)&d->inlet_u, pb)) ||
@@ -439,7 +451,8 @@ inline size_t domain_state_bytes(const Inputval* in, const lbm_options* opt) {
   auto r = [](size_t b) { return (b + 255) / 256 * 256; };
   const size_t e = storage_bytes(opt ? opt->storage : LBM_STORE_F32);
   const size_t nb = (size_t)s.N * sizeof(float), pb = (size_t)s.P * sizeof(float);
-  return 2 * r((size_t)Q * s.qs * e) + 5 * r(nb) + 3 * r(pb) + 2 * r(6 * pb);
+  const int lattices = opt && opt->stream_mode == LBM_STREAM_AA ? 1 : 2;
+  return lattices * r((size_t)Q * s.qs * e) + 5 * r(nb) + 3 * r(pb) + 2 * r(6 * pb);
 }
 
 // Upload the channel inlet profile u_x(y,z) = u_max 16 eta(1-eta) zeta(1-zeta).
@@ -482,14 +495,17 @@ inline int domain_launch_init(lbm_domain* d, cudaStream_t st) {
   int rc = with_storage(d->opt.storage, [&](auto tag) -> int {
     using S = typename decltype(tag)::type;
     return with_model<S>(d, [&](auto coll, auto les) -> int {
-      StepArgs<S> a = make_args<S>(d, nullptr, d->lat[1], 0);
+      // pull: arF_0 in lat[1], its collision in lat[0]; AA: arF_0 in the
+      // natural layout of lat[0], collided by the first step
+      const bool aa = d->opt.stream_mode == LBM_STREAM_AA;
+      StepArgs<S> a = make_args<S>(d, nullptr, d->lat[aa ? 0 : 1], 0);
       a.den_out = d->den[0];
       a.ux_out = d->ux;
       a.uy_out = d->uy;
       a.uz_out = d->uz;
       const dim3 b = block_of(d->g.nx), gr = grid_of(d->g, b);
       k_init<S, decltype(coll)::value, decltype(les)::value>
-          <<<gr, b, 0, st>>>(a, (S*)d->lat[0], ip);
+          <<<gr, b, 0, st>>>(a, aa ? nullptr : (S*)d->lat[0], ip);
       CK(cudaGetLastError());
       return LBM_OK;
     });
@@ -497,6 +513,7 @@ inline int domain_launch_init(lbm_domain* d, cudaStream_t st) {
   if (rc) return rc;
   d->cur = 0;
   d->post_direct = true;
+  d->aa_first = d->opt.stream_mode == LBM_STREAM_AA;
   d->step = 0;
   d->initialized = true;
   d->last_steps = 0;

@@ -505,13 +505,14 @@ __global__ void __launch_bounds__(128)
   });
   store_all<S>(a, f, cell);  // post-stream lattice
   write_macro<S>(a, x, y, z, rd, ux, uy, uz);
+  if (!collided) return;  // AA streaming: the first step collides
   // the first step collides with the rho, u that Initialize stored
   PairState<R> ps;
   make_pairs<R>(f, ps);
   ps.rho = rd;
-  ps.jx = rd * ux;
-  ps.jy = rd * uy;
-  ps.jz = rd * uz;
+  ps.jx = mul_rn(rd, ux);  // rounded products: the AA form repeats them exactly
+  ps.jy = mul_rn(rd, uy);
+  ps.jz = mul_rn(rd, uz);
   collide_node<S, COLL, LES, false, R>(f, ps, ux, uy, uz, vrcp(rd), a,
                                        StoreNode<S>{collided, a.qs, cell, a.scale});
 }
@@ -553,12 +554,172 @@ __global__ void __launch_bounds__(128)
   R rho, ux, uy, uz;
   macroscopic<R>(f, rho, ux, uy, uz);  // CurrDen / CurrVel in the codelet's order
   write_macro<S>(a, x, y, z, rho, ux, uy, uz);
+  if (!collided) return;  // AA streaming: the next step collides
   PairState<R> ps;
   make_pairs<R>(f, ps);
   const R inv_rho = velocity<R>(ps, ux, uy, uz);
   collide_node<S, COLL, LES, false, R>(f, ps, ux, uy, uz, inv_rho, a,
                                        StoreNode<S>{collided, a.qs, cell, a.scale});
 }
+
+// ------------------------------------------------------------------ //
+// AA streaming (in place, one lattice), for the cavity geometry.
+//
+// Two layouts alternate.  "Natural": slot (x, q) holds the post-stream,
+// post-boundary f_q(x) (arF).  A local step reads its node's natural
+// slots, collides and writes f*_q into its own slot (x, opp q): the layout
+// becomes "swapped", in which arF_q(x) = f*_q(x - c_q) sits in slot
+// (x - c_q, opp q).  A neighbour step reads those slots, collides and writes
+// f*_q(x) into (x + c_q, q), the natural slot of its destination: the
+// layout is natural again.  Each neighbour-step thread reads and writes the
+// same 19 slots, so the update is race-free in place.  Wall rules (on-node
+// bounce-back with the lid term, lbm_codelets.cpp:373-395) act where a slot
+// of the neighbour step lies outside the box: a donor x - c_q outside reads
+// the node's own f*_{opp q} from (x, q); a destination x + c_q outside
+// writes the wall value of population opp q into the node's natural slot
+// (x, opp q).  A local step needs no boundary logic.  Same node arithmetic
+// as the pull step; the two kernels agree to within a few FP32 roundings
+// (the compiler may fuse a multiply-add differently in each).
+// ------------------------------------------------------------------ //
+
+// arF of node (x, y, z) from the swapped layout
+template <class S>
+__device__ __forceinline__ void aa_pull_swapped(RealOf<S> (&f)[Q], const StepArgs<S>& a, int x,
+                                                int y, int z, int cell) {
+  const bool edge = (x == 0) | (x == a.g.nx - 1) | (y == 0) | (y == a.g.ny - 1) | (z == 0) |
+                    (z == a.g.nz - 1);
+  if (!edge) {
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      f[q] = ld(a.srcq[opp(q)] + (cell - a.off[q]), q, a.inv_scale);
+    });
+  } else {
+    const int t = node_type(a.g, x, y, z);
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      const int xs = x - cx(q), ys = y - cy(q), zs = z - cz(q);
+      const bool inside = (unsigned)xs < (unsigned)a.g.nx && (unsigned)ys < (unsigned)a.g.ny &&
+                          (unsigned)zs < (unsigned)a.g.nz;
+      if (inside) {
+        f[q] = ld(a.srcq[opp(q)] + (cell - a.off[q]), q, a.inv_scale);
+      } else {
+        const RealOf<S> fo = ld(a.srcq[q] + cell, q, a.inv_scale);  // own f*_{opp q}
+        f[q] = boundary_value<S, q>(a, t, fo, y, z);
+      }
+    });
+  }
+}
+
+// the wall value of population opp(d) at a node of type t from its f*_d:
+// boundary_value<S, opp d> with a run-time d (cavity node types)
+template <class S>
+__device__ __forceinline__ RealOf<S> aa_wall(const StepArgs<S>& a, int t, RealOf<S> fo, int d) {
+  using R = RealOf<S>;
+  if (t != NODE_MOVINGWALL) return fo;
+  R eu = add_rn(add_rn(mul_rn(R(cx(d)), a.ulx), mul_rn(R(cy(d)), a.uly)), mul_rn(R(cz(d)), a.ulz));
+  R term = mul_rn(mul_rn(mul_rn(R(6), weight<R>(d)), a.rho0), eu);
+  return sub_rn(fo, term);
+}
+
+// out(q) of the local step: the node's own slot opp(q)
+template <class S>
+struct AASwapOut {
+  const StepArgs<S>& a;
+  int cell;
+  __device__ __forceinline__ S* out(int q) const { return a.dstq[opp(q)] + cell; }
+  __device__ __forceinline__ float scale() const { return a.scale; }
+  __device__ __forceinline__ float nws(int c) const { return a.nws[c]; }
+};
+
+// One AA step; neighbor = 0: local step (natural -> swapped), 1: neighbour
+// step (swapped -> natural).  first = 1 for the first step after the
+// initial state: it collides with the rho, u that Initialize stored, as
+// k_init does for the pull form.  a.src = a.dst = the lattice.
+template <class S, int COLL, bool LES>
+__global__ void __launch_bounds__(128)
+    k_aa_step(const __grid_constant__ StepArgs<S> a, int neighbor, int first) {
+  using R = RealOf<S>;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int z = blockIdx.y, y = blockIdx.z;
+  if (x >= a.g.nx) return;
+  const int cell = x + a.g.px * (z + a.g.nz * y);
+  R f[Q];
+  if (!neighbor) {
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      f[q] = ld(a.srcq[q] + cell, q, a.inv_scale);
+    });
+    const AASwapOut<S> ad{a, cell};
+    if (!first) {
+      finish_node<S, COLL, LES>(f, a, ad, x, y, z);
+    } else {
+      const int t = node_type(a.g, x, y, z);
+      const InitState is = initial_state(a.g, a.init_kind, a.seed, a.noise_amp, (float)a.rho0,
+                                         (float)a.ulx, (float)a.uly, (float)a.ulz, a.inlet_u, x,
+                                         y, z, t);
+      const R rd = R(is.den), ux = R(is.ux), uy = R(is.uy), uz = R(is.uz);
+      write_macro<S>(a, x, y, z, rd, ux, uy, uz);
+      PairState<R> ps;
+      make_pairs<R>(f, ps);
+      ps.rho = rd;
+      ps.jx = mul_rn(rd, ux);
+      ps.jy = mul_rn(rd, uy);
+      ps.jz = mul_rn(rd, uz);
+      collide_node<S, COLL, LES, false, R>(f, ps, ux, uy, uz, vrcp(rd), a, [&](int q, R v) {
+        StoreTraits<S>::store_fma(ad.out(q), v, ad.scale(), ad.nws(wclass(q)));
+      });
+    }
+    return;
+  }
+  aa_pull_swapped<S>(f, a, x, y, z, cell);
+  const bool edge = (x == 0) | (x == a.g.nx - 1) | (y == 0) | (y == a.g.ny - 1) | (z == 0) |
+                    (z == a.g.nz - 1);
+  const int t = edge ? node_type(a.g, x, y, z) : NODE_FLUID;
+  PairState<R> ps;
+  make_pairs<R>(f, ps);
+  R ux, uy, uz;
+  const R inv_rho = velocity<R>(ps, ux, uy, uz);
+  write_macro<S>(a, x, y, z, ps.rho, ux, uy, uz);
+  collide_node<S, COLL, LES, false, R>(f, ps, ux, uy, uz, inv_rho, a, [&](int q, R v) {
+    const int xt = x + cx(q), yt = y + cy(q), zt = z + cz(q);
+    const bool inside = !edge || ((unsigned)xt < (unsigned)a.g.nx &&
+                                  (unsigned)yt < (unsigned)a.g.ny && (unsigned)zt < (unsigned)a.g.nz);
+    if (inside)
+      StoreTraits<S>::store_fma(a.dstq[q] + (cell + a.off[q]), v, a.scale, a.nws[wclass(q)]);
+    else
+      StoreTraits<S>::store_fma(a.dstq[opp(q)] + cell, aa_wall<S>(a, t, v, q), a.scale,
+                                a.nws[wclass(q)]);
+  });
+}
+
+// rho and u of arF in the current AA layout (swapped = 1 after a local
+// step), written through a.den_out / a.ux_out...: the same arithmetic as the
+// step kernels' side outputs
+template <class S>
+__global__ void __launch_bounds__(128) k_aa_macro(const __grid_constant__ StepArgs<S> a,
+                                                  int swapped) {
+  using R = RealOf<S>;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int z = blockIdx.y, y = blockIdx.z;
+  if (x >= a.g.nx) return;
+  const int cell = x + a.g.px * (z + a.g.nz * y);
+  R f[Q];
+  if (swapped) {
+    aa_pull_swapped<S>(f, a, x, y, z, cell);
+  } else {
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      f[q] = ld(a.srcq[q] + cell, q, a.inv_scale);
+    });
+  }
+  PairState<R> ps;
+  make_pairs<R>(f, ps);
+  R ux, uy, uz;
+  velocity<R>(ps, ux, uy, uz);
+  write_macro<S>(a, x, y, z, ps.rho, ux, uy, uz);
+}
+
+enum { kExportPull = 0, kExportDirect = 1, kExportAASwapped = 2 };
 
 // ------------------------------------------------------------------ //
 // Export of arF_k into a device AoS buffer.  post_direct: a.src already
@@ -569,7 +730,7 @@ __global__ void __launch_bounds__(128)
 template <class S>
 __global__ void __launch_bounds__(128)
     k_export(const __grid_constant__ StepArgs<S> a, float* __restrict__ aos, int padded,
-             int post_direct) {
+             int mode) {
   using R = RealOf<S>;
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int z = blockIdx.y, y = blockIdx.z;
@@ -578,11 +739,13 @@ __global__ void __launch_bounds__(128)
   R f[Q];
   if (has_struct(a.g) && node_type(a.g, x, y, z) == NODE_STRUCT) {
     static_for<0, Q>([&](auto qc) { f[decltype(qc)::value] = R(0); });
-  } else if (post_direct) {
+  } else if (mode == kExportDirect) {
     static_for<0, Q>([&](auto qc) {
       constexpr int q = decltype(qc)::value;
       f[q] = ld(a.src + q * a.qs + cell, q, a.inv_scale);
     });
+  } else if (mode == kExportAASwapped) {
+    aa_pull_swapped<S>(f, a, x, y, z, (int)cell);
   } else {
     pull<S>(f, a, PlaneAddr<S>(a, (int)cell, Scales{}), x, y, z);
   }

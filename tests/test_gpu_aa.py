@@ -1,0 +1,114 @@
+"""AA-pattern streaming (one lattice, in place) against the pull (A/B) form
+and the oracle.
+
+The AA steps evaluate the same node arithmetic on the same populations.  The
+first step after the initial state gives the same bits as the pull form;
+later steps differ by FP32 rounding (the two kernels may fuse a
+multiply-add differently; ~1e-7 after a few steps, ~1e-6 after a hundred), so
+they are compared at the 1e-5 parity tolerance, which both also meet against
+the oracle.  The 16-bit
+forms also round the lid's bounce-back value at a different point and are
+compared within the 16-bit tolerance."""
+import numpy as np
+import pytest
+
+import oracle_lib as O
+
+pkg = O.pkg
+pytestmark = pytest.mark.gpu
+CLOSE = 1e-5
+
+
+def cavity(nx, ny, nz, re=400.0, mrt=True, les=True):
+    return pkg.make_inputval(nx, ny, nz, casetype=pkg.CAVITY, re=re, u=0.1, mrt=mrt, les=les,
+                             cs=0.1, h=nx)
+
+
+def pair(iv, storage=pkg.STORE_F32):
+    o = dict(storage=storage, init_kind=pkg.INIT_DENSITY_NOISE, noise_amp=1e-6)
+    return (pkg.Domain(iv, pkg.default_options(stream_mode=pkg.STREAM_AA, **o)),
+            pkg.Domain(iv, pkg.default_options(stream_mode=pkg.STREAM_AB, **o)))
+
+
+@pytest.mark.parametrize("mrt,les", [(True, True), (False, False), (True, False)])
+def test_aa_matches_pull(mrt, les):
+    aa, ab = pair(cavity(34, 21, 19, mrt=mrt, les=les))
+    np.testing.assert_array_equal(aa.export_arF(), ab.export_arF())  # initial state
+    aa.run(1)
+    ab.run(1)
+    np.testing.assert_array_equal(aa.export_arF(), ab.export_arF())  # first step: same bits
+    for steps in (1, 2, 37, 70, 3):  # odd and even totals; 70 uses graph chunks
+        aa.run(steps)
+        ab.run(steps)
+        assert aa.steps() == ab.steps()
+        assert O.rel_field_err(aa.export_arF(), ab.export_arF()) <= CLOSE
+        pa, pb = aa.export_arF(padded=True), ab.export_arF(padded=True)
+        assert O.rel_field_err(pa, pb) <= CLOSE
+        assert not pa[0].any() and not pa[:, 0].any()  # ghost layer
+        den_a, *u_a = aa.macroscopic()
+        den_b, *u_b = ab.macroscopic()
+        assert O.rel_field_err(den_a, den_b) <= CLOSE
+        assert O.rel_vel_err(u_a, u_b) <= CLOSE
+        da, db = aa.diagnostics(), ab.diagnostics()
+        assert abs(da[0] - db[0]) <= 1e-6 * abs(db[0])  # mass
+        assert da[7] == db[7] == 0
+
+
+def test_aa_import_and_checkpoint_continue(tmp_path):
+    aa, ab = pair(cavity(24, 20, 22))
+    ab.run(41)
+    arF = ab.export_arF(padded=True)
+    aa.import_arF(arF, padded=True)
+    ab2 = pkg.Domain(cavity(24, 20, 22))
+    ab2.import_arF(arF, padded=True)
+    aa.run(65)
+    ab2.run(65)
+    assert O.rel_field_err(aa.export_arF(), ab2.export_arF()) <= CLOSE
+    aa.save_checkpoint(tmp_path / "aa.bin")
+    c = pkg.Domain(cavity(24, 20, 22), pkg.default_options(stream_mode=pkg.STREAM_AA))
+    c.load_checkpoint(tmp_path / "aa.bin")
+    c.run(10)
+    aa.run(10)
+    # the restart begins with a local step where the continued run takes a
+    # neighbour step: the same arithmetic in another kernel, rounding apart
+    assert O.rel_field_err(c.export_arF(), aa.export_arF()) <= CLOSE
+
+
+@pytest.mark.parametrize("storage", [pkg.STORE_F16_SHIFT, pkg.STORE_BF16_SHIFT])
+def test_aa_16bit_close_to_pull(storage):
+    aa, ab = pair(cavity(40, 32, 28), storage)
+    aa.run(150)
+    ab.run(150)
+    ua = np.stack(aa.macroscopic()[1:])
+    ub = np.stack(ab.macroscopic()[1:])
+    tol = 1e-3 if storage == pkg.STORE_F16_SHIFT else 1e-2
+    assert np.abs(ua - ub).max() / np.abs(ub).max() <= tol
+
+
+def test_aa_vs_oracle():
+    iv = cavity(30, 26, 22)
+    aa = pkg.Domain(iv, pkg.default_options(stream_mode=pkg.STREAM_AA,
+                                            init_kind=pkg.INIT_DENSITY_NOISE, noise_amp=1e-6))
+    ref = O.Run(iv, init_kind=1, amp=1e-6)
+    aa.run(101)
+    ref.step(101)
+    r = ref.fields()
+    den, ux, uy, uz = aa.macroscopic()
+    assert O.rel_field_err(den, r["den"]) <= 1e-5
+    assert O.rel_vel_err((ux, uy, uz), (r["ux"], r["uy"], r["uz"])) <= 1e-5
+
+
+def test_aa_halves_the_lattice_memory_and_rejects_other_cases():
+    iv = cavity(64, 64, 64)
+    aa, ab = pair(iv)
+    lat = 19 * 64 * 64 * 64 * 4
+    assert ab.device_bytes() - aa.device_bytes() >= lat
+    ch = pkg.make_inputval(32, 16, 16, casetype=pkg.CHANNEL, tau=0.6, u=0.05)
+    with pytest.raises(pkg.LbmError):
+        pkg.Domain(ch, pkg.default_options(stream_mode=pkg.STREAM_AA))
+    with pytest.raises(pkg.LbmError):
+        aa.set_solid_mask(np.ones((64, 64, 64), bool))
+    b = pkg.Batch(hbm_budget=64 << 20)
+    with pytest.raises(pkg.LbmError):
+        b.add(cavity(16, 16, 16), pkg.default_options(stream_mode=pkg.STREAM_AA), 4)
+    b.close()
