@@ -207,14 +207,26 @@ int run_aa(lbm_domain* d, int nsteps) {
       constexpr int C = decltype(coll)::value;
       constexpr bool L = decltype(les)::value;
       const dim3 b = block_of(d->g.nx), gr = grid_of(d->g, b);
-      auto args = [&](long long k, bool den) {
+      // slot tables of the two step kinds (see k_aa_step)
+      auto args = [&](long long k, bool den, int neighbor) {
         StepArgs<S> a = make_args<S>(d, d->lat[0], d->lat[0], k);
+        S* lat = (S*)d->lat[0];
+        for (int q = 0; q < Q; ++q) {
+          if (!neighbor) {
+            a.srcd[q] = lat + q * d->qs;
+            a.dstq[q] = lat + opp(q) * d->qs;
+          } else {
+            a.srcd[q] = lat + (opp(q) * d->qs - a.off[q]);
+            a.dstq[q] = lat + (q * d->qs + a.off[q]);
+          }
+        }
         if (den) a.den_out = d->den[(k - 1) & 1];  // rho of the step's input arF_{k-1}
         return a;
       };
       auto one = [&](bool den) {
         const long long k = d->step + 1;
-        k_aa_step<S, C, L><<<gr, b, 0, d->stream>>>(args(k, den), d->cur, d->aa_first ? 1 : 0);
+        k_aa_step<S, C, L><<<gr, b, 0, d->stream>>>(args(k, den, d->cur), d->cur,
+                                                    d->aa_first ? 1 : 0);
         d->aa_first = false;
         d->cur ^= 1;
         d->step = k;
@@ -234,7 +246,7 @@ int run_aa(lbm_domain* d, int nsteps) {
           long long k = d->step;
           for (int i = 0; i < kGraphSteps; ++i) {
             ++k;
-            k_aa_step<S, C, L><<<gr, b, 0, d->capture>>>(args(k, false), cur, 0);
+            k_aa_step<S, C, L><<<gr, b, 0, d->capture>>>(args(k, false, cur), cur, 0);
             cur ^= 1;
           }
           cudaGraph_t graph;

@@ -621,12 +621,17 @@ __device__ __forceinline__ RealOf<S> aa_wall(const StepArgs<S>& a, int t, RealOf
   return sub_rn(fo, term);
 }
 
-// out(q) of the local step: the node's own slot opp(q)
+// Slot addresses of an AA step, set per step in the kernel parameters so
+// that an interior node needs one address operation per access:
+//   local step:      a.srcd[q] = plane q,                 a.dstq[q] = plane opp q
+//   neighbour step:  a.srcd[q] = plane opp q, minus off_q, a.dstq[q] = plane q, plus off_q
+// (arF_q(x) is read at srcd[q] + cell, f*_q(x) written at dstq[q] + cell);
+// a.srcq[q] stays the plain plane q, for the rules at the box faces.
 template <class S>
-struct AASwapOut {
+struct AADst {
   const StepArgs<S>& a;
   int cell;
-  __device__ __forceinline__ S* out(int q) const { return a.dstq[opp(q)] + cell; }
+  __device__ __forceinline__ S* out(int q) const { return a.dstq[q] + cell; }
   __device__ __forceinline__ float scale() const { return a.scale; }
   __device__ __forceinline__ float nws(int c) const { return a.nws[c]; }
 };
@@ -643,13 +648,15 @@ __global__ void __launch_bounds__(128)
   const int z = blockIdx.y, y = blockIdx.z;
   if (x >= a.g.nx) return;
   const int cell = x + a.g.px * (z + a.g.nz * y);
+  const bool edge = (x == 0) | (x == a.g.nx - 1) | (y == 0) | (y == a.g.ny - 1) | (z == 0) |
+                    (z == a.g.nz - 1);
   R f[Q];
-  if (!neighbor) {
+  if (!neighbor || !edge) {
     static_for<0, Q>([&](auto qc) {
       constexpr int q = decltype(qc)::value;
-      f[q] = ld(a.srcq[q] + cell, q, a.inv_scale);
+      f[q] = ld(a.srcd[q] + cell, q, a.inv_scale);
     });
-    const AASwapOut<S> ad{a, cell};
+    const AADst<S> ad{a, cell};
     if (!first) {
       finish_node<S, COLL, LES>(f, a, ad, x, y, z);
     } else {
@@ -671,10 +678,20 @@ __global__ void __launch_bounds__(128)
     }
     return;
   }
-  aa_pull_swapped<S>(f, a, x, y, z, cell);
-  const bool edge = (x == 0) | (x == a.g.nx - 1) | (y == 0) | (y == a.g.ny - 1) | (z == 0) |
-                    (z == a.g.nz - 1);
-  const int t = edge ? node_type(a.g, x, y, z) : NODE_FLUID;
+  // neighbour step at a box face: slots outside the box are the node's own
+  const int t = node_type(a.g, x, y, z);
+  static_for<0, Q>([&](auto qc) {
+    constexpr int q = decltype(qc)::value;
+    const int xs = x - cx(q), ys = y - cy(q), zs = z - cz(q);
+    const bool inside = (unsigned)xs < (unsigned)a.g.nx && (unsigned)ys < (unsigned)a.g.ny &&
+                        (unsigned)zs < (unsigned)a.g.nz;
+    if (inside) {
+      f[q] = ld(a.srcd[q] + cell, q, a.inv_scale);
+    } else {
+      const RealOf<S> fo = ld(a.srcq[q] + cell, q, a.inv_scale);  // own f*_{opp q}
+      f[q] = boundary_value<S, q>(a, t, fo, y, z);
+    }
+  });
   PairState<R> ps;
   make_pairs<R>(f, ps);
   R ux, uy, uz;
@@ -682,13 +699,13 @@ __global__ void __launch_bounds__(128)
   write_macro<S>(a, x, y, z, ps.rho, ux, uy, uz);
   collide_node<S, COLL, LES, false, R>(f, ps, ux, uy, uz, inv_rho, a, [&](int q, R v) {
     const int xt = x + cx(q), yt = y + cy(q), zt = z + cz(q);
-    const bool inside = !edge || ((unsigned)xt < (unsigned)a.g.nx &&
-                                  (unsigned)yt < (unsigned)a.g.ny && (unsigned)zt < (unsigned)a.g.nz);
+    const bool inside = (unsigned)xt < (unsigned)a.g.nx && (unsigned)yt < (unsigned)a.g.ny &&
+                        (unsigned)zt < (unsigned)a.g.nz;
     if (inside)
-      StoreTraits<S>::store_fma(a.dstq[q] + (cell + a.off[q]), v, a.scale, a.nws[wclass(q)]);
+      StoreTraits<S>::store_fma(a.dstq[q] + cell, v, a.scale, a.nws[wclass(q)]);
     else
-      StoreTraits<S>::store_fma(a.dstq[opp(q)] + cell, aa_wall<S>(a, t, v, q), a.scale,
-                                a.nws[wclass(q)]);
+      StoreTraits<S>::store_fma(a.dst + (opp(q) * a.qs + cell), aa_wall<S>(a, t, v, q),
+                                a.scale, a.nws[wclass(q)]);
   });
 }
 
