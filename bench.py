@@ -477,7 +477,7 @@ def report_serving(args, pkg):
             v[3] -= took
         for i in b.poll():
             r, t_adm, nodes, _ = active.pop(i)
-            den, ux, uy, uz = b.member(i).macroscopic()  # the result reaches the host
+            den, ux, uy, uz = b.fetch(i)  # the result reaches the host
             t_done = time.perf_counter() - t0
             tts.append(t_done - r["t"])
             service.append(t_done - t_adm)
@@ -518,7 +518,7 @@ def main():
     ap.add_argument("--rate", type=float, default=200.0, help="serving: arrivals per second")
     ap.add_argument("--window", type=float, default=60.0, help="serving: wall-clock window (s)")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="serving: HBM budget")
-    ap.add_argument("--horizon", type=float, default=4.0,
+    ap.add_argument("--horizon", type=float, default=0.0,
                     help="serving: admit while the resident backlog is below this many seconds "
                          "of work at --nominal-mlups (0 = HBM budget only)")
     ap.add_argument("--nominal-mlups", type=float, default=30000.0,

@@ -457,6 +457,11 @@ int lbm_batch_poll(lbm_batch* b, int* ids, int max, int* n);
  * stream).  Owned by the batch. */
 int lbm_batch_domain(lbm_batch* b, int id, lbm_domain** d);
 
+/* CurrDen / CurrVel* of a member that reached its target, [ny][nz][nx]
+ * (any pointer may be NULL).  Waits only for the member's last chunk, so
+ * the chunks queued behind it keep running. */
+int lbm_batch_fetch(lbm_batch* b, int id, float* den, float* velx, float* vely, float* velz);
+
 /* Release a member's memory back to the pool (waits for its last chunk). */
 int lbm_batch_remove(lbm_batch* b, int id);
 

@@ -166,6 +166,7 @@ def lib():
         L.lbm_batch_poll.argtypes = [vp, vp, i32, C.POINTER(C.c_int)]
         L.lbm_batch_domain.argtypes = [vp, i32, C.POINTER(vp)]
         L.lbm_batch_remove.argtypes = [vp, i32]
+        L.lbm_batch_fetch.argtypes = [vp, i32, vp, vp, vp, vp]
         L.lbm_batch_sync.argtypes = [vp]
         L.lbm_batch_usage.argtypes = [vp, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t),
                                       C.POINTER(C.c_int)]
@@ -436,6 +437,14 @@ class Batch:
         h = C.c_void_p()
         check(lib().lbm_batch_domain(self.h, int(i), C.byref(h)))
         return _Member(h, self.ivs[i])
+
+    def fetch(self, i):
+        """rho, ux, uy, uz [ny][nz][nx] of a member that reached its target,
+        without waiting for the chunks queued behind its last one."""
+        iv = self.ivs[i]
+        out = [np.empty((iv.ny, iv.nz, iv.nx), np.float32) for _ in range(4)]
+        check(lib().lbm_batch_fetch(self.h, int(i), *[_ptr(a) for a in out]))
+        return tuple(out)
 
     def remove(self, i):
         check(lib().lbm_batch_remove(self.h, int(i)))

@@ -515,6 +515,7 @@ int lbm_diagnostics(lbm_domain* d, double out[8]) {
   if (!d->initialized) return set_error(LBM_ERR_STATE, "no state");
   int rc = ensure_device(d);
   if (rc) return rc;
+  if ((rc = ensure_diag_buffers(d))) return rc;
   const long long k = d->step;
   k_diag_partial<<<d->diag_blocks, kDiagThreads, 0, d->stream>>>(
       d->den[k & 1], d->den[(k + 1) & 1], d->ux, d->uy, d->uz, d->N, k > 0 ? 1 : 0, d->partial);

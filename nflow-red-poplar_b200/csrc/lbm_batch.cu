@@ -294,6 +294,8 @@ struct lbm_batch {
   int capacity = 0;               // image slots
   std::vector<int> free_images;
   // device tables and their pinned host images
+  unsigned char* h_images = nullptr;  // pinned host copy of d_images (async uploads)
+  cudaStream_t fetch = nullptr;       // results of finished members (lbm_batch_fetch)
   BatchTables* d_tab = nullptr;
   SlotMeta* d_meta = nullptr;
   long long* d_off = nullptr;
@@ -413,7 +415,10 @@ int ensure_graph(lbm_batch* b, const std::vector<std::pair<int, float>>& groups)
 // Argument images of a member: parity x {no output, rho, rho + u}.
 int upload_images(lbm_batch* b, lbm_batch::Member& m) {
   lbm_domain* d = m.d;
-  std::vector<unsigned char> buf((size_t)kImages * kArgsBytes, 0);
+  // the slot's pinned host image: its previous upload (an earlier member of
+  // the slot) ran before that member's first chunk, long complete
+  unsigned char* buf = b->h_images + (size_t)m.image_slot * kImages * kArgsBytes;
+  std::memset(buf, 0, (size_t)kImages * kArgsBytes);
   int rc = with_storage(d->opt.storage, [&](auto tag) -> int {
     using S = typename decltype(tag)::type;
     if constexpr (std::is_same<S, double>::value) {
@@ -435,18 +440,19 @@ int upload_images(lbm_batch* b, lbm_batch::Member& m) {
     }
   });
   if (rc) return rc;
-  CK(cudaMemcpyAsync(b->d_images + (size_t)m.image_slot * kImages * kArgsBytes, buf.data(),
-                     buf.size(), cudaMemcpyHostToDevice, b->stream));
-  CK(cudaStreamSynchronize(b->stream));  // buf is a local
+  CK(cudaMemcpyAsync(b->d_images + (size_t)m.image_slot * kImages * kArgsBytes, buf,
+                     (size_t)kImages * kArgsBytes, cudaMemcpyHostToDevice, b->stream));
   return LBM_OK;
 }
 
 int grow_images(lbm_batch* b) {
   const int cap = b->capacity ? b->capacity * 2 : 64;
   unsigned char* nimg = nullptr;
+  unsigned char* himg = nullptr;
   SlotMeta *dm = nullptr, *hm = nullptr;
   long long *doff = nullptr, *hoff = nullptr;
   CK(cudaMalloc(&nimg, (size_t)cap * kImages * kArgsBytes));
+  CK(cudaMallocHost(&himg, (size_t)cap * kImages * kArgsBytes));
   CK(cudaMalloc(&dm, (size_t)cap * sizeof(SlotMeta)));
   CK(cudaMalloc(&doff, (size_t)(cap + kGroups) * sizeof(long long)));
   CK(cudaMallocHost(&hm, (size_t)cap * sizeof(SlotMeta)));
@@ -455,7 +461,9 @@ int grow_images(lbm_batch* b) {
   if (b->d_images) {
     CK(cudaMemcpy(nimg, b->d_images, (size_t)b->capacity * kImages * kArgsBytes,
                   cudaMemcpyDeviceToDevice));
+    std::memcpy(himg, b->h_images, (size_t)b->capacity * kImages * kArgsBytes);
     cudaFree(b->d_images);
+    cudaFreeHost(b->h_images);
     cudaFree(b->d_meta);
     cudaFree(b->d_off);
     cudaFreeHost(b->h_meta);
@@ -463,6 +471,7 @@ int grow_images(lbm_batch* b) {
   }
   for (int i = cap - 1; i >= b->capacity; --i) b->free_images.push_back(i);
   b->d_images = nimg;
+  b->h_images = himg;
   b->d_meta = dm;
   b->d_off = doff;
   b->h_meta = hm;
@@ -556,8 +565,8 @@ int issue_chunk(lbm_batch* b, int steps_offered, long long* lups) {
 void destroy_member(lbm_batch* b, lbm_batch::Member& m) {
   lbm_domain* d = m.d;
   if (!d) return;
-  void* bufs[] = {d->lat[0], d->lat[1], d->den[0], d->den[1], d->ux,     d->uy,
-                  d->uz,     d->inlet_u, d->prho[0], d->prho[1], d->pu[0], d->pu[1]};
+  void* bufs[] = {d->lat[0], d->lat[1],  d->den[0], d->den[1], d->ux,    d->uy,  d->uz,
+                  d->inlet_u, d->prho[0], d->prho[1], d->pu[0], d->pu[1], d->flag};
   for (void* p : bufs) b->pool.release(p);
   d->stream = nullptr;  // the batch stream is not the domain's to destroy
   free_all(d);
@@ -620,6 +629,7 @@ int lbm_batch_create(const lbm_batch_options* bo, lbm_batch** out) {
   b->sm_count = prop.multiProcessorCount;
   if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&b->capture, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&b->fetch, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&b->tables_free, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess)
     return fail(set_error(LBM_ERR_CUDA, "stream/event creation failed"));
@@ -650,6 +660,8 @@ int lbm_batch_destroy(lbm_batch* b) {
   for (auto& ce : b->chunk_events) cudaEventDestroy(ce.second);
   if (b->graph) cudaGraphExecDestroy(b->graph);
   if (b->d_images) cudaFree(b->d_images);
+  if (b->h_images) cudaFreeHost(b->h_images);
+  if (b->fetch) cudaStreamDestroy(b->fetch);
   if (b->d_meta) cudaFree(b->d_meta);
   if (b->d_off) cudaFree(b->d_off);
   if (b->d_tab) cudaFree(b->d_tab);
@@ -716,18 +728,16 @@ int lbm_batch_add(lbm_batch* b, const Inputval* pinput, const lbm_options* opt,
     b->members.erase(new_id);
     return code;
   };
-  // the shared diagnostics / staging buffers of a member come from cudaMalloc
-  // on first use (lbm_diagnostics, lbm_export_arF)
-  cudaDeviceProp prop;
-  cudaGetDeviceProperties(&prop, b->opt.device);
-  d->diag_blocks = 4 * prop.multiProcessorCount;
-  if (cudaMalloc((void**)&d->partial, (size_t)d->diag_blocks * 8 * sizeof(double)) !=
-          cudaSuccess ||
-      cudaMalloc((void**)&d->dout, 8 * sizeof(double)) != cudaSuccess ||
-      cudaMalloc((void**)&d->flag, 2 * sizeof(int)) != cudaSuccess ||
-      cudaMemset(d->flag, 0, 2 * sizeof(int)) != cudaSuccess ||
+  // admission allocates only from the pool and synchronises nothing: the
+  // diagnostics / staging buffers of a member come from cudaMalloc on first
+  // use (lbm_diagnostics, lbm_export_arF)
+  d->diag_blocks = 4 * b->sm_count;
+  d->flag = (int*)b->pool.alloc(2 * sizeof(int));
+  if (!d->flag) return undo(set_error(LBM_ERR_BUDGET, "pool full"));
+  d->bytes += 256;
+  if (cudaMemsetAsync(d->flag, 0, 2 * sizeof(int), b->stream) != cudaSuccess ||
       cudaEventCreate(&d->ev0) != cudaSuccess || cudaEventCreate(&d->ev1) != cudaSuccess)
-    return undo(set_error(LBM_ERR_OOM, "member diagnostics buffers"));
+    return undo(set_error(LBM_ERR_CUDA, "member set-up"));
   if ((rc = domain_upload_profile(d, b->stream)) || (rc = domain_launch_init(d, b->stream)) ||
       (rc = upload_images(b, b->members[new_id])))
     return undo(rc);
@@ -799,12 +809,40 @@ int lbm_batch_remove(lbm_batch* b, int id) {
   auto it = b->members.find(id);
   if (it == b->members.end()) return set_error(LBM_ERR_INVALID, "no member %d", id);
   CK(cudaSetDevice(b->opt.device));
+  // a member still stepping is waited for; a finished one has no work in
+  // flight (chunks issued after its last one do not reference it), and
+  // anything that reuses its memory is queued behind those chunks
+  retire_completed(b);
   if (it->second.issued < it->second.target || it->second.done_chunk > b->chunks_completed)
     CK(cudaStreamSynchronize(b->stream));
-  else
-    CK(cudaEventSynchronize(b->tables_free));
   destroy_member(b, it->second);
   b->members.erase(it);
+  return LBM_OK;
+}
+
+int lbm_batch_fetch(lbm_batch* b, int id, float* den, float* velx, float* vely, float* velz) {
+  if (!b) return set_error(LBM_ERR_INVALID, "NULL batch");
+  auto it = b->members.find(id);
+  if (it == b->members.end()) return set_error(LBM_ERR_INVALID, "no member %d", id);
+  const lbm_batch::Member& m = it->second;
+  if (m.issued < m.target) return set_error(LBM_ERR_STATE, "member %d has not reached its target", id);
+  CK(cudaSetDevice(b->opt.device));
+  retire_completed(b);
+  if (m.done_chunk > b->chunks_completed) {
+    // wait for the member's last chunk only, not for the chunks behind it
+    for (auto& ce : b->chunk_events)
+      if (ce.first == m.done_chunk) {
+        CK(cudaEventSynchronize(ce.second));
+        break;
+      }
+  }
+  lbm_domain* d = m.d;
+  const size_t nb = (size_t)d->N * sizeof(float);
+  float* outs[4] = {den, velx, vely, velz};
+  const float* srcs[4] = {d->den[d->step & 1], d->ux, d->uy, d->uz};
+  for (int i = 0; i < 4; ++i)
+    if (outs[i]) CK(cudaMemcpyAsync(outs[i], srcs[i], nb, cudaMemcpyDeviceToHost, b->fetch));
+  CK(cudaStreamSynchronize(b->fetch));
   return LBM_OK;
 }
 

@@ -389,7 +389,7 @@ inline void free_all(lbm_domain* d) {
   if (d->snap_landed) cudaEventDestroy(d->snap_landed);
   if (d->snap_stream) cudaStreamDestroy(d->snap_stream);
   if (d->staging) cudaFree(d->staging);
-  if (d->flag) cudaFree(d->flag);
+  if (d->flag && !d->pooled) cudaFree(d->flag);  // batch members: from the pool
   if (d->partial) cudaFree(d->partial);
   if (d->dout) cudaFree(d->dout);
   for (int i = 0; i < 2; ++i)
@@ -456,19 +456,48 @@ inline size_t domain_state_bytes(const Inputval* in, const lbm_options* opt) {
 }
 
 // Upload the channel inlet profile u_x(y,z) = u_max 16 eta(1-eta) zeta(1-zeta).
+// u_x(y, z) of the channel inlet, on the device so that admission needs no
+// host synchronisation; every operation is a correctly rounded double
+// operation in the order of the host formula, so the values equal the host
+// (and oracle) profile bit for bit
+static __global__ void k_inlet_profile(float* __restrict__ prof, int ny, int nz, double umax) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ny * nz) return;
+  const int y = i / nz, z = i % nz;
+  const double eta = __ddiv_rn((double)y, (double)(ny - 1));
+  const double zeta = __ddiv_rn((double)z, (double)(nz - 1));
+  double v = __dmul_rn(umax, 16.0);
+  v = __dmul_rn(v, eta);
+  v = __dmul_rn(v, __dsub_rn(1.0, eta));
+  v = __dmul_rn(v, zeta);
+  v = __dmul_rn(v, __dsub_rn(1.0, zeta));
+  prof[i] = (float)v;
+}
+
+// Fill the channel inlet profile u_x(y,z) = u_max 16 eta(1-eta) zeta(1-zeta)
+// (asynchronous on st).
 inline int domain_upload_profile(lbm_domain* d, cudaStream_t st) {
   if (d->g.casetype != CHANNEL) return LBM_OK;
-  std::vector<float> prof((size_t)d->g.ny * d->g.nz);
-  for (int y = 0; y < d->g.ny; ++y)
-    for (int z = 0; z < d->g.nz; ++z) {
-      const double eta = (double)y / (double)(d->g.ny - 1);
-      const double zeta = (double)z / (double)(d->g.nz - 1);
-      prof[(size_t)y * d->g.nz + z] =
-          (float)((double)d->in.m_dRefVelx * 16.0 * eta * (1.0 - eta) * zeta * (1.0 - zeta));
-    }
-  CK(cudaMemcpyAsync(d->inlet_u, prof.data(), prof.size() * sizeof(float), cudaMemcpyHostToDevice,
-                     st));
-  CK(cudaStreamSynchronize(st));
+  const int n = d->g.ny * d->g.nz;
+  k_inlet_profile<<<(n + 255) / 256, 256, 0, st>>>(d->inlet_u, d->g.ny, d->g.nz,
+                                                   (double)d->in.m_dRefVelx);
+  CK(cudaGetLastError());
+  return LBM_OK;
+}
+
+// The diagnostics buffers of a domain (allocated on first use for batch
+// members, whose admission allocates nothing outside the pool).
+inline int ensure_diag_buffers(lbm_domain* d) {
+  if (d->partial && d->dout) return LBM_OK;
+  if (!d->partial && cudaMalloc((void**)&d->partial, (size_t)d->diag_blocks * 8 * sizeof(double)) !=
+                         cudaSuccess) {
+    d->partial = nullptr;
+    return set_error(LBM_ERR_OOM, "diagnostics buffer");
+  }
+  if (!d->dout && cudaMalloc((void**)&d->dout, 8 * sizeof(double)) != cudaSuccess) {
+    d->dout = nullptr;
+    return set_error(LBM_ERR_OOM, "diagnostics buffer");
+  }
   return LBM_OK;
 }
 

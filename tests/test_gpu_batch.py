@@ -146,3 +146,24 @@ def test_batch_rejects_fp64_and_bad_options():
         pkg.Batch(hbm_budget=64 << 20, schedule=2)
     with pytest.raises(pkg.LbmError):
         pkg.Batch(hbm_budget=64 << 20, regs=2)
+
+
+def test_fetch_returns_a_finished_members_fields_while_others_run():
+    b = pkg.Batch(hbm_budget=512 << 20, chunk_steps=8)
+    short = b.add(cavity(20, 18, 16), opts(pkg.STORE_F32, 1, 1e-6), 24)
+    long_ = b.add(channel(48, 12, 14), opts(pkg.STORE_F32, pkg.INIT_CHANNEL, 0.01), 10 ** 6)
+    with pytest.raises(pkg.LbmError):
+        b.fetch(short)  # not finished yet
+    b.step(24)
+    b.step(64)  # the long member keeps going
+    while short not in b.poll():
+        b.sync()
+    got = b.fetch(short)
+    _, want = alone(cavity(20, 18, 16), opts(pkg.STORE_F32, 1, 1e-6), 24)
+    for x, y in zip(got, want):
+        np.testing.assert_array_equal(x, y)
+    b.remove(short)
+    b.step(8)
+    b.sync()
+    assert b.member(long_).steps() == 24 + 64 + 8
+    b.close()
