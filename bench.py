@@ -243,7 +243,12 @@ def run_reference_arm(args, pkg, w):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
         "config": {"workload": args.workload, "nx": w["nx"], "ny": w["ny"], "nz": w["nz"],
-                   "device": "host CPU"},
+                   "collision": "MRT" if iv.bEnableMRT else "SRT", "les": bool(iv.bEnableLES),
+                   "cs": round(float(iv.m_dSmagorinsky), 6), "tau": round(float(iv.m_dTau), 6),
+                   "storage": "f32", "device": "host CPU",
+                   "implementation": ("reference lbm_codelets.cpp (OpenMP over the decomposition "
+                                      "tiles)" if which == "ref" else "oracle port"),
+                   "parallelism": "host threads"},
         "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": cores,
                          "kind": "reference" if which == "ref" else "port", "sample": sample},
         "e2e": {"value": v, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
