@@ -149,10 +149,7 @@ int lbm_create(const Inputval* pinput, const lbm_options* opt, lbm_domain** out)
     return fail(rc);
   if (cudaMemset(d->flag, 0, 2 * sizeof(int)) != cudaSuccess)
     return fail(set_error(LBM_ERR_CUDA, "flag reset failed"));
-  rc = with_storage(d->opt.storage, [&](auto tag) -> int {
-    using S = typename decltype(tag)::type;
-    return domain_tensor_maps<S>(d, prop.multiProcessorCount);
-  });
+  rc = storage_ops(d->opt.storage).tensor_maps(d, prop.multiProcessorCount);
   if (rc) return fail(rc);
   d->diag_blocks = 4 * prop.multiProcessorCount;
   if ((rc = alloc((void**)&d->partial, (size_t)d->diag_blocks * 8 * sizeof(double))) ||
@@ -194,95 +191,6 @@ int lbm_initialize(lbm_domain* d) {
 
 }  // extern "C"
 
-namespace {
-
-// nsteps AA steps (local and neighbour steps alternate with the layout),
-// in graph chunks where possible; the last two steps write the rho of their
-// input arF (the previous-step density of the residual), then k_aa_macro
-// writes rho and u of the final arF.
-int run_aa(lbm_domain* d, int nsteps) {
-  return with_storage(d->opt.storage, [&](auto tag) -> int {
-    using S = typename decltype(tag)::type;
-    return with_model<S>(d, [&](auto coll, auto les) -> int {
-      constexpr int C = decltype(coll)::value;
-      constexpr bool L = decltype(les)::value;
-      const dim3 b = block_of(d->g.nx), gr = grid_of(d->g, b);
-      // slot tables of the two step kinds (see k_aa_step)
-      auto args = [&](long long k, bool den, int neighbor) {
-        StepArgs<S> a = make_args<S>(d, d->lat[0], d->lat[0], k);
-        S* lat = (S*)d->lat[0];
-        for (int q = 0; q < Q; ++q) {
-          if (!neighbor) {
-            a.srcd[q] = lat + q * d->qs;
-            a.dstq[q] = lat + opp(q) * d->qs;
-          } else {
-            a.srcd[q] = lat + (opp(q) * d->qs - a.off[q]);
-            a.dstq[q] = lat + (q * d->qs + a.off[q]);
-          }
-        }
-        if (den) a.den_out = d->den[(k - 1) & 1];  // rho of the step's input arF_{k-1}
-        return a;
-      };
-      auto one = [&](bool den) {
-        const long long k = d->step + 1;
-        k_aa_step<S, C, L><<<gr, b, 0, d->stream>>>(args(k, den, d->cur), d->cur,
-                                                    d->aa_first ? 1 : 0);
-        d->aa_first = false;
-        d->cur ^= 1;
-        d->step = k;
-      };
-      int left = nsteps;
-      if (d->aa_first && left > 0) {  // never inside a graph: it has its own collision
-        one(left <= 2);
-        --left;
-      }
-      int plain = left > 2 ? left - 2 : 0;
-      if (plain >= 2 * kGraphSteps) {
-        cudaGraphExec_t& g = d->chunk[d->cur];
-        if (!g) {
-          if (!d->capture) CK(cudaStreamCreateWithFlags(&d->capture, cudaStreamNonBlocking));
-          CK(cudaStreamBeginCapture(d->capture, cudaStreamCaptureModeThreadLocal));
-          int cur = d->cur;
-          long long k = d->step;
-          for (int i = 0; i < kGraphSteps; ++i) {
-            ++k;
-            k_aa_step<S, C, L><<<gr, b, 0, d->capture>>>(args(k, false, cur), cur, 0);
-            cur ^= 1;
-          }
-          cudaGraph_t graph;
-          CK(cudaStreamEndCapture(d->capture, &graph));
-          cudaError_t e = cudaGraphInstantiate(&g, graph, 0);
-          cudaGraphDestroy(graph);
-          if (e != cudaSuccess)
-            return set_error(LBM_ERR_CUDA, "graph instantiation failed: %s",
-                             cudaGetErrorString(e));
-        }
-        while (plain >= kGraphSteps) {
-          CK(cudaGraphLaunch(g, d->stream));
-          d->step += kGraphSteps;  // even: the layout is unchanged
-          plain -= kGraphSteps;
-          left -= kGraphSteps;
-        }
-      }
-      while (left > 0) {
-        one(left <= 2);
-        --left;
-      }
-      StepArgs<S> m = make_args<S>(d, d->lat[0], d->lat[0], d->step);
-      m.den_out = d->den[d->step & 1];
-      m.ux_out = d->ux;
-      m.uy_out = d->uy;
-      m.uz_out = d->uz;
-      k_aa_macro<S><<<gr, b, 0, d->stream>>>(m, d->cur);
-      d->post_direct = false;
-      CK(cudaGetLastError());
-      return LBM_OK;
-    });
-  });
-}
-
-}  // namespace
-
 extern "C" {
 
 int lbm_set_solid_mask(lbm_domain* d, const unsigned char* mask) {
@@ -320,68 +228,13 @@ int lbm_run_simulation(lbm_domain* d, int nsteps) {
   if (rc) return rc;
   CK(cudaEventRecord(d->ev0, d->stream));
   if (d->opt.stream_mode == LBM_STREAM_AA) {
-    rc = run_aa(d, nsteps);
+    rc = storage_ops(d->opt.storage).run_aa(d, nsteps);
     if (rc) return rc;
     CK(cudaEventRecord(d->ev1, d->stream));
     d->last_steps = nsteps;
     return LBM_OK;
   }
-  rc = with_storage(d->opt.storage, [&](auto tag) -> int {
-    using S = typename decltype(tag)::type;
-    return with_model<S>(d, [&](auto coll, auto les) -> int {
-      constexpr int C = decltype(coll)::value;
-      constexpr bool L = decltype(les)::value;
-      // one plain step (no side outputs unless requested)
-      auto step_args = [&](long long k, bool den, bool vel, int cur) {
-        StepArgs<S> a = make_args<S>(d, d->lat[cur], d->lat[cur ^ 1], k);
-        if (den) a.den_out = d->den[k & 1];
-        if (vel) {
-          a.ux_out = d->ux;
-          a.uy_out = d->uy;
-          a.uz_out = d->uz;
-        }
-        return a;
-      };
-      int plain = nsteps > 2 ? nsteps - 2 : 0;  // the last two steps write rho / u
-      // whole graph chunks of kGraphSteps plain steps
-      if (plain >= 2 * kGraphSteps) {
-        cudaGraphExec_t& g = d->chunk[d->cur];
-        if (!g) {
-          if (!d->capture) CK(cudaStreamCreateWithFlags(&d->capture, cudaStreamNonBlocking));
-          CK(cudaStreamBeginCapture(d->capture, cudaStreamCaptureModeThreadLocal));
-          int cur = d->cur;
-          long long k = d->step;
-          for (int i = 0; i < kGraphSteps; ++i) {
-            ++k;
-            launch_step<S, C, L>(d, step_args(k, false, false, cur), d->capture);
-            cur ^= 1;
-          }
-          cudaGraph_t graph;
-          CK(cudaStreamEndCapture(d->capture, &graph));
-          cudaError_t e = cudaGraphInstantiate(&g, graph, 0);
-          cudaGraphDestroy(graph);
-          if (e != cudaSuccess)
-            return set_error(LBM_ERR_CUDA, "graph instantiation failed: %s",
-                             cudaGetErrorString(e));
-        }
-        while (plain >= kGraphSteps) {
-          CK(cudaGraphLaunch(g, d->stream));
-          d->step += kGraphSteps;  // even: cur and plane parity unchanged
-          plain -= kGraphSteps;
-        }
-      }
-      const int rest = plain + (nsteps > 2 ? 2 : nsteps);
-      for (int i = 0; i < rest; ++i) {
-        const long long k = d->step + 1;
-        launch_step<S, C, L>(d, step_args(k, i >= rest - 2, i == rest - 1, d->cur), d->stream);
-        d->cur ^= 1;
-        d->step = k;
-      }
-      d->post_direct = false;
-      CK(cudaGetLastError());
-      return LBM_OK;
-    });
-  });
+  rc = storage_ops(d->opt.storage).run_pull(d, nsteps);
   if (rc) return rc;
   CK(cudaEventRecord(d->ev1, d->stream));
   d->last_steps = nsteps;
@@ -425,22 +278,7 @@ int lbm_import_arF(lbm_domain* d, const float* arF, int padded) {
     d->initialized = false;
     return set_error(LBM_ERR_NOT_FINITE, "lbm_import_arF: input holds NaN/Inf");
   }
-  rc = with_storage(d->opt.storage, [&](auto tag) -> int {
-    using S = typename decltype(tag)::type;
-    return with_model<S>(d, [&](auto coll, auto les) -> int {
-      const bool aa = d->opt.stream_mode == LBM_STREAM_AA;
-      StepArgs<S> a = make_args<S>(d, nullptr, d->lat[aa ? 0 : 1], 0);
-      a.den_out = d->den[0];
-      a.ux_out = d->ux;
-      a.uy_out = d->uy;
-      a.uz_out = d->uz;
-      const dim3 b = block_of(d->g.nx), gr = grid_of(d->g, b);
-      k_import<S, decltype(coll)::value, decltype(les)::value>
-          <<<gr, b, 0, d->stream>>>(a, d->staging, padded, aa ? nullptr : (S*)d->lat[0]);
-      CK(cudaGetLastError());
-      return LBM_OK;
-    });
-  });
+  rc = storage_ops(d->opt.storage).import_staging(d, padded);
   if (rc) return rc;
   d->cur = 0;
   d->post_direct = true;
@@ -461,17 +299,7 @@ int lbm_export_arF(lbm_domain* d, float* arF, int padded) {
   const size_t bytes = (size_t)nodes * Q * sizeof(float);
   if ((rc = ensure_staging(d, bytes))) return rc;
   if (padded) CK(cudaMemsetAsync(d->staging, 0, bytes, d->stream));
-  rc = with_storage(d->opt.storage, [&](auto tag) -> int {
-    using S = typename decltype(tag)::type;
-    const bool aa = d->opt.stream_mode == LBM_STREAM_AA;
-    StepArgs<S> a = make_args<S>(d, d->lat[aa ? 0 : d->cur ^ 1], nullptr, d->step);
-    const int mode = aa ? (d->cur ? kExportAASwapped : kExportDirect)
-                        : (d->post_direct ? kExportDirect : kExportPull);
-    const dim3 b = block_of(d->g.nx), gr = grid_of(d->g, b);
-    k_export<S><<<gr, b, 0, d->stream>>>(a, d->staging, padded, mode);
-    CK(cudaGetLastError());
-    return LBM_OK;
-  });
+  rc = storage_ops(d->opt.storage).export_staging(d, padded);
   if (rc) return rc;
   CK(cudaMemcpyAsync(arF, d->staging, bytes, cudaMemcpyDeviceToHost, d->stream));
   CK(cudaStreamSynchronize(d->stream));

@@ -501,6 +501,26 @@ inline int ensure_diag_buffers(lbm_domain* d) {
   return LBM_OK;
 }
 
+// The storage-typed work of a single domain, one table per storage format,
+// each built in its own translation unit (lbm_ops_impl.cuh).
+struct StorageOps {
+  int (*tensor_maps)(lbm_domain*, int sm_count);
+  int (*launch_init)(lbm_domain*, cudaStream_t);
+  int (*run_pull)(lbm_domain*, int nsteps);
+  int (*run_aa)(lbm_domain*, int nsteps);
+  int (*import_staging)(lbm_domain*, int padded);
+  int (*export_staging)(lbm_domain*, int padded);
+};
+extern const StorageOps kOps_f32, kOps_f16, kOps_bf16, kOps_f64;
+inline const StorageOps& storage_ops(int storage) {
+  switch (storage) {
+    case LBM_STORE_F16_SHIFT: return kOps_f16;
+    case LBM_STORE_BF16_SHIFT: return kOps_bf16;
+    case LBM_STORE_F64: return kOps_f64;
+    default: return kOps_f32;
+  }
+}
+
 // InitParams of the domain's initial condition.
 inline InitParams init_params(const lbm_domain* d) {
   InitParams ip;
@@ -514,31 +534,14 @@ inline InitParams init_params(const lbm_domain* d) {
   return ip;
 }
 
-// Launch the initial-state kernel of d on st (post lattice lat[1], first
-// collision into lat[0]) and reset the step state.
+// Launch the initial-state kernel of d on st (pull form: post lattice
+// lat[1], first collision into lat[0]; AA: arF_0 in lat[0]) and reset the
+// step state.
 inline int domain_launch_init(lbm_domain* d, cudaStream_t st) {
-  const InitParams ip = init_params(d);
   const size_t nb = (size_t)d->N * sizeof(float);
   CK(cudaMemsetAsync(d->den[0], 0, nb, st));
   CK(cudaMemsetAsync(d->den[1], 0, nb, st));
-  int rc = with_storage(d->opt.storage, [&](auto tag) -> int {
-    using S = typename decltype(tag)::type;
-    return with_model<S>(d, [&](auto coll, auto les) -> int {
-      // pull: arF_0 in lat[1], its collision in lat[0]; AA: arF_0 in the
-      // natural layout of lat[0], collided by the first step
-      const bool aa = d->opt.stream_mode == LBM_STREAM_AA;
-      StepArgs<S> a = make_args<S>(d, nullptr, d->lat[aa ? 0 : 1], 0);
-      a.den_out = d->den[0];
-      a.ux_out = d->ux;
-      a.uy_out = d->uy;
-      a.uz_out = d->uz;
-      const dim3 b = block_of(d->g.nx), gr = grid_of(d->g, b);
-      k_init<S, decltype(coll)::value, decltype(les)::value>
-          <<<gr, b, 0, st>>>(a, aa ? nullptr : (S*)d->lat[0], ip);
-      CK(cudaGetLastError());
-      return LBM_OK;
-    });
-  });
+  int rc = storage_ops(d->opt.storage).launch_init(d, st);
   if (rc) return rc;
   d->cur = 0;
   d->post_direct = true;

@@ -1,0 +1,221 @@
+// lbm_ops_impl.cuh — the storage-typed work of a single domain (initial
+// state, the pull and AA step loops, import and export), written once as
+// templates and instantiated for one storage format per translation unit
+// (lbm_ops_f32.cu, lbm_ops_f16.cu, lbm_ops_bf16.cu, lbm_ops_f64.cu), so that
+// the kernels of the four formats compile in parallel.
+#pragma once
+#include "lbm_domain.cuh"
+
+namespace lbm {
+
+template <class S>
+int ops_tensor_maps(lbm_domain* d, int sm_count) {
+  return domain_tensor_maps<S>(d, sm_count);
+}
+
+// k_init: pull form: arF_0 in lat[1], its collision in lat[0]; AA: arF_0 in
+// the natural layout of lat[0], collided by the first step
+template <class S>
+int ops_launch_init(lbm_domain* d, cudaStream_t st) {
+  const InitParams ip = init_params(d);
+  return with_model<S>(d, [&](auto coll, auto les) -> int {
+    // pull: arF_0 in lat[1], its collision in lat[0]; AA: arF_0 in the
+    // natural layout of lat[0], collided by the first step
+    const bool aa = d->opt.stream_mode == LBM_STREAM_AA;
+    StepArgs<S> a = make_args<S>(d, nullptr, d->lat[aa ? 0 : 1], 0);
+    a.den_out = d->den[0];
+    a.ux_out = d->ux;
+    a.uy_out = d->uy;
+    a.uz_out = d->uz;
+    const dim3 b = block_of(d->g.nx), gr = grid_of(d->g, b);
+    k_init<S, decltype(coll)::value, decltype(les)::value>
+        <<<gr, b, 0, st>>>(a, aa ? nullptr : (S*)d->lat[0], ip);
+    CK(cudaGetLastError());
+    return LBM_OK;
+  });
+}
+
+template <class S>
+int ops_run_pull(lbm_domain* d, int nsteps) {
+  return with_model<S>(d, [&](auto coll, auto les) -> int {
+    constexpr int C = decltype(coll)::value;
+    constexpr bool L = decltype(les)::value;
+    // one plain step (no side outputs unless requested)
+    auto step_args = [&](long long k, bool den, bool vel, int cur) {
+      StepArgs<S> a = make_args<S>(d, d->lat[cur], d->lat[cur ^ 1], k);
+      if (den) a.den_out = d->den[k & 1];
+      if (vel) {
+        a.ux_out = d->ux;
+        a.uy_out = d->uy;
+        a.uz_out = d->uz;
+      }
+      return a;
+    };
+    int plain = nsteps > 2 ? nsteps - 2 : 0;  // the last two steps write rho / u
+    // whole graph chunks of kGraphSteps plain steps
+    if (plain >= 2 * kGraphSteps) {
+      cudaGraphExec_t& g = d->chunk[d->cur];
+      if (!g) {
+        if (!d->capture) CK(cudaStreamCreateWithFlags(&d->capture, cudaStreamNonBlocking));
+        CK(cudaStreamBeginCapture(d->capture, cudaStreamCaptureModeThreadLocal));
+        int cur = d->cur;
+        long long k = d->step;
+        for (int i = 0; i < kGraphSteps; ++i) {
+          ++k;
+          launch_step<S, C, L>(d, step_args(k, false, false, cur), d->capture);
+          cur ^= 1;
+        }
+        cudaGraph_t graph;
+        CK(cudaStreamEndCapture(d->capture, &graph));
+        cudaError_t e = cudaGraphInstantiate(&g, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess)
+          return set_error(LBM_ERR_CUDA, "graph instantiation failed: %s",
+                           cudaGetErrorString(e));
+      }
+      while (plain >= kGraphSteps) {
+        CK(cudaGraphLaunch(g, d->stream));
+        d->step += kGraphSteps;  // even: cur and plane parity unchanged
+        plain -= kGraphSteps;
+      }
+    }
+    const int rest = plain + (nsteps > 2 ? 2 : nsteps);
+    for (int i = 0; i < rest; ++i) {
+      const long long k = d->step + 1;
+      launch_step<S, C, L>(d, step_args(k, i >= rest - 2, i == rest - 1, d->cur), d->stream);
+      d->cur ^= 1;
+      d->step = k;
+    }
+    d->post_direct = false;
+    CK(cudaGetLastError());
+    return LBM_OK;
+  });
+}
+
+// nsteps AA steps (local and neighbour steps alternate with the layout),
+// in graph chunks where possible; the last two steps write the rho of their
+// input arF (the previous-step density of the residual), then k_aa_macro
+// writes rho and u of the final arF.
+template <class S>
+int ops_run_aa(lbm_domain* d, int nsteps) {
+  return with_model<S>(d, [&](auto coll, auto les) -> int {
+    constexpr int C = decltype(coll)::value;
+    constexpr bool L = decltype(les)::value;
+    const dim3 b = block_of(d->g.nx), gr = grid_of(d->g, b);
+    // slot tables of the two step kinds (see k_aa_step)
+    auto args = [&](long long k, bool den, int neighbor) {
+      StepArgs<S> a = make_args<S>(d, d->lat[0], d->lat[0], k);
+      S* lat = (S*)d->lat[0];
+      for (int q = 0; q < Q; ++q) {
+        if (!neighbor) {
+          a.srcd[q] = lat + q * d->qs;
+          a.dstq[q] = lat + opp(q) * d->qs;
+        } else {
+          a.srcd[q] = lat + (opp(q) * d->qs - a.off[q]);
+          a.dstq[q] = lat + (q * d->qs + a.off[q]);
+        }
+      }
+      if (den) a.den_out = d->den[(k - 1) & 1];  // rho of the step's input arF_{k-1}
+      return a;
+    };
+    auto one = [&](bool den) {
+      const long long k = d->step + 1;
+      k_aa_step<S, C, L><<<gr, b, 0, d->stream>>>(args(k, den, d->cur), d->cur,
+                                                  d->aa_first ? 1 : 0);
+      d->aa_first = false;
+      d->cur ^= 1;
+      d->step = k;
+    };
+    int left = nsteps;
+    if (d->aa_first && left > 0) {  // never inside a graph: it has its own collision
+      one(left <= 2);
+      --left;
+    }
+    int plain = left > 2 ? left - 2 : 0;
+    if (plain >= 2 * kGraphSteps) {
+      cudaGraphExec_t& g = d->chunk[d->cur];
+      if (!g) {
+        if (!d->capture) CK(cudaStreamCreateWithFlags(&d->capture, cudaStreamNonBlocking));
+        CK(cudaStreamBeginCapture(d->capture, cudaStreamCaptureModeThreadLocal));
+        int cur = d->cur;
+        long long k = d->step;
+        for (int i = 0; i < kGraphSteps; ++i) {
+          ++k;
+          k_aa_step<S, C, L><<<gr, b, 0, d->capture>>>(args(k, false, cur), cur, 0);
+          cur ^= 1;
+        }
+        cudaGraph_t graph;
+        CK(cudaStreamEndCapture(d->capture, &graph));
+        cudaError_t e = cudaGraphInstantiate(&g, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess)
+          return set_error(LBM_ERR_CUDA, "graph instantiation failed: %s",
+                           cudaGetErrorString(e));
+      }
+      while (plain >= kGraphSteps) {
+        CK(cudaGraphLaunch(g, d->stream));
+        d->step += kGraphSteps;  // even: the layout is unchanged
+        plain -= kGraphSteps;
+        left -= kGraphSteps;
+      }
+    }
+    while (left > 0) {
+      one(left <= 2);
+      --left;
+    }
+    StepArgs<S> m = make_args<S>(d, d->lat[0], d->lat[0], d->step);
+    m.den_out = d->den[d->step & 1];
+    m.ux_out = d->ux;
+    m.uy_out = d->uy;
+    m.uz_out = d->uz;
+    k_aa_macro<S><<<gr, b, 0, d->stream>>>(m, d->cur);
+    d->post_direct = false;
+    CK(cudaGetLastError());
+    return LBM_OK;
+  });
+}
+
+// k_import from d->staging (the AoS arF already on the device)
+template <class S>
+int ops_import(lbm_domain* d, int padded) {
+  return with_model<S>(d, [&](auto coll, auto les) -> int {
+    const bool aa = d->opt.stream_mode == LBM_STREAM_AA;
+    StepArgs<S> a = make_args<S>(d, nullptr, d->lat[aa ? 0 : 1], 0);
+    a.den_out = d->den[0];
+    a.ux_out = d->ux;
+    a.uy_out = d->uy;
+    a.uz_out = d->uz;
+    const dim3 b = block_of(d->g.nx), gr = grid_of(d->g, b);
+    k_import<S, decltype(coll)::value, decltype(les)::value>
+        <<<gr, b, 0, d->stream>>>(a, d->staging, padded, aa ? nullptr : (S*)d->lat[0]);
+    CK(cudaGetLastError());
+    return LBM_OK;
+  });
+}
+
+// k_export into d->staging
+template <class S>
+int ops_export(lbm_domain* d, int padded) {
+  const bool aa = d->opt.stream_mode == LBM_STREAM_AA;
+  StepArgs<S> a = make_args<S>(d, d->lat[aa ? 0 : d->cur ^ 1], nullptr, d->step);
+  const int mode = aa ? (d->cur ? kExportAASwapped : kExportDirect)
+                      : (d->post_direct ? kExportDirect : kExportPull);
+  const dim3 b = block_of(d->g.nx), gr = grid_of(d->g, b);
+  k_export<S><<<gr, b, 0, d->stream>>>(a, d->staging, padded, mode);
+  CK(cudaGetLastError());
+  return LBM_OK;
+}
+
+template <class S>
+StorageOps make_ops() {
+  StorageOps o;
+  o.tensor_maps = &ops_tensor_maps<S>;
+  o.launch_init = &ops_launch_init<S>;
+  o.run_pull = &ops_run_pull<S>;
+  o.run_aa = &ops_run_aa<S>;
+  o.import_staging = &ops_import<S>;
+  o.export_staging = &ops_export<S>;
+  return o;
+}
+
+}  // namespace lbm
