@@ -46,13 +46,13 @@ def load_package():
 
 
 WORKLOADS = {
-    # the headline metric's configuration
+    # the headline workload: 256^3 lid-driven cavity, MRT + LES, Re 5000
     "cavity256_mrt_les": dict(nx=256, ny=256, nz=256, case="cavity", re=5000.0, u=0.1, cs=0.1,
                               mrt=True, les=True, init=1, amp=1e-6),
-    # the reference's CPU-runnable case
+    # the small SRT cavity the reference's CPU path runs in seconds
     "cavity64_srt": dict(nx=64, ny=64, nz=64, case="cavity", tau=0.6, u=0.1, cs=0.0, mrt=False,
                          les=False, init=1, amp=1e-6),
-    # channel, Re = u_max*ny/nu = 1000
+    # channel, Re = u_max*ny/nu = 1000 (precision comparison)
     "channel512x128x128_mrt_les": dict(nx=512, ny=128, nz=128, case="channel", re_ch=1000.0,
                                        u=0.05, cs=0.1, mrt=True, les=True, init=2, amp=0.01),
 }
@@ -257,8 +257,9 @@ def run_reference_arm(args, pkg, w):
 
 
 # --------------------------------------------------------------------------
-# Further forms (run with --report): precision, batched
-# (configs[3]) and serving.  Each prints one JSON line.
+# Further forms (run with --report): precision (FP16/BF16 vs FP32 storage on
+# the 512x128x128 channel), batched (256 mixed domains) and serving (Poisson
+# arrivals).  Each prints one JSON line.
 # --------------------------------------------------------------------------
 def _enstrophy(ux, uy, uz):
     """0.5 * sum |curl u|^2 over the interior, central differences, FP64.
@@ -275,7 +276,7 @@ def _enstrophy(ux, uy, uz):
 
 
 def report_precision(args, pkg):
-    """channel 512x128x128 MRT+LES, parabolic inlet u_max=0.05,
+    """Channel 512x128x128 MRT+LES, parabolic inlet u_max=0.05,
     outlet rho=1, walls, 1 % seeded velocity perturbation, Re = u_max ny / nu
     = 1000; the same run with FP16-shift, BF16-shift and FP32 storage against
     the FP64 build."""
@@ -335,7 +336,7 @@ def report_precision(args, pkg):
 
 
 def _c4_domains(seed, n, storage):
-    """edge from {32,48,64,96,128}; 50 % cavities e^3 (lid 0.1),
+    """Mixed domains: edge from {32,48,64,96,128}; 50 % cavities e^3 (lid 0.1),
     50 % channels 4e x e x e (u_max 0.05); Re log-uniform in [100, 5000]
     (nu = u e / Re, tau = 3 nu + 0.5); 50 % SRT, 50 % MRT+LES (Cs 0.1)."""
     rng = np.random.default_rng(seed)
@@ -363,7 +364,7 @@ def _case_iv(pkg, c):
 
 
 def report_batch(args, pkg):
-    """configs[3]: 256 independent domains in one persistent launch per step
+    """256 independent domains in one persistent launch per step
     (CUDA-graph chunks, autotuned launch shape) vs each domain launched
     alone, for FP32 and FP16-shift storage."""
     ndom = 256
@@ -419,7 +420,7 @@ def report_batch(args, pkg):
 
 
 def report_serving(args, pkg):
-    """seeded Poisson arrivals, cavity/channel solves with edge
+    """Seeded Poisson arrivals, cavity/channel solves with edge
     32-192, steps U[500, 5000], Re log-U[100, 5000], FP16-shift or FP32 per
     request (MRT+LES), admitted by an HBM budget and stepped by continuous
     batching; time-to-solution (arrival -> result on the host) and service

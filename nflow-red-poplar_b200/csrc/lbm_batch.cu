@@ -46,8 +46,8 @@ struct SlotMeta {
 };
 
 // model: 0 SRT, 1 SRT+LES, 2 MRT, 3 MRT+LES; variant = storage * 4 + model
-// A launch group is the domains of one variant with one storage scale; each
-// step launches the group's kernel once, the scale being a kernel parameter.
+// A launch group is the domains of one variant; each step launches the
+// group's kernel once.  Storage scales travel in the argument images.
 constexpr int kGroups = 32;
 
 // The domains of one group: meta[slot0 .. slot0 + nslots) and their tile
@@ -89,7 +89,7 @@ struct CurSlot {
 // the nodes of local tile lt of the current domain
 template <class S, int COLL, bool LES>
 __device__ __forceinline__ void batch_tile(const StepArgs<S>& a, const CurSlot& cur,
-                                           unsigned lt, int npt, const Scales& sc) {
+                                           unsigned lt, int npt) {
   const unsigned base = lt * (unsigned)(blockDim.x * npt);
   for (int i = 0; i < npt; ++i) {
     const unsigned n = base + (unsigned)i * blockDim.x + threadIdx.x;
@@ -98,7 +98,7 @@ __device__ __forceinline__ void batch_tile(const StepArgs<S>& a, const CurSlot& 
     const int x = (int)(n - r * (unsigned)cur.m.nx);
     const unsigned y = fastdiv(r, cur.m.mnz);
     const int z = (int)(r - y * (unsigned)cur.m.nz);
-    step_node<S, COLL, LES, IndexAddr>(a, x, (int)y, z, sc);
+    step_node<S, COLL, LES>(a, x, (int)y, z);
   }
 }
 
@@ -142,7 +142,7 @@ __device__ __forceinline__ void enter_slot(CurSlot& cur, unsigned char* img,
 }
 
 // One time step (launch j of a chunk) of every active domain of launch
-// group g (one variant, one storage scale sc).  Schedule 0 gives CTA c the
+// group g (one variant).  Schedule 0 gives CTA c the
 // contiguous tiles [c*per, (c+1)*per) of the group's list; schedule 1 walks
 // t = blockIdx.x, += gridDim.x.  Either way the CTA moves forward through the
 // domains and reloads a domain's arguments only when it enters it.  The
@@ -151,7 +151,7 @@ __device__ __forceinline__ void enter_slot(CurSlot& cur, unsigned char* img,
 // registers, 3 -> 80) trades occupancy against spills; the autotuner picks.
 template <class S, int COLL, bool LES, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_batch_step(const BatchTables* __restrict__ tab,
-                                                          int g, int j, int npt, const Scales sc) {
+                                                          int g, int j, int npt) {
   __shared__ __align__(16) unsigned char img[kArgsBytes];
   __shared__ CurSlot cur;
   const StepArgs<S>& a = *reinterpret_cast<const StepArgs<S>*>(img);
@@ -171,18 +171,18 @@ __global__ void __launch_bounds__(256, MINB) k_batch_step(const BatchTables* __r
         t = cur.end - 1;
         continue;
       }
-      batch_tile<S, COLL, LES>(a, cur, (unsigned)(t - cur.begin), npt, sc);
+      batch_tile<S, COLL, LES>(a, cur, (unsigned)(t - cur.begin), npt);
     }
   } else {
     for (long long t = blockIdx.x; t < cur.ntiles; t += gridDim.x) {
       if (t >= cur.end) enter_slot(cur, img, tab, g, t, j);
       if (!cur.ok) continue;
-      batch_tile<S, COLL, LES>(a, cur, (unsigned)(t - cur.begin), npt, sc);
+      batch_tile<S, COLL, LES>(a, cur, (unsigned)(t - cur.begin), npt);
     }
   }
 }
 
-using BatchKernel = void (*)(const BatchTables*, int, int, int, const Scales);
+using BatchKernel = void (*)(const BatchTables*, int, int, int);
 
 template <class S, int MINB>
 constexpr BatchKernel batch_kernel_of(int model) {
@@ -307,7 +307,7 @@ struct lbm_batch {
   // chunk graph
   cudaGraphExec_t graph = nullptr;
   int graph_block = 0, graph_npt = 0, graph_steps = 0, graph_sched = -1;
-  std::vector<std::pair<int, float>> graph_groups;  // (variant, scale) per launch group
+  std::vector<int> graph_groups;  // variant per launch group
   int graph_ctas = -1, graph_regs = -1;
   // completion tracking
   long long chunks_issued = 0;
@@ -342,42 +342,26 @@ int member_variant(const lbm_domain* d) {
   return storage_index(d->opt.storage) * 4 + model_of(d->in);
 }
 
-float member_scale(const lbm_domain* d) {
-  return d->opt.storage == LBM_STORE_F32 ? 1.0f : d->scale;
-}
-
-// Launch groups (variant, storage scale) of the members that still have
-// steps to take, in a fixed order.
-std::vector<std::pair<int, float>> pending_groups(const lbm_batch* b) {
-  std::vector<std::pair<int, float>> gs;
+// Launch groups (variants) of the members that still have steps to take,
+// in a fixed order.
+std::vector<int> pending_groups(const lbm_batch* b) {
+  std::vector<int> gs;
   for (auto& kv : b->members)
     if (kv.second.issued < kv.second.target) {
-      const std::pair<int, float> key(member_variant(kv.second.d), member_scale(kv.second.d));
+      const int key = member_variant(kv.second.d);
       if (std::find(gs.begin(), gs.end(), key) == gs.end()) gs.push_back(key);
     }
   std::sort(gs.begin(), gs.end());
   return gs;
 }
 
-Scales scales_of(float scale) {
-  Scales sc;
-  sc.scale = scale;
-  sc.inv_scale = 1.0f / scale;
-  for (int c = 0; c < 3; ++c) {
-    const float w = c == 0 ? 1.0f / 3.0f : (c == 1 ? 1.0f / 18.0f : 1.0f / 36.0f);
-    sc.nws[c] = -w * scale;
-  }
-  return sc;
-}
-
 // (Re)capture the chunk graph: chunk_steps steps, each one launch per
 // launch group, for the current launch shape.
-int ensure_graph(lbm_batch* b, const std::vector<std::pair<int, float>>& groups) {
+int ensure_graph(lbm_batch* b, const std::vector<int>& groups) {
   const int block = launch_block(b), npt = launch_npt(b), steps = chunk_steps(b);
   const int sched = b->opt.schedule == 1 ? 1 : 0;
   if ((int)groups.size() > kGroups)
-    return set_error(LBM_ERR_INVALID, "more than %d (model, storage, scale) groups in a batch",
-                     kGroups);
+    return set_error(LBM_ERR_INVALID, "more than %d (model, storage) groups in a batch", kGroups);
   if (b->graph && b->graph_block == block && b->graph_npt == npt && b->graph_steps == steps &&
       b->graph_groups == groups && b->graph_sched == sched &&
       b->graph_ctas == b->opt.ctas_per_sm && b->graph_regs == b->opt.regs)
@@ -388,14 +372,14 @@ int ensure_graph(lbm_batch* b, const std::vector<std::pair<int, float>>& groups)
   }
   std::vector<int> grids(groups.size());
   for (size_t g = 0; g < groups.size(); ++g) {
-    int rc = launch_grid(b, groups[g].first, block, &grids[g]);
+    int rc = launch_grid(b, groups[g], block, &grids[g]);
     if (rc) return rc;
   }
   CK(cudaStreamBeginCapture(b->capture, cudaStreamCaptureModeThreadLocal));
   for (int j = 0; j < steps; ++j)
     for (size_t g = 0; g < groups.size(); ++g)
-      batch_kernel(groups[g].first, b->opt.regs)<<<grids[g], block, 0, b->capture>>>(
-          b->d_tab, (int)g, j, npt, scales_of(groups[g].second));
+      batch_kernel(groups[g], b->opt.regs)<<<grids[g], block, 0, b->capture>>>(b->d_tab, (int)g,
+                                                                              j, npt);
   cudaGraph_t gr;
   CK(cudaStreamEndCapture(b->capture, &gr));
   cudaError_t e = cudaGraphInstantiate(&b->graph, gr, 0);
@@ -495,7 +479,7 @@ void retire_completed(lbm_batch* b) {
 int issue_chunk(lbm_batch* b, int steps_offered, long long* lups) {
   const int S = chunk_steps(b);
   *lups = 0;
-  const std::vector<std::pair<int, float>> groups = pending_groups(b);
+  const std::vector<int> groups = pending_groups(b);
   if (groups.empty()) return LBM_OK;
   int rc = ensure_graph(b, groups);
   if (rc) return rc;
@@ -513,8 +497,7 @@ int issue_chunk(lbm_batch* b, int steps_offered, long long* lups) {
       lbm_batch::Member& m = kv.second;
       lbm_domain* d = m.d;
       const long long left = m.target - m.issued;
-      if (left <= 0 || member_variant(d) != groups[g].first || member_scale(d) != groups[g].second)
-        continue;
+      if (left <= 0 || member_variant(d) != groups[g]) continue;
       const int active = (int)std::min<long long>(std::min(S, steps_offered), left);
       SlotMeta& sm = b->h_meta[n];
       sm.image_base = m.image_slot * kImages;
@@ -694,11 +677,6 @@ int lbm_batch_add(lbm_batch* b, const Inputval* pinput, const lbm_options* opt,
   if (b->free_images.empty() && (rc = grow_images(b))) return rc;
   lbm_domain* d = new lbm_domain();
   domain_prepare(d, pinput, opt);
-  if ((long long)Q * d->qs >= (1LL << 31)) {  // 32-bit population indices (IndexAddr)
-    delete d;
-    return set_error(LBM_ERR_INVALID,
-                     "batch members need 19 x plane size < 2^31 (about 113M nodes)");
-  }
   d->opt.device = b->opt.device;
   d->pooled = true;
   d->stream = b->stream;
@@ -751,7 +729,7 @@ int lbm_batch_step(lbm_batch* b, int steps) {
   if (steps < 0) return set_error(LBM_ERR_INVALID, "negative steps");
   CK(cudaSetDevice(b->opt.device));
   // capture before the first event so that the timed span holds GPU work only
-  const std::vector<std::pair<int, float>> groups = pending_groups(b);
+  const std::vector<int> groups = pending_groups(b);
   int rc = groups.empty() ? LBM_OK : ensure_graph(b, groups);
   if (rc) return rc;
   CK(cudaEventRecord(b->ev0, b->stream));

@@ -130,32 +130,19 @@ __device__ __forceinline__ RealOf<S> ld(const S* p, int q, float inv_scale) {
   return StoreTraits<S>::load(p, weight<RealOf<S>>(q), inv_scale);
 }
 
-// Boundary value of population q at a node whose donor x - c_q is outside
-// the domain.  d = opp(q) is the reference's "outside" direction; fo is
-// f*_{k-1}[d] at the node itself (arFTemp[d](x) in the reference).
-// Storage scale factors of the shifted 16-bit forms: f = h * inv_scale + w
-// on load, h = f * scale - w * scale on store (nws[c] = -w * scale for the
-// weight class c).
-struct Scales {
-  float scale, inv_scale;
-  float nws[3];
-};
-
 // Where the populations of a node live (cell = in-plane index of the node)
-// and the storage scales.  PlaneAddr takes the per-population plane
-// pointers and scales of StepArgs: in the kernel parameter space they are
-// free operands, one address instruction per access.  IndexAddr derives
-// every address from the two lattice bases and the strides, and takes the
-// scales from a separate Scales value: for arguments held in shared memory
-// (the batched kernel), where 38 plane pointers and the scales would
-// otherwise be loaded into registers or reloaded per access.  IndexAddr
-// needs Q * qs < 2^31.
+// and the storage scales of the shifted 16-bit forms (f = h * inv_scale + w
+// on load, h = f * scale - w * scale on store, nws[c] = -w * scale for the
+// weight class c).  PlaneAddr takes the per-population plane pointers and
+// scales of StepArgs, wherever the arguments are held: in the kernel
+// parameter space (single-domain kernels) every pointer is a free operand;
+// in shared memory (the batched kernel) each is one broadcast load, issued
+// next to its use, so no per-population offset stays live in registers.
 template <class S>
 struct PlaneAddr {
   const StepArgs<S>& a;
   int cell;
-  __device__ __forceinline__ PlaneAddr(const StepArgs<S>& args, int c, const Scales&)
-      : a(args), cell(c) {}
+  __device__ __forceinline__ PlaneAddr(const StepArgs<S>& args, int c) : a(args), cell(c) {}
   __device__ __forceinline__ const S* donor(int q) const { return a.srcd[q] + cell; }
   __device__ __forceinline__ const S* own(int q) const { return a.srcq[q] + cell; }
   __device__ __forceinline__ S* out(int q) const { return a.dstq[q] + cell; }
@@ -164,25 +151,9 @@ struct PlaneAddr {
   __device__ __forceinline__ float nws(int c) const { return a.nws[c]; }
 };
 
-template <class S>
-struct IndexAddr {
-  const S* src;
-  S* dst;
-  int cell, qs, px, pxnz;
-  const Scales& sc;
-  __device__ __forceinline__ IndexAddr(const StepArgs<S>& a, int c, const Scales& scales)
-      : src(a.src), dst(a.dst), cell(c), qs((int)a.qs), px(a.g.px), pxnz(a.g.px * a.g.nz),
-        sc(scales) {}
-  __device__ __forceinline__ const S* donor(int q) const {
-    return src + (cell + q * qs - (cx(q) + px * cz(q) + pxnz * cy(q)));
-  }
-  __device__ __forceinline__ const S* own(int q) const { return src + (cell + q * qs); }
-  __device__ __forceinline__ S* out(int q) const { return dst + (cell + q * qs); }
-  __device__ __forceinline__ float inv_scale() const { return sc.inv_scale; }
-  __device__ __forceinline__ float scale() const { return sc.scale; }
-  __device__ __forceinline__ float nws(int c) const { return sc.nws[c]; }
-};
-
+// Boundary value of population q at a node whose donor x - c_q is outside
+// the domain.  d = opp(q) is the reference's "outside" direction; fo is
+// f*_{k-1}[d] at the node itself (arFTemp[d](x) in the reference).
 template <class S, int q>
 __device__ __forceinline__ RealOf<S> boundary_value(const StepArgs<S>& a, int t, RealOf<S> fo,
                                                     int y, int z) {
@@ -441,16 +412,15 @@ __device__ __forceinline__ void finish_node(const RealOf<S> (&f)[Q], const StepA
 
 // One fused step of the node (x, y, z): pull + boundary rules, macroscopic,
 // LES, collision, store.  Shared by the single-domain and batched kernels,
-// so a domain gets the same bits alone and in a batch (the addressing
-// policy changes where the operands come from, not the arithmetic).
-template <class S, int COLL, bool LES, template <class> class Addr = PlaneAddr>
-__device__ __forceinline__ void step_node(const StepArgs<S>& a, int x, int y, int z,
-                                          const Scales& sc = Scales{}) {
+// so a domain gets the same bits alone and in a batch (only where the
+// arguments are held differs, not the arithmetic).
+template <class S, int COLL, bool LES>
+__device__ __forceinline__ void step_node(const StepArgs<S>& a, int x, int y, int z) {
   using R = RealOf<S>;
   // STRUCT nodes are never streamed, collided or measured (kernel.cu:294,
   // 323, 362, 464, 495, 1105)
   if (has_struct(a.g) && node_type(a.g, x, y, z) == NODE_STRUCT) return;
-  const Addr<S> ad(a, x + a.g.px * (z + a.g.nz * y), sc);
+  const PlaneAddr<S> ad(a, x + a.g.px * (z + a.g.nz * y));
   R f[Q];
   pull<S>(f, a, ad, x, y, z);
   finish_node<S, COLL, LES>(f, a, ad, x, y, z);
@@ -764,7 +734,7 @@ __global__ void __launch_bounds__(128)
   } else if (mode == kExportAASwapped) {
     aa_pull_swapped<S>(f, a, x, y, z, (int)cell);
   } else {
-    pull<S>(f, a, PlaneAddr<S>(a, (int)cell, Scales{}), x, y, z);
+    pull<S>(f, a, PlaneAddr<S>(a, (int)cell), x, y, z);
   }
   long long node;
   if (padded)
@@ -853,9 +823,9 @@ __global__ void __launch_bounds__(64, LBM_PACKED_MIN_BLOCKS) k_step2(const __gri
     });
   } else {
     float fa[Q], fb[Q];
-    pull<S>(fa, a, PlaneAddr<S>(a, cell, Scales{}), x0, y, z);
+    pull<S>(fa, a, PlaneAddr<S>(a, cell), x0, y, z);
     if (two) {
-      pull<S>(fb, a, PlaneAddr<S>(a, cell + 1, Scales{}), x0 + 1, y, z);
+      pull<S>(fb, a, PlaneAddr<S>(a, cell + 1), x0 + 1, y, z);
     } else {
       static_for<0, Q>([&](auto qc) { fb[decltype(qc)::value] = fa[decltype(qc)::value]; });
     }

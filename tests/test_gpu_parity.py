@@ -51,7 +51,7 @@ def assert_fields_close(dom, ref, tol=TOL):
 
 
 def test_c1_srt_cavity_64_1000_steps():
-    """configs[0]: SRT cavity 64^3, tau=0.6, lid u_x=0.1 on +y, rho noise 1e-6, 1000 steps."""
+    """SRT cavity 64^3, tau=0.6, lid u_x=0.1 on +y, rho noise 1e-6, 1000 steps."""
     iv = cavity(64, tau=0.6)
     dom = gpu_run(iv, 1000, kind=pkg.INIT_DENSITY_NOISE, amp=1e-6)
     ref = O.Run(iv, init_kind=1, amp=1e-6)
@@ -252,7 +252,7 @@ def test_kernelcu_golden(name):
 
 
 def test_c2_full_size_properties():
-    """configs[1] size (256^3 MRT+LES, Cs=0.1, Re=5000): size-independent checks.
+    """Headline size (256^3 MRT+LES, Cs=0.1, Re=5000): size-independent checks.
 
     The FP32 kernel tracks the FP64 build of the same kernels, the closed
     cavity conserves mass, and the solution keeps the z-mirror symmetry of
