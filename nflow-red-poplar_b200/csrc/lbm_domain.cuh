@@ -32,7 +32,7 @@ struct lbm_domain {
   size_t elem = 4;    // bytes per stored population
   void* lat[2] = {nullptr, nullptr};
   int cur = 0;               // lattice holding f*_k
-  bool post_direct = false;  // lat[cur^1] holds arF_k itself
+  bool post_direct = false;  // A/B: lat[cur^1] holds arF_k itself; AA: complete natural layout
   long long step = 0;
   bool initialized = false;
   float* den[2] = {nullptr, nullptr};  // rho_k in den[k&1], rho_{k-1} in den[(k-1)&1]
@@ -138,9 +138,11 @@ inline int validate(const Inputval* in, const lbm_options* opt) {
       return set_error(LBM_ERR_INVALID, "unknown init_kind %d", opt->init_kind);
     if (opt->stream_mode != LBM_STREAM_AB && opt->stream_mode != LBM_STREAM_AA)
       return set_error(LBM_ERR_INVALID, "stream_mode %d not supported", opt->stream_mode);
-    if (opt->stream_mode == LBM_STREAM_AA && in->casetype != CAVITY)
+    if (opt->stream_mode == LBM_STREAM_AA && in->casetype != CAVITY && in->casetype != CHANNEL)
       return set_error(LBM_ERR_INVALID,
-                       "AA streaming is implemented for the cavity (casetype %d) only", CAVITY);
+                       "AA streaming is implemented for the cavity (casetype %d) and the channel "
+                       "(casetype %d) only",
+                       CAVITY, CHANNEL);
     if (opt->kernel < LBM_KERNEL_AUTO || opt->kernel > LBM_KERNEL_TMA)
       return set_error(LBM_ERR_INVALID, "unknown kernel %d", opt->kernel);
     if (!std::isfinite(opt->noise_amp) || !std::isfinite(opt->store_scale) ||

@@ -547,9 +547,21 @@ __global__ void __launch_bounds__(128)
 // of the neighbour step lies outside the box: a donor x - c_q outside reads
 // the node's own f*_{opp q} from (x, q); a destination x + c_q outside
 // writes the wall value of population opp q into the node's natural slot
-// (x, opp q).  A local step needs no boundary logic.  Same node arithmetic
-// as the pull step; the two kernels agree to within a few FP32 roundings
-// (the compiler may fuse a multiply-add differently in each).
+// (x, opp q).  Inlet and outlet rules (CHANNEL, kernel.cu:566-657) need the
+// face densities / velocities of the step before, which the neighbour step
+// is still computing when it writes: there the neighbour step writes the
+// plain f*_q into (x, opp q) like a fixed wall, and the rule is applied
+// when the natural slot is read (the next local step, the macroscopic and
+// export kernels), with the face buffers of that step.  The natural layout
+// is "complete" after the initial state and an import (every slot holds
+// arF, rules applied) and "pending" after a neighbour step.  Same node
+// arithmetic as the pull step; the two kernels agree to within a few FP32
+// roundings (the compiler may fuse a multiply-add differently in each).
+//
+// Face buffers: AA step k reads arF_{k-1} and writes its rho / u into
+// prho[k & 1] / pu[k & 1] (make_args with k); the rules for arF_{k-1} read
+// those of step k-1.  Kernels that read the state after step s therefore
+// take make_args with k = s + 1.
 // ------------------------------------------------------------------ //
 
 // arF of node (x, y, z) from the swapped layout
@@ -591,6 +603,24 @@ __device__ __forceinline__ RealOf<S> aa_wall(const StepArgs<S>& a, int t, RealOf
   return sub_rn(fo, term);
 }
 
+// Inlet / outlet rules of a node of the natural layout whose slots are
+// pending: each population whose donor x - c_q lies outside the box holds
+// the node's own f*_{opp q} (see above); replace it by the boundary value.
+template <class S>
+__device__ __forceinline__ void aa_open_face_rules(RealOf<S> (&f)[Q], const StepArgs<S>& a, int x,
+                                                   int y, int z) {
+  if (a.g.casetype != CHANNEL) return;
+  const int t = node_type(a.g, x, y, z);
+  if (t != NODE_INLET && t != NODE_OUTLET) return;
+  static_for<0, Q>([&](auto qc) {
+    constexpr int q = decltype(qc)::value;
+    const int xs = x - cx(q), ys = y - cy(q), zs = z - cz(q);
+    const bool inside = (unsigned)xs < (unsigned)a.g.nx && (unsigned)ys < (unsigned)a.g.ny &&
+                        (unsigned)zs < (unsigned)a.g.nz;
+    if (!inside) f[q] = boundary_value<S, q>(a, t, f[q], y, z);
+  });
+}
+
 // Slot addresses of an AA step, set per step in the kernel parameters so
 // that an interior node needs one address operation per access:
 //   local step:      a.srcd[q] = plane q,                 a.dstq[q] = plane opp q
@@ -607,12 +637,16 @@ struct AADst {
 };
 
 // One AA step; neighbor = 0: local step (natural -> swapped), 1: neighbour
-// step (swapped -> natural).  first = 1 for the first step after the
-// initial state: it collides with the rho, u that Initialize stored, as
-// k_init does for the pull form.  a.src = a.dst = the lattice.
+// step (swapped -> natural).  entry (local steps): kAAPending, the natural
+// slots are pending; kAAFromInit, the first step after the initial state,
+// which collides with the rho, u that Initialize stored, as k_init does for
+// the pull form; kAAComplete, the slots hold arF (after an import).
+// a.src = a.dst = the lattice.
+enum { kAAPending = 0, kAAFromInit = 1, kAAComplete = 2 };
+
 template <class S, int COLL, bool LES>
 __global__ void __launch_bounds__(128)
-    k_aa_step(const __grid_constant__ StepArgs<S> a, int neighbor, int first) {
+    k_aa_step(const __grid_constant__ StepArgs<S> a, int neighbor, int entry) {
   using R = RealOf<S>;
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int z = blockIdx.y, y = blockIdx.z;
@@ -626,8 +660,9 @@ __global__ void __launch_bounds__(128)
       constexpr int q = decltype(qc)::value;
       f[q] = ld(a.srcd[q] + cell, q, a.inv_scale);
     });
+    if (!neighbor && edge && entry == kAAPending) aa_open_face_rules<S>(f, a, x, y, z);
     const AADst<S> ad{a, cell};
-    if (!first) {
+    if (entry != kAAFromInit) {
       finish_node<S, COLL, LES>(f, a, ad, x, y, z);
     } else {
       const int t = node_type(a.g, x, y, z);
@@ -679,25 +714,29 @@ __global__ void __launch_bounds__(128)
   });
 }
 
-// rho and u of arF in the current AA layout (swapped = 1 after a local
-// step), written through a.den_out / a.ux_out...: the same arithmetic as the
-// step kernels' side outputs
+// rho and u of arF in the current AA layout, written through a.den_out /
+// a.ux_out...: the same arithmetic as the step kernels' side outputs.
+// layout: kAASwapped (after a local step), kAANaturalPending (after a
+// neighbour step), kAANaturalComplete.
+enum { kAANaturalComplete = 0, kAASwapped = 1, kAANaturalPending = 2 };
+
 template <class S>
 __global__ void __launch_bounds__(128) k_aa_macro(const __grid_constant__ StepArgs<S> a,
-                                                  int swapped) {
+                                                  int layout) {
   using R = RealOf<S>;
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int z = blockIdx.y, y = blockIdx.z;
   if (x >= a.g.nx) return;
   const int cell = x + a.g.px * (z + a.g.nz * y);
   R f[Q];
-  if (swapped) {
+  if (layout == kAASwapped) {
     aa_pull_swapped<S>(f, a, x, y, z, cell);
   } else {
     static_for<0, Q>([&](auto qc) {
       constexpr int q = decltype(qc)::value;
       f[q] = ld(a.srcq[q] + cell, q, a.inv_scale);
     });
+    if (layout == kAANaturalPending) aa_open_face_rules<S>(f, a, x, y, z);
   }
   PairState<R> ps;
   make_pairs<R>(f, ps);
@@ -706,13 +745,15 @@ __global__ void __launch_bounds__(128) k_aa_macro(const __grid_constant__ StepAr
   write_macro<S>(a, x, y, z, ps.rho, ux, uy, uz);
 }
 
-enum { kExportPull = 0, kExportDirect = 1, kExportAASwapped = 2 };
+enum { kExportPull = 0, kExportDirect = 1, kExportAASwapped = 2, kExportAANaturalPending = 3 };
 
 // ------------------------------------------------------------------ //
-// Export of arF_k into a device AoS buffer.  post_direct: a.src already
-// holds arF_k (right after initialize/import); otherwise a.src holds
-// f*_{k-1} and arF_k is reconstructed by the same pull + boundary code as
-// the step kernel.  Padded output zeroes the ghost layer.
+// Export of arF_k into a device AoS buffer.  kExportDirect: a.src holds
+// arF_k itself (right after initialize/import, or an AA lattice in the
+// complete natural layout); kExportPull: a.src holds f*_{k-1} and arF_k is
+// reconstructed by the same pull + boundary code as the step kernel; the
+// AA modes read the lattice in the swapped or the pending natural layout.
+// Padded output zeroes the ghost layer.
 // ------------------------------------------------------------------ //
 template <class S>
 __global__ void __launch_bounds__(128)
@@ -726,11 +767,12 @@ __global__ void __launch_bounds__(128)
   R f[Q];
   if (has_struct(a.g) && node_type(a.g, x, y, z) == NODE_STRUCT) {
     static_for<0, Q>([&](auto qc) { f[decltype(qc)::value] = R(0); });
-  } else if (mode == kExportDirect) {
+  } else if (mode == kExportDirect || mode == kExportAANaturalPending) {
     static_for<0, Q>([&](auto qc) {
       constexpr int q = decltype(qc)::value;
       f[q] = ld(a.src + q * a.qs + cell, q, a.inv_scale);
     });
+    if (mode == kExportAANaturalPending) aa_open_face_rules<S>(f, a, x, y, z);
   } else if (mode == kExportAASwapped) {
     aa_pull_swapped<S>(f, a, x, y, z, (int)cell);
   } else {

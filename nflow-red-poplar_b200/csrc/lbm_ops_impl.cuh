@@ -120,14 +120,17 @@ int ops_run_aa(lbm_domain* d, int nsteps) {
     };
     auto one = [&](bool den) {
       const long long k = d->step + 1;
-      k_aa_step<S, C, L><<<gr, b, 0, d->stream>>>(args(k, den, d->cur), d->cur,
-                                                  d->aa_first ? 1 : 0);
+      const int entry = d->aa_first ? kAAFromInit : (d->post_direct ? kAAComplete : kAAPending);
+      k_aa_step<S, C, L><<<gr, b, 0, d->stream>>>(args(k, den, d->cur), d->cur, entry);
       d->aa_first = false;
+      d->post_direct = false;
       d->cur ^= 1;
       d->step = k;
     };
     int left = nsteps;
-    if (d->aa_first && left > 0) {  // never inside a graph: it has its own collision
+    // the first step from a complete natural layout (initial state, import)
+    // has its own entry mode: never inside a graph
+    if ((d->aa_first || d->post_direct) && left > 0) {
       one(left <= 2);
       --left;
     }
@@ -141,7 +144,7 @@ int ops_run_aa(lbm_domain* d, int nsteps) {
         long long k = d->step;
         for (int i = 0; i < kGraphSteps; ++i) {
           ++k;
-          k_aa_step<S, C, L><<<gr, b, 0, d->capture>>>(args(k, false, cur), cur, 0);
+          k_aa_step<S, C, L><<<gr, b, 0, d->capture>>>(args(k, false, cur), cur, kAAPending);
           cur ^= 1;
         }
         cudaGraph_t graph;
@@ -163,13 +166,15 @@ int ops_run_aa(lbm_domain* d, int nsteps) {
       one(left <= 2);
       --left;
     }
-    StepArgs<S> m = make_args<S>(d, d->lat[0], d->lat[0], d->step);
+    // the state after step s: face buffers of AA step s (k = s + 1)
+    StepArgs<S> m = make_args<S>(d, d->lat[0], d->lat[0], d->step + 1);
     m.den_out = d->den[d->step & 1];
     m.ux_out = d->ux;
     m.uy_out = d->uy;
     m.uz_out = d->uz;
-    k_aa_macro<S><<<gr, b, 0, d->stream>>>(m, d->cur);
-    d->post_direct = false;
+    const int layout =
+        d->cur ? kAASwapped : (d->post_direct ? kAANaturalComplete : kAANaturalPending);
+    k_aa_macro<S><<<gr, b, 0, d->stream>>>(m, layout);
     CK(cudaGetLastError());
     return LBM_OK;
   });
@@ -197,8 +202,10 @@ int ops_import(lbm_domain* d, int padded) {
 template <class S>
 int ops_export(lbm_domain* d, int padded) {
   const bool aa = d->opt.stream_mode == LBM_STREAM_AA;
-  StepArgs<S> a = make_args<S>(d, d->lat[aa ? 0 : d->cur ^ 1], nullptr, d->step);
-  const int mode = aa ? (d->cur ? kExportAASwapped : kExportDirect)
+  // AA: the face buffers of AA step s are those of make_args with k = s + 1
+  StepArgs<S> a = make_args<S>(d, d->lat[aa ? 0 : d->cur ^ 1], nullptr, d->step + (aa ? 1 : 0));
+  const int mode = aa ? (d->cur ? kExportAASwapped
+                                : (d->post_direct ? kExportDirect : kExportAANaturalPending))
                       : (d->post_direct ? kExportDirect : kExportPull);
   const dim3 b = block_of(d->g.nx), gr = grid_of(d->g, b);
   k_export<S><<<gr, b, 0, d->stream>>>(a, d->staging, padded, mode);

@@ -1,5 +1,6 @@
 """AA-pattern streaming (one lattice, in place) against the pull (A/B) form
-and the oracle.
+and the oracle, for cavities and channels (inlet / outlet rules applied when
+the natural layout is read).
 
 The AA steps evaluate the same node arithmetic on the same populations.  The
 first step after the initial state gives the same bits as the pull form;
@@ -24,15 +25,26 @@ def cavity(nx, ny, nz, re=400.0, mrt=True, les=True):
                              cs=0.1, h=nx)
 
 
+def channel(nx, ny, nz, tau=0.56, mrt=True, les=True):
+    return pkg.make_inputval(nx, ny, nz, casetype=pkg.CHANNEL, tau=tau, u=0.05, mrt=mrt, les=les,
+                             cs=0.1)
+
+
 def pair(iv, storage=pkg.STORE_F32):
-    o = dict(storage=storage, init_kind=pkg.INIT_DENSITY_NOISE, noise_amp=1e-6)
+    if iv.casetype == pkg.CHANNEL:
+        o = dict(storage=storage, init_kind=pkg.INIT_CHANNEL, noise_amp=0.01)
+    else:
+        o = dict(storage=storage, init_kind=pkg.INIT_DENSITY_NOISE, noise_amp=1e-6)
     return (pkg.Domain(iv, pkg.default_options(stream_mode=pkg.STREAM_AA, **o)),
             pkg.Domain(iv, pkg.default_options(stream_mode=pkg.STREAM_AB, **o)))
 
 
+@pytest.mark.parametrize("case", ["cavity", "channel"])
 @pytest.mark.parametrize("mrt,les", [(True, True), (False, False), (True, False)])
-def test_aa_matches_pull(mrt, les):
-    aa, ab = pair(cavity(34, 21, 19, mrt=mrt, les=les))
+def test_aa_matches_pull(case, mrt, les):
+    iv = cavity(34, 21, 19, mrt=mrt, les=les) if case == "cavity" else \
+        channel(34, 13, 15, mrt=mrt, les=les)
+    aa, ab = pair(iv)
     np.testing.assert_array_equal(aa.export_arF(), ab.export_arF())  # initial state
     aa.run(1)
     ab.run(1)
@@ -54,18 +66,26 @@ def test_aa_matches_pull(mrt, les):
         assert da[7] == db[7] == 0
 
 
-def test_aa_import_and_checkpoint_continue(tmp_path):
-    aa, ab = pair(cavity(24, 20, 22))
+@pytest.mark.parametrize("case", ["cavity", "channel"])
+def test_aa_import_and_checkpoint_continue(tmp_path, case):
+    mk = (lambda: cavity(24, 20, 22)) if case == "cavity" else (lambda: channel(30, 12, 14))
+    aa, ab = pair(mk())
     ab.run(41)
     arF = ab.export_arF(padded=True)
     aa.import_arF(arF, padded=True)
-    ab2 = pkg.Domain(cavity(24, 20, 22))
+    np.testing.assert_array_equal(aa.export_arF(padded=True), arF)  # complete layout
+    ab2 = pkg.Domain(mk())
     ab2.import_arF(arF, padded=True)
-    aa.run(65)
-    ab2.run(65)
-    assert O.rel_field_err(aa.export_arF(), ab2.export_arF()) <= CLOSE
-    aa.save_checkpoint(tmp_path / "aa.bin")
-    c = pkg.Domain(cavity(24, 20, 22), pkg.default_options(stream_mode=pkg.STREAM_AA))
+    for steps in (1, 1, 65):  # from the complete layout, then pending / swapped
+        aa.run(steps)
+        ab2.run(steps)
+        assert O.rel_field_err(aa.export_arF(), ab2.export_arF()) <= CLOSE
+        den_a, *u_a = aa.macroscopic()
+        den_b, *u_b = ab2.macroscopic()
+        assert O.rel_field_err(den_a, den_b) <= CLOSE
+        assert O.rel_vel_err(u_a, u_b) <= CLOSE
+    aa.save_checkpoint(tmp_path / "aa.bin")  # odd step count: swapped layout
+    c = pkg.Domain(mk(), pkg.default_options(stream_mode=pkg.STREAM_AA))
     c.load_checkpoint(tmp_path / "aa.bin")
     c.run(10)
     aa.run(10)
@@ -74,9 +94,10 @@ def test_aa_import_and_checkpoint_continue(tmp_path):
     assert O.rel_field_err(c.export_arF(), aa.export_arF()) <= CLOSE
 
 
+@pytest.mark.parametrize("case", ["cavity", "channel"])
 @pytest.mark.parametrize("storage", [pkg.STORE_F16_SHIFT, pkg.STORE_BF16_SHIFT])
-def test_aa_16bit_close_to_pull(storage):
-    aa, ab = pair(cavity(40, 32, 28), storage)
+def test_aa_16bit_close_to_pull(storage, case):
+    aa, ab = pair(cavity(40, 32, 28) if case == "cavity" else channel(48, 16, 18), storage)
     aa.run(150)
     ab.run(150)
     ua = np.stack(aa.macroscopic()[1:])
@@ -85,13 +106,17 @@ def test_aa_16bit_close_to_pull(storage):
     assert np.abs(ua - ub).max() / np.abs(ub).max() <= tol
 
 
-def test_aa_vs_oracle():
-    iv = cavity(30, 26, 22)
-    aa = pkg.Domain(iv, pkg.default_options(stream_mode=pkg.STREAM_AA,
-                                            init_kind=pkg.INIT_DENSITY_NOISE, noise_amp=1e-6))
-    ref = O.Run(iv, init_kind=1, amp=1e-6)
-    aa.run(101)
-    ref.step(101)
+@pytest.mark.parametrize("case,steps", [("cavity", 101), ("channel", 250), ("channel", 251)])
+def test_aa_vs_oracle(case, steps):
+    if case == "cavity":
+        iv, kind, amp = cavity(30, 26, 22), 1, 1e-6
+    else:
+        iv, kind, amp = channel(40, 14, 18, tau=0.6), pkg.INIT_CHANNEL, 0.01
+    aa = pkg.Domain(iv, pkg.default_options(stream_mode=pkg.STREAM_AA, init_kind=kind,
+                                            noise_amp=amp))
+    ref = O.Run(iv, init_kind=kind, amp=amp)
+    aa.run(steps)
+    ref.step(steps)
     r = ref.fields()
     den, ux, uy, uz = aa.macroscopic()
     assert O.rel_field_err(den, r["den"]) <= 1e-5
@@ -103,9 +128,9 @@ def test_aa_halves_the_lattice_memory_and_rejects_other_cases():
     aa, ab = pair(iv)
     lat = 19 * 64 * 64 * 64 * 4
     assert ab.device_bytes() - aa.device_bytes() >= lat
-    ch = pkg.make_inputval(32, 16, 16, casetype=pkg.CHANNEL, tau=0.6, u=0.05)
+    pipe = pkg.make_inputval(32, 16, 16, casetype=pkg.POISEUILLE, tau=0.6, u=0.05)
     with pytest.raises(pkg.LbmError):
-        pkg.Domain(ch, pkg.default_options(stream_mode=pkg.STREAM_AA))
+        pkg.Domain(pipe, pkg.default_options(stream_mode=pkg.STREAM_AA))
     with pytest.raises(pkg.LbmError):
         aa.set_solid_mask(np.ones((64, 64, 64), bool))
     b = pkg.Batch(hbm_budget=64 << 20)
