@@ -366,14 +366,17 @@ def _case_iv(pkg, c):
 def report_batch(args, pkg):
     """256 independent domains in one persistent launch per step
     (CUDA-graph chunks, autotuned launch shape) vs each domain launched
-    alone, for FP32 and FP16-shift storage."""
+    alone, for FP32 and FP16-shift storage; --streaming aa keeps every
+    domain in one lattice (AA pattern), ab in two (pull)."""
     ndom = 256
+    mode = pkg.STREAM_AA if args.streaming == "aa" else pkg.STREAM_AB
     res = {"report": "batch", "domains": ndom, "steps": args.steps, "data": "synthetic (seeded)",
-           "forms": {}}
+           "streaming": args.streaming, "forms": {}}
     for sname, st in (("f32", pkg.STORE_F32), ("f16_shift", pkg.STORE_F16_SHIFT)):
         cases = _c4_domains(7, ndom, st)
         ivs = [_case_iv(pkg, c) for c in cases]
-        opts = [pkg.default_options(storage=st, init_kind=k, noise_amp=a, seed=i + 1)
+        opts = [pkg.default_options(storage=st, init_kind=k, noise_amp=a, seed=i + 1,
+                                    stream_mode=mode)
                 for i, (iv, k, a) in enumerate(ivs)]
         need = sum(pkg.batch_domain_bytes(iv, o) for (iv, _, _), o in zip(ivs, opts))
         b = pkg.Batch(hbm_budget=int(need * 1.02) + (64 << 20), chunk_steps=32)

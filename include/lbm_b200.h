@@ -158,8 +158,8 @@ enum {
 enum {
   LBM_STREAM_AB = 0,   /* pull, two population lattices (A/B)             */
   LBM_STREAM_AA = 1    /* in-place AA pattern, one lattice (half memory);
-                          CAVITY and CHANNEL cases, single domains (not
-                          batches, not with a solid mask)                   */
+                          CAVITY and CHANNEL cases, alone or as batch
+                          members (not with a solid mask)                   */
 };
 
 /* Kernel variant of the fused step (FP32-arithmetic storage formats). */

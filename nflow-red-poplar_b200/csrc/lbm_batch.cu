@@ -9,9 +9,11 @@
 // tile_off[] is the prefix sum over the active domains; a CTA walks the
 // global tile index t = blockIdx.x, += gridDim.x, finds its domain by binary
 // search and copies that domain's kernel arguments into shared memory.
-// Each node then runs step_node<S, COLL, LES>() — the very function of the
-// single-domain kernel — so a domain produces the same bits alone and in a
-// batch, whatever else is resident (no cross-domain data, no atomics).
+// Each node then runs step_node<S, COLL, LES>() (aa_step_node for members
+// with AA streaming) — the very function of the single-domain kernel — so a
+// domain produces the same bits alone and in a batch, whatever else is
+// resident (no cross-domain data, no atomics).  The kernels live in
+// lbm_batch_kernel.cuh, one translation unit per storage format.
 //
 // Graphs.  All kernel inputs live in device tables, so the graph of a chunk
 // (chunk_steps launches, launch j reading the tables) stays valid while the
@@ -20,189 +22,19 @@
 #include <map>
 #include <vector>
 
-#include "lbm_domain.cuh"
+#include "lbm_batch_kernel.cuh"
 
 using namespace lbm;
+using namespace lbm::batch;
 
 namespace {
 
-constexpr int kArgsBytes = 1024;  // one StepArgs<S> image, 16-byte multiple
-static_assert(sizeof(StepArgs<float>) <= kArgsBytes, "StepArgs too large");
-static_assert(sizeof(StepArgs<__half>) <= kArgsBytes, "StepArgs too large");
-static_assert(sizeof(StepArgs<__nv_bfloat16>) <= kArgsBytes, "StepArgs too large");
-// argument images per domain: lattice parity (2) x output kind (3: none,
-// rho, rho + u)
-constexpr int kImages = 6;
-
-// per active domain, per chunk
-struct SlotMeta {
-  int image_base;    // index of the domain's first argument image
-  int nx, nz;
-  int active;        // steps the domain takes in this chunk
-  unsigned long long mnx, mnz;  // ceil(2^64 / n): exact 32-bit division
-  long long nodes;
-  int cur0;          // lattice holding f* at chunk start
-  int pad;
-};
-
-// model: 0 SRT, 1 SRT+LES, 2 MRT, 3 MRT+LES; variant = storage * 4 + model
-// A launch group is the domains of one variant; each step launches the
-// group's kernel once.  Storage scales travel in the argument images.
-constexpr int kGroups = 32;
-
-// The domains of one group: meta[slot0 .. slot0 + nslots) and their tile
-// prefix sums tile_off[off0 .. off0 + nslots] (tiles of the group's list).
-struct GroupList {
-  int nslots;
-  int slot0;
-  int off0;
-  int pad;
-  long long ntiles;
-};
-
-struct BatchTables {
-  int tile;          // nodes per tile = block * npt
-  int schedule;      // 0: contiguous tile range per CTA, 1: grid-stride
-  GroupList v[kGroups];
-  const SlotMeta* meta;
-  const long long* tile_off;
-  const unsigned char* images;   // [capacity * kImages][kArgsBytes]
-};
-
-__device__ __forceinline__ unsigned fastdiv(unsigned n, unsigned long long m) {
-  return (unsigned)__umul64hi(m, (unsigned long long)n);
-}
-
-// the CTA's current domain, in shared memory: everything the tile loop
-// needs besides the tile index itself, so that little stays live in
-// registers across the node step
-struct CurSlot {
-  SlotMeta m;
-  long long begin, end;  // the domain's tiles [begin, end) in the group list
-  long long ntiles;      // tiles of the group
-  int s;                 // slot index in the group, -1 before the first
-  int ok;                // the domain takes step j
-  int image;             // argument image in img[], -1 = none
-  int fetch;             // image to copy into img[] on entry, -1 = none
-};
-
-// the nodes of local tile lt of the current domain
-template <class S, int COLL, bool LES>
-__device__ __forceinline__ void batch_tile(const StepArgs<S>& a, const CurSlot& cur,
-                                           unsigned lt, int npt) {
-  const unsigned base = lt * (unsigned)(blockDim.x * npt);
-  for (int i = 0; i < npt; ++i) {
-    const unsigned n = base + (unsigned)i * blockDim.x + threadIdx.x;
-    if (n >= (unsigned)cur.m.nodes) break;
-    const unsigned r = fastdiv(n, cur.m.mnx);
-    const int x = (int)(n - r * (unsigned)cur.m.nx);
-    const unsigned y = fastdiv(r, cur.m.mnz);
-    const int z = (int)(r - y * (unsigned)cur.m.nz);
-    step_node<S, COLL, LES>(a, x, (int)y, z);
-  }
-}
-
-// Make the slot holding tile t (at or after the current one) the CTA's
-// current domain: meta, tile range and, when it takes step j, its argument
-// image for launch j.  All threads of the CTA take the same path.
-__device__ __forceinline__ void enter_slot(CurSlot& cur, unsigned char* img,
-                                           const BatchTables* __restrict__ tab, int g, long long t,
-                                           int j) {
-  __syncthreads();  // every thread is done with the previous domain
-  if (threadIdx.x == 0) {
-    const GroupList& L = tab->v[g];
-    const long long* off = tab->tile_off + L.off0;
-    int lo = cur.s < 0 ? 0 : cur.s, hi = L.nslots;  // off[lo] <= t < off[hi]
-    while (hi - lo > 1) {
-      const int mid = (lo + hi) >> 1;
-      if (off[mid] <= t)
-        lo = mid;
-      else
-        hi = mid;
-    }
-    const SlotMeta m = tab->meta[L.slot0 + lo];
-    cur.m = m;
-    cur.s = lo;
-    cur.begin = off[lo];
-    cur.end = off[lo + 1];
-    cur.ok = j < m.active;
-    const int image = m.image_base + ((m.cur0 + j) & 1) * 3 +
-                      (j >= m.active - 1 ? 2 : (j >= m.active - 2 ? 1 : 0));
-    cur.fetch = cur.ok && image != cur.image ? image : -1;
-    if (cur.ok) cur.image = image;
-  }
-  __syncthreads();
-  const int fetch = cur.fetch;
-  if (fetch >= 0) {
-    const int4* src = reinterpret_cast<const int4*>(tab->images + (size_t)fetch * kArgsBytes);
-    int4* dst = reinterpret_cast<int4*>(img);
-    for (int i = threadIdx.x; i < kArgsBytes / 16; i += blockDim.x) dst[i] = src[i];
-    __syncthreads();
-  }
-}
-
-// One time step (launch j of a chunk) of every active domain of launch
-// group g (one variant).  Schedule 0 gives CTA c the
-// contiguous tiles [c*per, (c+1)*per) of the group's list; schedule 1 walks
-// t = blockIdx.x, += gridDim.x.  Either way the CTA moves forward through the
-// domains and reloads a domain's arguments only when it enters it.  The
-// domain's arguments and meta stay in shared memory (uniform over the CTA).
-// MINB (resident 256-thread CTAs the register budget must allow: 4 -> 64
-// registers, 3 -> 80) trades occupancy against spills; the autotuner picks.
-template <class S, int COLL, bool LES, int MINB>
-__global__ void __launch_bounds__(256, MINB) k_batch_step(const BatchTables* __restrict__ tab,
-                                                          int g, int j, int npt) {
-  __shared__ __align__(16) unsigned char img[kArgsBytes];
-  __shared__ CurSlot cur;
-  const StepArgs<S>& a = *reinterpret_cast<const StepArgs<S>*>(img);
-  if (threadIdx.x == 0) {
-    cur.s = -1;
-    cur.image = -1;
-    cur.end = 0;
-    cur.ntiles = tab->v[g].ntiles;
-  }
-  __syncthreads();
-  if (tab->schedule == 0) {
-    const long long per = (cur.ntiles + gridDim.x - 1) / gridDim.x;
-    const long long t0 = (long long)blockIdx.x * per;
-    for (long long t = t0; t < min(t0 + per, cur.ntiles); ++t) {
-      if (t >= cur.end) enter_slot(cur, img, tab, g, t, j);
-      if (!cur.ok) {
-        t = cur.end - 1;
-        continue;
-      }
-      batch_tile<S, COLL, LES>(a, cur, (unsigned)(t - cur.begin), npt);
-    }
-  } else {
-    for (long long t = blockIdx.x; t < cur.ntiles; t += gridDim.x) {
-      if (t >= cur.end) enter_slot(cur, img, tab, g, t, j);
-      if (!cur.ok) continue;
-      batch_tile<S, COLL, LES>(a, cur, (unsigned)(t - cur.begin), npt);
-    }
-  }
-}
-
-using BatchKernel = void (*)(const BatchTables*, int, int, int);
-
-template <class S, int MINB>
-constexpr BatchKernel batch_kernel_of(int model) {
-  return model == 0   ? k_batch_step<S, COLL_SRT, false, MINB>
-         : model == 1 ? k_batch_step<S, COLL_SRT, true, MINB>
-         : model == 2 ? k_batch_step<S, COLL_MRT, false, MINB>
-                      : k_batch_step<S, COLL_MRT, true, MINB>;
-}
-
-template <int MINB>
-BatchKernel batch_kernel_minb(int variant) {
-  const int st = variant >> 2, model = variant & 3;
-  return st == 0   ? batch_kernel_of<float, MINB>(model)
-         : st == 1 ? batch_kernel_of<__half, MINB>(model)
-                   : batch_kernel_of<__nv_bfloat16, MINB>(model);
-}
-
-// regs: 0 -> the 64-register build, 1 -> the 80-register build
+// variant -> kernel: storage = variant >> 3, model = (variant >> 1) & 3,
+// aa = variant & 1
 BatchKernel batch_kernel(int variant, int regs) {
-  return regs == 1 ? batch_kernel_minb<3>(variant) : batch_kernel_minb<4>(variant);
+  const int st = variant >> 3, model = (variant >> 1) & 3, aa = variant & 1;
+  const BatchKernels& t = st == 0 ? kBatch_f32 : (st == 1 ? kBatch_f16 : kBatch_bf16);
+  return t.k[model][regs == 1 ? 1 : 0][aa];
 }
 
 // First-fit device pool with coalescing (offsets 256-byte aligned).
@@ -288,6 +120,7 @@ struct lbm_batch {
     int image_slot = 0;       // index in the image table
     long long issued = 0;     // steps issued so far
     long long done_chunk = -1;  // chunk whose completion makes the result final
+    int last_active = 0;        // steps taken in the last chunk issued
   };
   std::map<int, Member> members;
   int next_id = 1;
@@ -339,7 +172,8 @@ int launch_grid(lbm_batch* b, int variant, int block, int* grid) {
 }
 
 int member_variant(const lbm_domain* d) {
-  return storage_index(d->opt.storage) * 4 + model_of(d->in);
+  return (storage_index(d->opt.storage) * 4 + model_of(d->in)) * 2 +
+         (d->opt.stream_mode == LBM_STREAM_AA ? 1 : 0);
 }
 
 // Launch groups (variants) of the members that still have steps to take,
@@ -361,7 +195,7 @@ int ensure_graph(lbm_batch* b, const std::vector<int>& groups) {
   const int block = launch_block(b), npt = launch_npt(b), steps = chunk_steps(b);
   const int sched = b->opt.schedule == 1 ? 1 : 0;
   if ((int)groups.size() > kGroups)
-    return set_error(LBM_ERR_INVALID, "more than %d (model, storage) groups in a batch", kGroups);
+    return set_error(LBM_ERR_INVALID, "more than %d (model, storage, streaming) groups in a batch", kGroups);
   if (b->graph && b->graph_block == block && b->graph_npt == npt && b->graph_steps == steps &&
       b->graph_groups == groups && b->graph_sched == sched &&
       b->graph_ctas == b->opt.ctas_per_sm && b->graph_regs == b->opt.regs)
@@ -408,11 +242,15 @@ int upload_images(lbm_batch* b, lbm_batch::Member& m) {
     if constexpr (std::is_same<S, double>::value) {
       return set_error(LBM_ERR_INVALID, "FP64 storage is not supported in batches");
     } else {
+      const bool aa = d->opt.stream_mode == LBM_STREAM_AA;
       for (int par = 0; par < 2; ++par)
         for (int kind = 0; kind < 3; ++kind) {
-          // a step starting from lattice `par` has step number of parity par^1
-          StepArgs<S> a = make_args<S>(d, d->lat[par], d->lat[par ^ 1], par ^ 1);
-          if (kind >= 1) a.den_out = d->den[par ^ 1];
+          // a step starting from lattice (AA: layout) `par` has step number
+          // of parity par^1; an AA step from layout par is a local (0) or a
+          // neighbour (1) step and writes rho of its input
+          StepArgs<S> a = aa ? aa_args<S>(d, par ^ 1, kind >= 1, par)
+                             : make_args<S>(d, d->lat[par], d->lat[par ^ 1], par ^ 1);
+          if (kind >= 1 && !aa) a.den_out = d->den[par ^ 1];
           if (kind == 2) {
             a.ux_out = d->ux;
             a.uy_out = d->uy;
@@ -488,6 +326,7 @@ int issue_chunk(lbm_batch* b, int steps_offered, long long* lups) {
   std::memset(b->h_tab->v, 0, sizeof(b->h_tab->v));
   int n = 0, noff = 0;
   long long updates = 0;
+  for (auto& kv : b->members) kv.second.last_active = 0;
   for (size_t g = 0; g < groups.size(); ++g) {
     GroupList& L = b->h_tab->v[g];
     L.slot0 = n;
@@ -508,7 +347,7 @@ int issue_chunk(lbm_batch* b, int steps_offered, long long* lups) {
       sm.nodes = d->N;
       sm.active = active;
       sm.cur0 = d->cur;
-      sm.pad = 0;
+      sm.entry0 = d->aa_first ? kAAFromInit : (d->post_direct ? kAAComplete : kAAPending);
       b->h_off[noff++] = tiles;
       tiles += (d->N + tile - 1) / tile;
       updates += d->N * active;
@@ -516,7 +355,9 @@ int issue_chunk(lbm_batch* b, int steps_offered, long long* lups) {
       d->step += active;
       d->cur ^= (active & 1);
       d->post_direct = false;
+      d->aa_first = false;
       m.issued += active;
+      m.last_active = active;
       if (m.issued >= m.target) m.done_chunk = b->chunks_issued + 1;
       ++n;
     }
@@ -536,6 +377,14 @@ int issue_chunk(lbm_batch* b, int steps_offered, long long* lups) {
   CK(cudaMemcpyAsync(b->d_tab, b->h_tab, sizeof(BatchTables), cudaMemcpyHostToDevice, b->stream));
   CK(cudaEventRecord(b->tables_free, b->stream));
   CK(cudaGraphLaunch(b->graph, b->stream));
+  // AA members: rho, u of the state the chunk ends in (a single-domain AA
+  // run ends the same way), before the chunk's completion event
+  for (auto& kv : b->members) {
+    lbm_domain* d = kv.second.d;
+    if (d->opt.stream_mode == LBM_STREAM_AA && kv.second.last_active > 0 &&
+        (rc = storage_ops(d->opt.storage).aa_macro(d)))
+      return rc;
+  }
   ++b->chunks_issued;
   cudaEvent_t ev;
   CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
@@ -671,8 +520,6 @@ int lbm_batch_add(lbm_batch* b, const Inputval* pinput, const lbm_options* opt,
     return set_error(LBM_ERR_INVALID, "FP64 storage is not supported in batches");
   if (opt && opt->kernel == LBM_KERNEL_PACKED)
     return set_error(LBM_ERR_INVALID, "batches use the one-node-per-thread kernel");
-  if (opt && opt->stream_mode == LBM_STREAM_AA)
-    return set_error(LBM_ERR_INVALID, "batches use the pull (A/B) streaming");
   CK(cudaSetDevice(b->opt.device));
   if (b->free_images.empty() && (rc = grow_images(b))) return rc;
   lbm_domain* d = new lbm_domain();

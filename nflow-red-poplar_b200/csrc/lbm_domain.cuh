@@ -233,6 +233,29 @@ StepArgs<S> make_args(const lbm_domain* d, const void* src, void* dst, long long
   return a;
 }
 
+// Arguments of AA step k (one lattice, lat[0]) with the slot tables of its
+// kind (k_aa_step):
+//   local step:      srcd[q] = plane q,                 dstq[q] = plane opp q
+//   neighbour step:  srcd[q] = plane opp q, minus off_q, dstq[q] = plane q, plus off_q
+// den: the step writes rho of its input arF_{k-1}.
+template <class S>
+StepArgs<S> aa_args(const lbm_domain* d, long long k, bool den, int neighbor) {
+  StepArgs<S> a = make_args<S>(d, d->lat[0], d->lat[0], k);
+  S* lat = (S*)d->lat[0];
+  for (int q = 0; q < Q; ++q) {
+    if (!neighbor) {
+      a.srcd[q] = lat + q * d->qs;
+      a.dstq[q] = lat + opp(q) * d->qs;
+    } else {
+      a.srcd[q] = lat + (opp(q) * d->qs - a.off[q]);
+      a.dstq[q] = lat + (q * d->qs + a.off[q]);
+    }
+  }
+  if (den) a.den_out = d->den[(k - 1) & 1];
+  a.aa_step = 1 + neighbor;
+  return a;
+}
+
 // kernel selection by (collision, LES) at run time
 template <class S, class F>
 int with_model(const lbm_domain* d, F&& f) {
@@ -512,6 +535,7 @@ struct StorageOps {
   int (*run_aa)(lbm_domain*, int nsteps);
   int (*import_staging)(lbm_domain*, int padded);
   int (*export_staging)(lbm_domain*, int padded);
+  int (*aa_macro)(lbm_domain*);  // rho, u of the AA state after step d->step
 };
 extern const StorageOps kOps_f32, kOps_f16, kOps_bf16, kOps_f64;
 inline const StorageOps& storage_ops(int storage) {

@@ -123,6 +123,8 @@ struct StepArgs {
   int init_kind;
   float noise_amp;
   unsigned long long seed;
+  // batched kernel: 0 pull step, 1 AA local step, 2 AA neighbour step
+  int aa_step;
 };
 
 template <class S>
@@ -636,7 +638,8 @@ struct AADst {
   __device__ __forceinline__ float nws(int c) const { return a.nws[c]; }
 };
 
-// One AA step; neighbor = 0: local step (natural -> swapped), 1: neighbour
+// One AA step of node (x, y, z) (shared by the single-domain and batched
+// kernels); neighbor = 0: local step (natural -> swapped), 1: neighbour
 // step (swapped -> natural).  entry (local steps): kAAPending, the natural
 // slots are pending; kAAFromInit, the first step after the initial state,
 // which collides with the rho, u that Initialize stored, as k_init does for
@@ -645,12 +648,9 @@ struct AADst {
 enum { kAAPending = 0, kAAFromInit = 1, kAAComplete = 2 };
 
 template <class S, int COLL, bool LES>
-__global__ void __launch_bounds__(128)
-    k_aa_step(const __grid_constant__ StepArgs<S> a, int neighbor, int entry) {
+__device__ __forceinline__ void aa_step_node(const StepArgs<S>& a, int x, int y, int z,
+                                             int neighbor, int entry) {
   using R = RealOf<S>;
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int z = blockIdx.y, y = blockIdx.z;
-  if (x >= a.g.nx) return;
   const int cell = x + a.g.px * (z + a.g.nz * y);
   const bool edge = (x == 0) | (x == a.g.nx - 1) | (y == 0) | (y == a.g.ny - 1) | (z == 0) |
                     (z == a.g.nz - 1);
@@ -712,6 +712,15 @@ __global__ void __launch_bounds__(128)
       StoreTraits<S>::store_fma(a.dst + (opp(q) * a.qs + cell), aa_wall<S>(a, t, v, q),
                                 a.scale, a.nws[wclass(q)]);
   });
+}
+
+template <class S, int COLL, bool LES>
+__global__ void __launch_bounds__(128)
+    k_aa_step(const __grid_constant__ StepArgs<S> a, int neighbor, int entry) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int z = blockIdx.y, y = blockIdx.z;
+  if (x >= a.g.nx) return;
+  aa_step_node<S, COLL, LES>(a, x, y, z, neighbor, entry);
 }
 
 // rho and u of arF in the current AA layout, written through a.den_out /

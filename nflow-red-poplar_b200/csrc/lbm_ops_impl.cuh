@@ -96,27 +96,31 @@ int ops_run_pull(lbm_domain* d, int nsteps) {
 // in graph chunks where possible; the last two steps write the rho of their
 // input arF (the previous-step density of the residual), then k_aa_macro
 // writes rho and u of the final arF.
+// rho and u of the AA state after step d->step into den[step & 1] and u,
+// from either layout; the face buffers are those of AA step s (k = s + 1)
+template <class S>
+int ops_aa_macro(lbm_domain* d) {
+  StepArgs<S> m = make_args<S>(d, d->lat[0], d->lat[0], d->step + 1);
+  m.den_out = d->den[d->step & 1];
+  m.ux_out = d->ux;
+  m.uy_out = d->uy;
+  m.uz_out = d->uz;
+  const int layout =
+      d->cur ? kAASwapped : (d->post_direct ? kAANaturalComplete : kAANaturalPending);
+  const dim3 b = block_of(d->g.nx), gr = grid_of(d->g, b);
+  k_aa_macro<S><<<gr, b, 0, d->stream>>>(m, layout);
+  CK(cudaGetLastError());
+  return LBM_OK;
+}
+
 template <class S>
 int ops_run_aa(lbm_domain* d, int nsteps) {
   return with_model<S>(d, [&](auto coll, auto les) -> int {
     constexpr int C = decltype(coll)::value;
     constexpr bool L = decltype(les)::value;
     const dim3 b = block_of(d->g.nx), gr = grid_of(d->g, b);
-    // slot tables of the two step kinds (see k_aa_step)
     auto args = [&](long long k, bool den, int neighbor) {
-      StepArgs<S> a = make_args<S>(d, d->lat[0], d->lat[0], k);
-      S* lat = (S*)d->lat[0];
-      for (int q = 0; q < Q; ++q) {
-        if (!neighbor) {
-          a.srcd[q] = lat + q * d->qs;
-          a.dstq[q] = lat + opp(q) * d->qs;
-        } else {
-          a.srcd[q] = lat + (opp(q) * d->qs - a.off[q]);
-          a.dstq[q] = lat + (q * d->qs + a.off[q]);
-        }
-      }
-      if (den) a.den_out = d->den[(k - 1) & 1];  // rho of the step's input arF_{k-1}
-      return a;
+      return aa_args<S>(d, k, den, neighbor);
     };
     auto one = [&](bool den) {
       const long long k = d->step + 1;
@@ -166,17 +170,7 @@ int ops_run_aa(lbm_domain* d, int nsteps) {
       one(left <= 2);
       --left;
     }
-    // the state after step s: face buffers of AA step s (k = s + 1)
-    StepArgs<S> m = make_args<S>(d, d->lat[0], d->lat[0], d->step + 1);
-    m.den_out = d->den[d->step & 1];
-    m.ux_out = d->ux;
-    m.uy_out = d->uy;
-    m.uz_out = d->uz;
-    const int layout =
-        d->cur ? kAASwapped : (d->post_direct ? kAANaturalComplete : kAANaturalPending);
-    k_aa_macro<S><<<gr, b, 0, d->stream>>>(m, layout);
-    CK(cudaGetLastError());
-    return LBM_OK;
+    return ops_aa_macro<S>(d);
   });
 }
 
@@ -222,6 +216,7 @@ StorageOps make_ops() {
   o.run_aa = &ops_run_aa<S>;
   o.import_staging = &ops_import<S>;
   o.export_staging = &ops_export<S>;
+  o.aa_macro = &ops_aa_macro<S>;
   return o;
 }
 

@@ -123,7 +123,7 @@ def test_aa_vs_oracle(case, steps):
     assert O.rel_vel_err((ux, uy, uz), (r["ux"], r["uy"], r["uz"])) <= 1e-5
 
 
-def test_aa_halves_the_lattice_memory_and_rejects_other_cases():
+def test_aa_halves_the_lattice_memory_and_rejects_struct_geometries():
     iv = cavity(64, 64, 64)
     aa, ab = pair(iv)
     lat = 19 * 64 * 64 * 64 * 4
@@ -133,7 +133,4 @@ def test_aa_halves_the_lattice_memory_and_rejects_other_cases():
         pkg.Domain(pipe, pkg.default_options(stream_mode=pkg.STREAM_AA))
     with pytest.raises(pkg.LbmError):
         aa.set_solid_mask(np.ones((64, 64, 64), bool))
-    b = pkg.Batch(hbm_budget=64 << 20)
-    with pytest.raises(pkg.LbmError):
-        b.add(cavity(16, 16, 16), pkg.default_options(stream_mode=pkg.STREAM_AA), 4)
-    b.close()
+
