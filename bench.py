@@ -463,7 +463,9 @@ def report_serving(args, pkg):
         while queue and backlog < backlog_cap:  # FIFO while the head fits the budget
             r = queue[0]
             iv, k, a = _case_iv(pkg, dict(e=r["e"], cavity=r["cavity"], re=r["re"], mrt=True))
-            o = pkg.default_options(storage=r["storage"], init_kind=k, noise_amp=a, seed=nxt + 1)
+            o = pkg.default_options(storage=r["storage"], init_kind=k, noise_amp=a, seed=nxt + 1,
+                                    stream_mode=(pkg.STREAM_AA if args.streaming == "aa"
+                                                 else pkg.STREAM_AB))
             try:
                 i = b.add(iv, o, r["steps"])
             except pkg.LbmError as ex:
@@ -499,6 +501,7 @@ def report_serving(args, pkg):
         return float(np.percentile(v, p)) if v else None
     print(json.dumps({
         "report": "serving", "rate_req_s": rate, "window_s": window, "budget_GB": budget / 1e9,
+        "streaming": args.streaming,
         "arrived": nxt, "admitted": admitted, "completed": len(tts), "queued_at_end": len(queue),
         "tts_p50_s": pct(tts, 50), "tts_p99_s": pct(tts, 99),
         "service_p50_s": pct(service, 50), "service_p99_s": pct(service, 99),
