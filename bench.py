@@ -368,7 +368,7 @@ def report_batch(args, pkg):
     (CUDA-graph chunks, autotuned launch shape) vs each domain launched
     alone, for FP32 and FP16-shift storage; --streaming aa keeps every
     domain in one lattice (AA pattern), ab in two (pull)."""
-    ndom = 256
+    ndom = args.domains
     mode = pkg.STREAM_AA if args.streaming == "aa" else pkg.STREAM_AB
     res = {"report": "batch", "domains": ndom, "steps": args.steps, "data": "synthetic (seeded)",
            "streaming": args.streaming, "forms": {}}
@@ -379,13 +379,17 @@ def report_batch(args, pkg):
                                     stream_mode=mode)
                 for i, (iv, k, a) in enumerate(ivs)]
         need = sum(pkg.batch_domain_bytes(iv, o) for (iv, _, _), o in zip(ivs, opts))
-        b = pkg.Batch(hbm_budget=int(need * 1.02) + (64 << 20), chunk_steps=32)
+        shape = {}
+        if args.batch_shape:  # fixed launch shape, no autotuning (profiling)
+            sc, rg, bl, npt = (int(v) for v in args.batch_shape.split(","))
+            shape = dict(schedule=sc, regs=rg, block=bl, nodes_per_thread=npt)
+        b = pkg.Batch(hbm_budget=int(need * 1.02) + (64 << 20), chunk_steps=32, **shape)
         t0 = time.perf_counter()
         for (iv, _, _), o in zip(ivs, opts):
             b.add(iv, o, 10 ** 9)
         b.sync()
         t_admit = time.perf_counter() - t0
-        cfg = b.autotune(trial_steps=32)
+        cfg = b.autotune(trial_steps=32) if not shape else dict(shape, fixed=True)
         b.step(args.warmup)
         b.sync()
         b.step(args.steps)
@@ -527,6 +531,12 @@ def main():
     ap.add_argument("--streaming", default="ab", choices=["ab", "aa"],
                     help="ab: pull between two lattices; aa: AA pattern in one lattice (cavity)")
     ap.add_argument("--report", default="", choices=["", "precision", "batch", "serving"])
+    ap.add_argument("--domains", type=int, default=256,
+                    help="batch: number of seeded domains (256 = the batched workload; fewer "
+                         "for a small profiling case)")
+    ap.add_argument("--batch-shape", default="",
+                    help="batch: fixed launch shape 'schedule,regs,block,nodes_per_thread' "
+                         "instead of autotuning")
     ap.add_argument("--rate", type=float, default=200.0, help="serving: arrivals per second")
     ap.add_argument("--window", type=float, default=60.0, help="serving: wall-clock window (s)")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="serving: HBM budget")
