@@ -714,13 +714,16 @@ __device__ __forceinline__ void aa_step_node(const StepArgs<S>& a, int x, int y,
   });
 }
 
-template <class S, int COLL, bool LES>
-__global__ void __launch_bounds__(128)
-    k_aa_step(const __grid_constant__ StepArgs<S> a, int neighbor, int entry) {
+// One kernel per step kind (NB = neighbor): the local step, which has no
+// box-face logic besides the open-face rules, fits 56 registers (9 CTAs of
+// 128 per SM) without spills; the neighbour step keeps 64.
+template <class S, int COLL, bool LES, int NB>
+__global__ void __launch_bounds__(128, NB ? 8 : 9)
+    k_aa_step(const __grid_constant__ StepArgs<S> a, int entry) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int z = blockIdx.y, y = blockIdx.z;
   if (x >= a.g.nx) return;
-  aa_step_node<S, COLL, LES>(a, x, y, z, neighbor, entry);
+  aa_step_node<S, COLL, LES>(a, x, y, z, NB, entry);
 }
 
 // rho and u of arF in the current AA layout, written through a.den_out /

@@ -125,7 +125,10 @@ int ops_run_aa(lbm_domain* d, int nsteps) {
     auto one = [&](bool den) {
       const long long k = d->step + 1;
       const int entry = d->aa_first ? kAAFromInit : (d->post_direct ? kAAComplete : kAAPending);
-      k_aa_step<S, C, L><<<gr, b, 0, d->stream>>>(args(k, den, d->cur), d->cur, entry);
+      if (d->cur)
+        k_aa_step<S, C, L, 1><<<gr, b, 0, d->stream>>>(args(k, den, 1), entry);
+      else
+        k_aa_step<S, C, L, 0><<<gr, b, 0, d->stream>>>(args(k, den, 0), entry);
       d->aa_first = false;
       d->post_direct = false;
       d->cur ^= 1;
@@ -148,7 +151,10 @@ int ops_run_aa(lbm_domain* d, int nsteps) {
         long long k = d->step;
         for (int i = 0; i < kGraphSteps; ++i) {
           ++k;
-          k_aa_step<S, C, L><<<gr, b, 0, d->capture>>>(args(k, false, cur), cur, kAAPending);
+          if (cur)
+            k_aa_step<S, C, L, 1><<<gr, b, 0, d->capture>>>(args(k, false, 1), kAAPending);
+          else
+            k_aa_step<S, C, L, 0><<<gr, b, 0, d->capture>>>(args(k, false, 0), kAAPending);
           cur ^= 1;
         }
         cudaGraph_t graph;
