@@ -154,6 +154,31 @@ def test_estimate_bytes():
     assert b2.value < b.value * 0.6
 
 
+def test_aa_streaming_cases_and_footprint():
+    """AA streaming: cavities and channels pass validation, POISEUILLE (STRUCT
+    geometry) does not; the footprint (single domain and batch member) drops
+    by one population lattice."""
+    L = pkg.lib()
+    h = C.c_void_p()
+    aa = pkg.default_options(stream_mode=pkg.STREAM_AA)
+    pipe = pkg.make_inputval(32, 16, 16, casetype=pkg.POISEUILLE, tau=0.6, u=0.05)
+    assert L.lbm_create(C.byref(pipe), C.byref(aa), C.byref(h)) == pkg.LBM_ERR_INVALID
+    assert b"AA streaming" in L.lbm_last_error()
+    for case in (pkg.CAVITY, pkg.CHANNEL):
+        iv = pkg.make_inputval(64, 32, 32, casetype=case, tau=0.6, u=0.05)
+        for st, size in ((pkg.STORE_F32, 4), (pkg.STORE_F16_SHIFT, 2)):
+            ab_o = pkg.default_options(storage=st, stream_mode=pkg.STREAM_AB)
+            aa_o = pkg.default_options(storage=st, stream_mode=pkg.STREAM_AA)
+            lattice = 19 * 64 * 32 * 32 * size
+            b_ab, b_aa = C.c_size_t(), C.c_size_t()
+            assert L.lbm_estimate_bytes(C.byref(iv), C.byref(ab_o), C.byref(b_ab)) == 0
+            assert L.lbm_estimate_bytes(C.byref(iv), C.byref(aa_o), C.byref(b_aa)) == 0
+            assert b_ab.value - b_aa.value >= lattice
+            assert pkg.batch_domain_bytes(iv, ab_o) - pkg.batch_domain_bytes(iv, aa_o) >= lattice
+    with pytest.raises(pkg.LbmError):
+        pkg.batch_domain_bytes(pipe, aa)
+
+
 def _has_gpu():
     try:
         import torch
