@@ -728,7 +728,7 @@ int lbm_batch_autotune(lbm_batch* b, int trial_steps, lbm_batch_options* chosen)
   for (int phase = 0; phase < 3 && !done; ++phase) {
     if (phase == 1) {
       stage.clear();
-      for (int np : {1, 4}) {
+      for (int np : {1, 4, 8}) {
         lbm_batch_options o = best_opt;
         o.nodes_per_thread = np;
         stage.push_back(o);
