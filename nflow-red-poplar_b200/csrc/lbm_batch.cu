@@ -440,8 +440,8 @@ int lbm_batch_create(const lbm_batch_options* bo, lbm_batch** out) {
     return set_error(LBM_ERR_INVALID, "chunk_steps must be even");
   if (o.block != 0 && o.block != 128 && o.block != 256)
     return set_error(LBM_ERR_INVALID, "block must be 128 or 256");
-  if (o.nodes_per_thread < 0 || o.nodes_per_thread > 8)
-    return set_error(LBM_ERR_INVALID, "nodes_per_thread must be 1..8");
+  if (o.nodes_per_thread < 0 || o.nodes_per_thread > 16)
+    return set_error(LBM_ERR_INVALID, "nodes_per_thread must be 1..16");
   if (o.schedule < 0 || o.schedule > 1) return set_error(LBM_ERR_INVALID, "schedule must be 0 or 1");
   if (o.regs < 0 || o.regs > 1) return set_error(LBM_ERR_INVALID, "regs must be 0 or 1");
   int ndev = 0;
@@ -728,7 +728,7 @@ int lbm_batch_autotune(lbm_batch* b, int trial_steps, lbm_batch_options* chosen)
   for (int phase = 0; phase < 3 && !done; ++phase) {
     if (phase == 1) {
       stage.clear();
-      for (int np : {1, 4, 8}) {
+      for (int np : {1, 4, 8, 16}) {
         lbm_batch_options o = best_opt;
         o.nodes_per_thread = np;
         stage.push_back(o);

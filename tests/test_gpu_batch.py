@@ -48,11 +48,11 @@ def alone(iv, o, steps):
 
 
 # launch shapes: (schedule, register build, block, nodes per thread)
-SHAPES = [(0, 0, 256, 2), (1, 1, 128, 1), (0, 1, 256, 4), (1, 0, 128, 3)]
+SHAPES = [(0, 0, 256, 2), (1, 1, 128, 1), (0, 1, 256, 4), (1, 0, 128, 3), (1, 0, 256, 16)]
 
 
 @pytest.mark.parametrize("shape", SHAPES, ids=["s0r0b256n2", "s1r1b128n1", "s0r1b256n4",
-                                               "s1r0b128n3"])
+                                               "s1r0b128n3", "s1r0b256n16"])
 @pytest.mark.parametrize("steps", [1, 37, 100])
 def test_batch_matches_alone_bit_for_bit(steps, shape):
     sched, regs, block, npt = shape
