@@ -275,29 +275,27 @@ def _enstrophy(ux, uy, uz):
     return 0.5 * float(w2.sum())
 
 
-def report_precision(args, pkg):
-    """Channel 512x128x128 MRT+LES, parabolic inlet u_max=0.05,
-    outlet rho=1, walls, 1 % seeded velocity perturbation, Re = u_max ny / nu
-    = 1000; the same run with FP16-shift, BF16-shift and FP32 storage against
-    the FP64 build."""
+def precision_c3(pkg, steps, kernel, size=None, warmup=0):
+    """Channel 512x128x128 MRT+LES, parabolic inlet u_max=0.05, outlet rho=1,
+    walls, 1 % seeded velocity perturbation, Re = u_max ny / nu = 1000; the
+    same run with FP16-shift, BF16-shift and FP32 storage against the FP64
+    build of the same kernels.  Errors of rho, u (max over nodes, rms and
+    relative L2 norm ||u - u64|| / ||u64||), kinetic energy and enstrophy."""
     import torch
     w = WORKLOADS["channel512x128x128_mrt_les"]
-    iv = make_case(pkg, w, args.size or None)
-    steps = args.steps
-    out = {"report": "precision", "workload": "channel512x128x128_mrt_les", "steps": steps,
+    iv = make_case(pkg, w, size)
+    out = {"workload": "channel512x128x128_mrt_les", "steps": steps,
            "nx": iv.nx, "ny": iv.ny, "nz": iv.nz, "re": w["re_ch"], "tau": float(iv.m_dTau),
            "data": "synthetic", "forms": {}}
-    kern = {"auto": pkg.KERNEL_AUTO, "scalar": pkg.KERNEL_SCALAR, "packed": pkg.KERNEL_PACKED,
-            "tma": pkg.KERNEL_TMA}[args.kernel]
 
-    def run(storage, kernel):
+    def run(storage, kern):
         o = pkg.default_options(storage=storage, init_kind=w["init"], noise_amp=w["amp"], seed=1,
-                                kernel=kernel)
+                                kernel=kern)
         d = pkg.Domain(iv, o)
-        d.run(args.warmup)
+        d.run(warmup)
         d.sync()
         t0 = time.perf_counter()
-        d.run(steps - args.warmup)
+        d.run(steps - warmup)
         d.sync()
         dt = time.perf_counter() - t0
         den, ux, uy, uz = d.macroscopic()
@@ -305,34 +303,68 @@ def report_precision(args, pkg):
         d.close()
         torch.cuda.synchronize()
         return dict(den=den, ux=ux, uy=uy, uz=uz, ke=float(diag[5]),
-                    mlups=iv.nx * iv.ny * iv.nz * (steps - args.warmup) / dt / 1e6,
+                    mlups=iv.nx * iv.ny * iv.nz * (steps - warmup) / dt / 1e6,
                     nonfinite=int(diag[7]))
 
     ref = run(pkg.STORE_F64, pkg.KERNEL_SCALAR)
     ens_ref = _enstrophy(ref["ux"], ref["uy"], ref["uz"])
-    umax = float(np.sqrt(ref["ux"].astype(np.float64) ** 2 + ref["uy"] ** 2 + ref["uz"] ** 2).max())
+    u2_ref = (ref["ux"].astype(np.float64) ** 2 + ref["uy"].astype(np.float64) ** 2 +
+              ref["uz"].astype(np.float64) ** 2)
+    umax = float(np.sqrt(u2_ref.max()))
     out["fp64"] = {"MLUPS": ref["mlups"], "kinetic_energy": ref["ke"], "enstrophy": ens_ref,
                    "max_u": umax}
     for name, st in (("f32", pkg.STORE_F32), ("f16_shift", pkg.STORE_F16_SHIFT),
                      ("bf16_shift", pkg.STORE_BF16_SHIFT)):
-        r = run(st, kern)
-        du = max(float(np.abs(r[k].astype(np.float64) - ref[k]).max()) for k in ("ux", "uy", "uz"))
+        r = run(st, kernel)
+        d2 = sum((r[k].astype(np.float64) - ref[k].astype(np.float64)) ** 2
+                 for k in ("ux", "uy", "uz"))
         ens = _enstrophy(r["ux"], r["uy"], r["uz"])
         out["forms"][name] = {
             "MLUPS": r["mlups"],
             "rho_max_abs_err": float(np.abs(r["den"].astype(np.float64) - ref["den"]).max()),
-            "u_max_err_rel_umax": du / umax,
-            "u_rms_err_rel_umax": float(np.sqrt(np.mean(
-                (r["ux"].astype(np.float64) - ref["ux"]) ** 2 +
-                (r["uy"].astype(np.float64) - ref["uy"]) ** 2 +
-                (r["uz"].astype(np.float64) - ref["uz"]) ** 2))) / umax,
+            "u_max_err_rel_umax": float(np.sqrt(d2.max())) / umax,
+            "u_rms_err_rel_umax": float(np.sqrt(d2.mean())) / umax,
+            "u_rel_l2_err": float(np.sqrt(d2.sum() / u2_ref.sum())),
             "kinetic_energy_rel_err": abs(r["ke"] - ref["ke"]) / abs(ref["ke"]),
             "enstrophy_rel_err": abs(ens - ens_ref) / abs(ens_ref),
             "nonfinite_nodes": r["nonfinite"]}
     f32 = out["forms"]["f32"]["MLUPS"]
     for name in ("f16_shift", "bf16_shift"):
         out["forms"][name]["speedup_vs_f32"] = out["forms"][name]["MLUPS"] / f32
+    return out
+
+
+def report_precision(args, pkg):
+    """--report precision: precision_c3 with --steps steps as one JSON line."""
+    kern = {"auto": pkg.KERNEL_AUTO, "scalar": pkg.KERNEL_SCALAR, "packed": pkg.KERNEL_PACKED,
+            "tma": pkg.KERNEL_TMA}[args.kernel]
+    out = precision_c3(pkg, args.steps, kern, args.size or None, args.warmup)
+    out["report"] = "precision"
     print(json.dumps(out), flush=True)
+
+
+def pattern_ceilings(pkg, n=256, iters=20):
+    """MLUPS / GB/s of the bare memory patterns of the step forms on an n^3
+    box (lbm_pattern_ceiling): the upper bound of any kernel with that
+    memory pattern."""
+    out = {}
+    for name, pat, st in (
+            ("copy_f32", pkg.PATTERN_COPY, pkg.STORE_F32),
+            ("copy_f16", pkg.PATTERN_COPY, pkg.STORE_F16_SHIFT),
+            ("pull_f32", pkg.PATTERN_PULL, pkg.STORE_F32),
+            ("pull_f16", pkg.PATTERN_PULL, pkg.STORE_F16_SHIFT),
+            ("pull_paired_f16", pkg.PATTERN_PULL_PAIRED, pkg.STORE_F16_SHIFT),
+            ("aa_local_f32", pkg.PATTERN_AA_LOCAL, pkg.STORE_F32),
+            ("aa_neighbor_f32", pkg.PATTERN_AA_NEIGHBOR, pkg.STORE_F32),
+            ("aa_local_f16", pkg.PATTERN_AA_LOCAL, pkg.STORE_F16_SHIFT),
+            ("aa_neighbor_f16", pkg.PATTERN_AA_NEIGHBOR, pkg.STORE_F16_SHIFT),
+            ("aa_local_v8_f16", pkg.PATTERN_AA_LOCAL_V8, pkg.STORE_F16_SHIFT),
+            ("aa_local_v16_f16", pkg.PATTERN_AA_LOCAL_V16, pkg.STORE_F16_SHIFT),
+            ("aa_local_v16_f32", pkg.PATTERN_AA_LOCAL_V16, pkg.STORE_F32)):
+        m, g = pkg.pattern_ceiling(pat, st, n, iters)
+        out[name] = {"MLUPS": round(m, 1), "GB_s": round(g, 1)}
+    out["box"] = f"{n}^3, {iters} timed launches after 3, CUDA events"
+    return out
 
 
 def _c4_domains(seed, n, storage):
@@ -545,6 +577,9 @@ def main():
                          "of work at --nominal-mlups (0 = HBM budget only)")
     ap.add_argument("--nominal-mlups", type=float, default=30000.0,
                     help="serving: throughput the backlog horizon is converted with")
+    ap.add_argument("--c3-steps", type=int, default=20000,
+                    help="steps of the precision comparison on the 512x128x128 channel that the "
+                         "default run reports (precision_c3)")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip cpu baseline, e2e and storage forms (profiling runs)")
     args = ap.parse_args()
@@ -691,6 +726,8 @@ def main():
         line["storage_forms"] = forms
         if rank == 0 and world == 1:
             line["cpu_baseline"] = cpu_baseline(pkg, w)
+            line["pattern_ceilings"] = pattern_ceilings(pkg)
+            line["precision_c3"] = precision_c3(pkg, args.c3_steps, pkg.KERNEL_AUTO)
     else:
         dom.close()
 

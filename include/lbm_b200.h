@@ -384,11 +384,15 @@ int lbm_save_file(lbm_domain* d, int savetype, const char* dir, int index);
  * library sized for at most 67,108,864 nodes (264 KB, held by every GPU that
  * loads the library until exit); larger n returns LBM_ERR_INVALID.
  * den_prev may be NULL (out[4] is then 0).  Work is ordered on `stream`
- * (a cudaStream_t, NULL = default stream) and the call synchronises it.
- * The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress); make that first call before any stream capture.
- * All calls on a device share the array: calls that overlap on the GPU race
- * and must be serialised by the caller. */
+ * (a cudaStream_t, NULL = default stream); every call synchronises that
+ * stream and copies the 8 results to the host before it returns.
+ * The first call on a device also looks up the array's device address
+ * (cudaGetSymbolAddress) and keeps it for later calls on that device; make
+ * that first call before any stream capture begins, and do not use the
+ * function across a cudaDeviceReset of the device (the kept address would
+ * be stale).  All calls on a device share the array and it keeps the last
+ * call's contents: calls that overlap on the GPU race and must be
+ * serialised by the caller. */
 int lbm_field_diagnostics_static(const float* den, const float* den_prev, const float* velx,
                                  const float* vely, const float* velz, long long n,
                                  double out[8], void* stream);
@@ -407,6 +411,31 @@ int lbm_estimate_bytes(const Inputval* pinput, const lbm_options* opt,
  * lbm_run_simulation call, measured with CUDA events on the handle's
  * stream around the kernel launches (synchronises). */
 int lbm_last_run_ms(lbm_domain* d, float* ms);
+
+/* ---------------------------------------------------------------------
+ * Memory-pattern ceilings (no counterpart in the reference: a measurement
+ * tool).  Times `iters` launches of a kernel that performs exactly the
+ * global loads and stores of one lattice update of a step form (19 loads
+ * and 19 stores per node, same addresses, access widths and thread
+ * mapping) with a token amount of arithmetic, on an n^3 box (n a multiple
+ * of 32, 32..512) of F32 or F16 storage, after 3 untimed launches.  No step
+ * kernel with that memory pattern can be faster.  *mlups = updated nodes per
+ * second / 1e6, *gbs = 2*19*bytes per node at that rate.  Allocates and
+ * frees two lattices of 19*n^3 elements; synchronises the device work it
+ * issued on its own stream.
+ * --------------------------------------------------------------------- */
+enum {
+  LBM_PATTERN_COPY = 0,         /* 19 planes in, 19 out, at the node, 16-byte vectors */
+  LBM_PATTERN_PULL = 1,         /* pull from x - c_q, one element per access   */
+  LBM_PATTERN_PULL_PAIRED = 2,  /* 16-bit rows as words (w, w + px/2): 32-bit
+                                   accesses, two nodes per thread              */
+  LBM_PATTERN_AA_LOCAL = 3,     /* AA local step, one element per access       */
+  LBM_PATTERN_AA_NEIGHBOR = 4,  /* AA neighbour step, one element per access   */
+  LBM_PATTERN_AA_LOCAL_V8 = 5,  /* AA local step, 8-byte vectors per lane      */
+  LBM_PATTERN_AA_LOCAL_V16 = 6  /* AA local step, 16-byte vectors per lane     */
+};
+int lbm_pattern_ceiling(int pattern, int storage, int n, int iters, double* mlups,
+                        double* gbs);
 
 /* ------------------------------------------------------------------ */
 /* Batches: many independent domains of uneven size resident on one    */
@@ -474,9 +503,13 @@ int lbm_batch_usage(lbm_batch* b, size_t* used, size_t* largest_free, int* ndoma
 int lbm_batch_domain_bytes(const Inputval* pinput, const lbm_options* opt, size_t* bytes);
 
 /* Project autotuner: run `trial_steps` real steps of the current batch with
- * each candidate (block, nodes per thread, CTAs per SM) and keep the
- * fastest; writes the choice into *chosen (may be NULL).  The trial steps
- * advance the domains like any other steps. */
+ * each candidate (register build, schedule, block, nodes per thread, CTAs per
+ * SM) and keep the fastest; writes the choice into *chosen (may be NULL).
+ * The trials consume the members' steps: up to 13 candidates each run
+ * `trial_steps` real steps, so up to 13 * trial_steps steps of every member
+ * count toward its target (a member that reaches its target stops, as in
+ * lbm_batch_step).  Tune on members whose targets leave room for this, or on
+ * throwaway members of the same mix. */
 int lbm_batch_autotune(lbm_batch* b, int trial_steps, lbm_batch_options* chosen);
 
 /* Average milliseconds per step of the last lbm_batch_step call, measured

@@ -42,6 +42,8 @@ STORE_F32, STORE_F16_SHIFT, STORE_BF16_SHIFT, STORE_F64 = 0, 1, 2, 3
 INIT_REFERENCE, INIT_DENSITY_NOISE, INIT_CHANNEL = 0, 1, 2
 STREAM_AB, STREAM_AA = 0, 1
 KERNEL_AUTO, KERNEL_SCALAR, KERNEL_PACKED, KERNEL_TMA = 0, 1, 2, 3
+(PATTERN_COPY, PATTERN_PULL, PATTERN_PULL_PAIRED, PATTERN_AA_LOCAL, PATTERN_AA_NEIGHBOR,
+ PATTERN_AA_LOCAL_V8, PATTERN_AA_LOCAL_V16) = range(7)
 
 
 class Inputval(C.Structure):
@@ -174,6 +176,8 @@ def lib():
                                              C.POINTER(C.c_size_t)]
         L.lbm_batch_autotune.argtypes = [vp, i32, C.POINTER(BatchOptions)]
         L.lbm_batch_last_step_ms.argtypes = [vp, C.POINTER(C.c_float), C.POINTER(C.c_longlong)]
+        L.lbm_pattern_ceiling.argtypes = [i32, i32, i32, i32, C.POINTER(C.c_double),
+                                          C.POINTER(C.c_double)]
         _lib = L
     return _lib
 
@@ -188,6 +192,14 @@ def check(rc):
     if rc < 0:
         raise LbmError(rc, lib().lbm_last_error().decode())
     return rc
+
+
+def pattern_ceiling(pattern, storage, n=256, iters=20):
+    """(MLUPS, GB/s) of a bare memory pattern of the step (lbm_pattern_ceiling)."""
+    m, g = C.c_double(), C.c_double()
+    check(lib().lbm_pattern_ceiling(int(pattern), int(storage), int(n), int(iters), C.byref(m),
+                                    C.byref(g)))
+    return m.value, g.value
 
 
 def default_options(**kw):

@@ -121,6 +121,7 @@ struct lbm_batch {
     long long issued = 0;     // steps issued so far
     long long done_chunk = -1;  // chunk whose completion makes the result final
     int last_active = 0;        // steps taken in the last chunk issued
+    cudaEvent_t admitted = nullptr;  // initial state and images written (batch stream)
   };
   std::map<int, Member> members;
   int next_id = 1;
@@ -401,6 +402,8 @@ void destroy_member(lbm_batch* b, lbm_batch::Member& m) {
                   d->inlet_u, d->prho[0], d->prho[1], d->pu[0], d->pu[1], d->flag};
   for (void* p : bufs) b->pool.release(p);
   d->stream = nullptr;  // the batch stream is not the domain's to destroy
+  if (m.admitted) cudaEventDestroy(m.admitted);
+  m.admitted = nullptr;
   free_all(d);
   delete d;
   m.d = nullptr;
@@ -566,6 +569,13 @@ int lbm_batch_add(lbm_batch* b, const Inputval* pinput, const lbm_options* opt,
   if ((rc = domain_upload_profile(d, b->stream)) || (rc = domain_launch_init(d, b->stream)) ||
       (rc = upload_images(b, b->members[new_id])))
     return undo(rc);
+  // a member counts as finished only once its initial state exists on the
+  // device: poll and fetch also wait for this event (a member with a step
+  // target of 0 has no chunk of its own to wait for)
+  if (cudaEventCreateWithFlags(&b->members[new_id].admitted, cudaEventDisableTiming) !=
+          cudaSuccess ||
+      cudaEventRecord(b->members[new_id].admitted, b->stream) != cudaSuccess)
+    return undo(set_error(LBM_ERR_CUDA, "member admission event"));
   if (target_steps == 0) b->members[new_id].done_chunk = b->chunks_issued;
   *id = new_id;
   return LBM_OK;
@@ -612,7 +622,8 @@ int lbm_batch_poll(lbm_batch* b, int* ids, int max, int* n) {
   int k = 0;
   for (auto& kv : b->members) {
     const lbm_batch::Member& m = kv.second;
-    if (m.issued >= m.target && m.done_chunk <= b->chunks_completed) {
+    if (m.issued >= m.target && m.done_chunk <= b->chunks_completed &&
+        (!m.admitted || cudaEventQuery(m.admitted) == cudaSuccess)) {
       if (k < max) ids[k] = kv.first;
       ++k;
     }
@@ -661,6 +672,9 @@ int lbm_batch_fetch(lbm_batch* b, int id, float* den, float* velx, float* vely, 
         break;
       }
   }
+  // the fields exist once the member's initial state has been built (the
+  // copies run on the fetch stream, not the batch stream)
+  if (m.admitted) CK(cudaStreamWaitEvent(b->fetch, m.admitted, 0));
   lbm_domain* d = m.d;
   const size_t nb = (size_t)d->N * sizeof(float);
   float* outs[4] = {den, velx, vely, velz};

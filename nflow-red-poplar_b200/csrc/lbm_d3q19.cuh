@@ -82,64 +82,61 @@ __host__ __device__ __forceinline__ void static_for(F&& f) {
 
 // ------------------------------------------------------------------ //
 // Storage formats.  R is the arithmetic type (float, or double for the
-// FP64 build).  Shifted 16-bit formats hold (f - w) * scale.
+// FP64 build).  The node arithmetic works on "internal" population values:
+// the populations f themselves for FP32 / FP64, and the deviations
+// g = f - w from the rest state for the shifted 16-bit formats, which hold
+// g * scale.  Carrying g through the arithmetic (not only through the
+// store) keeps every sum over populations a sum of small numbers: summed as
+// f = w + g, the FP32 roundings of the sums follow the fixed bit patterns
+// of the weights and add up to a systematic drift of the density (a mass
+// gain of ~3e-7 per node and step was measured that way), which g avoids.
 // ------------------------------------------------------------------ //
 template <class S>
 struct StoreTraits;
 template <>
 struct StoreTraits<float> {
   using R = float;
-  static constexpr bool shifted = false;
-  __device__ static __forceinline__ float from_raw(float h, float, float) { return h; }
-  __device__ static __forceinline__ float load(const float* p, float, float) { return *p; }
-  __device__ static __forceinline__ void store(float* p, float v, float, float) { *p = v; }
-  __device__ static __forceinline__ void store_fma(float* p, float v, float, float) { *p = v; }
+  static constexpr bool dev = false;  // internal value = f
+  __device__ static __forceinline__ float from_raw(float h, float) { return h; }
+  __device__ static __forceinline__ float load(const float* p, float) { return *p; }
+  __device__ static __forceinline__ void store(float* p, float v, float) { *p = v; }
 };
 template <>
 struct StoreTraits<double> {
   using R = double;
-  static constexpr bool shifted = false;
-  __device__ static __forceinline__ double from_raw(double h, double, double) { return h; }
-  __device__ static __forceinline__ double load(const double* p, double, double) { return *p; }
-  __device__ static __forceinline__ void store(double* p, double v, double, double) { *p = v; }
-  __device__ static __forceinline__ void store_fma(double* p, double v, float, float) { *p = v; }
+  static constexpr bool dev = false;
+  __device__ static __forceinline__ double from_raw(double h, float) { return h; }
+  __device__ static __forceinline__ double load(const double* p, float) { return *p; }
+  __device__ static __forceinline__ void store(double* p, double v, float) { *p = v; }
 };
 template <>
 struct StoreTraits<__half> {
   using R = float;
-  static constexpr bool shifted = true;
-  // f from the stored value h
-  __device__ static __forceinline__ float from_raw(__half h, float w, float inv_scale) {
-    return fmaf(__half2float(h), inv_scale, w);
+  static constexpr bool dev = true;  // internal value = f - w
+  // g from the stored value h (exact: the scale is a power of two)
+  __device__ static __forceinline__ float from_raw(__half h, float inv_scale) {
+    return __half2float(h) * inv_scale;
   }
-  __device__ static __forceinline__ float load(const __half* p, float w, float inv_scale) {
-    return from_raw(*p, w, inv_scale);
+  __device__ static __forceinline__ float load(const __half* p, float inv_scale) {
+    return from_raw(*p, inv_scale);
   }
-  __device__ static __forceinline__ void store(__half* p, float v, float w, float scale) {
-    *p = __float2half_rn((v - w) * scale);
-  }
-  // the same value as store(): (v - w) * scale with scale a power of two is
-  // v * scale - w * scale rounded once; nws = -w * scale
-  __device__ static __forceinline__ void store_fma(__half* p, float v, float scale, float nws) {
-    *p = __float2half_rn(fmaf(v, scale, nws));
+  // h = g * scale, rounded once
+  __device__ static __forceinline__ void store(__half* p, float g, float scale) {
+    *p = __float2half_rn(g * scale);
   }
 };
 template <>
 struct StoreTraits<__nv_bfloat16> {
   using R = float;
-  static constexpr bool shifted = true;
-  __device__ static __forceinline__ float from_raw(__nv_bfloat16 h, float w, float inv_scale) {
-    return fmaf(__bfloat162float(h), inv_scale, w);
+  static constexpr bool dev = true;
+  __device__ static __forceinline__ float from_raw(__nv_bfloat16 h, float inv_scale) {
+    return __bfloat162float(h) * inv_scale;
   }
-  __device__ static __forceinline__ float load(const __nv_bfloat16* p, float w, float inv_scale) {
-    return from_raw(*p, w, inv_scale);
+  __device__ static __forceinline__ float load(const __nv_bfloat16* p, float inv_scale) {
+    return from_raw(*p, inv_scale);
   }
-  __device__ static __forceinline__ void store(__nv_bfloat16* p, float v, float w, float scale) {
-    *p = __float2bfloat16_rn((v - w) * scale);
-  }
-  __device__ static __forceinline__ void store_fma(__nv_bfloat16* p, float v, float scale,
-                                                   float nws) {
-    *p = __float2bfloat16_rn(fmaf(v, scale, nws));
+  __device__ static __forceinline__ void store(__nv_bfloat16* p, float g, float scale) {
+    *p = __float2bfloat16_rn(g * scale);
   }
 };
 
@@ -269,107 +266,6 @@ __device__ __forceinline__ void macroscopic(const V (&f)[Q], V& rho, V& ux, V& u
 }
 
 // ------------------------------------------------------------------ //
-// Smagorinsky eddy relaxation time (ComputeTurbulence_LES,
-// lbm_codelets.cpp:611-662).  The non-equilibrium momentum flux
-// Pi = sum c c (f - feq) is formed from the raw second moments and the
-// closed-form second moment of the D3Q19 equilibrium,
-// sum c_a c_b feq = rho/3 delta_ab + rho u_a u_b.
-//   tau_eddy = -tau/2 + 1/2 sqrt(tau^2 + 18 sqrt(2) Cs^2 sqrt(Pi:Pi) / rho)
-// les_c = 18*sqrt(2)*Cs^2 (host constant).
-// ------------------------------------------------------------------ //
-template <class V>
-__device__ __forceinline__ V les_tau_eddy(const V (&f)[Q], V rho, V ux, V uy, V uz, V tau,
-                                          V les_c) {
-  V pxx, pyy, pzz, pxy, pxz, pyz;
-  static_for<1, Q>([&](auto qc) {
-    constexpr int q = decltype(qc)::value;
-    // first terms: xx q=1, yy q=5, zz q=3, xy q=11, xz q=7, yz q=15
-    if constexpr (cx(q) != 0) {
-      if constexpr (q == 1) pxx = f[q];
-      else pxx = pxx + f[q];
-    }
-    if constexpr (cy(q) != 0) {
-      if constexpr (q == 5) pyy = f[q];
-      else pyy = pyy + f[q];
-    }
-    if constexpr (cz(q) != 0) {
-      if constexpr (q == 3) pzz = f[q];
-      else pzz = pzz + f[q];
-    }
-    if constexpr (cx(q) * cy(q) != 0) {
-      if constexpr (q == 11) pxy = f[q];
-      else pxy = acc_term<cx(q) * cy(q)>(pxy, f[q]);
-    }
-    if constexpr (cx(q) * cz(q) != 0) {
-      if constexpr (q == 7) pxz = -f[q];
-      else pxz = acc_term<cx(q) * cz(q)>(pxz, f[q]);
-    }
-    if constexpr (cy(q) * cz(q) != 0) {
-      if constexpr (q == 15) pyz = -f[q];
-      else pyz = acc_term<cy(q) * cz(q)>(pyz, f[q]);
-    }
-  });
-  const V r3 = rho * bc<V>(1.0 / 3.0);
-  const V jx = rho * ux, jy = rho * uy, jz = rho * uz;
-  const V txx = pxx - fma_(jx, ux, r3);
-  const V tyy = pyy - fma_(jy, uy, r3);
-  const V tzz = pzz - fma_(jz, uz, r3);
-  const V txy = pxy - jx * uy;
-  const V txz = pxz - jx * uz;
-  const V tyz = pyz - jy * uz;
-  V off = txy * txy;
-  off = fma_(txz, txz, off);
-  off = fma_(tyz, tyz, off);
-  V qq = txx * txx;
-  qq = fma_(tyy, tyy, qq);
-  qq = fma_(tzz, tzz, qq);
-  qq = fma_(bc<V>(2), off, qq);
-  return fma_(bc<V>(0.5), vsqrt(fma_(tau, tau, les_c * vsqrt(qq) / rho)), bc<V>(-0.5) * tau);
-}
-
-// ------------------------------------------------------------------ //
-// SRT collision of keCollision_SRT (kernel.cu:479-486):
-//   f* = f - (f - feq)/(tau + tau_eddy),
-//   feq = w rho (1 + 3 c.u + 4.5 (c.u)^2 - 1.5 u^2)
-// ------------------------------------------------------------------ //
-template <class V>
-__device__ __forceinline__ void collide_srt(V (&f)[Q], V rho, V ux, V uy, V uz, V inv_tau) {
-  V usq = ux * ux;
-  usq = fma_(uy, uy, usq);
-  usq = fma_(uz, uz, usq);
-  const V c0 = fma_(bc<V>(-1.5), usq, bc<V>(1));  // 1 - 1.5 u^2
-  const V wr0 = rho * bc<V>(1.0 / 3.0), wr1 = rho * bc<V>(1.0 / 18.0),
-          wr2 = rho * bc<V>(1.0 / 36.0);
-  static_for<0, Q>([&](auto qc) {
-    constexpr int q = decltype(qc)::value;
-    V br;
-    if constexpr (q == 0) {
-      br = c0;
-    } else {
-      V eu;
-      bool first = true;
-      if constexpr (cx(q) != 0) {
-        eu = first_term<cx(q)>(ux);
-        first = false;
-      }
-      if constexpr (cy(q) != 0) {
-        if (first) eu = first_term<cy(q)>(uy);
-        else eu = acc_term<cy(q)>(eu, uy);
-        first = false;
-      }
-      if constexpr (cz(q) != 0) {
-        if (first) eu = first_term<cz(q)>(uz);
-        else eu = acc_term<cz(q)>(eu, uz);
-      }
-      br = fma_(eu, fma_(bc<V>(4.5), eu, bc<V>(3)), c0);
-    }
-    const V wr = wclass(q) == 0 ? wr0 : (wclass(q) == 1 ? wr1 : wr2);
-    const V feq = wr * br;
-    f[q] = fma_(feq - f[q], inv_tau, f[q]);
-  });
-}
-
-// ------------------------------------------------------------------ //
 // MRT collision of Collision_MRT (lbm_codelets.cpp:449-544):
 //   m = M f;  dm_k = s_k (m_k - meq_k);  f* = f - M^-1 dm
 // with the d'Humieres equilibrium moments of lbm_codelets.cpp:468-486 and
@@ -381,88 +277,11 @@ template <class R>
 struct MrtParams {
   R rho0_inv;  // 1/RefDen
   R weps, wepsj, wxx;
+  // deviation arithmetic: M_2 . w - weps = 3 - weps, the part of the
+  // epsilon moment's difference m_2 - meq_2 that the deviations g do not
+  // carry (0 for the standard weps = 3, and 0 when the populations are f)
+  R e2c;
 };
-
-template <int K>
-__host__ __device__ constexpr bool mrt_relaxed() {
-  return !(K == 0 || K == 3 || K == 5 || K == 7);
-}
-// relaxation rate of moment K when it is a constant (0 = uses s_nu)
-template <int K>
-__host__ __device__ constexpr double mrt_rate_const() {
-  return K == 1 ? 1.19 : (K == 2 || K == 10 || K == 12) ? 1.4
-       : (K == 4 || K == 6 || K == 8) ? 1.2 : (K >= 16) ? 1.98 : 0.0;
-}
-
-template <class V, class R>
-__device__ __forceinline__ void collide_mrt(V (&f)[Q], V rho, V ux, V uy, V uz, V s_nu,
-                                            const MrtParams<R>& p) {
-  const V rho0_inv = bcast_param<V>(p.rho0_inv);
-  const V jx = rho * ux, jy = rho * uy, jz = rho * uz;
-  V jj = jx * jx;
-  jj = fma_(jy, jy, jj);
-  jj = fma_(jz, jz, jj);
-  const V jj0 = jj * rho0_inv;
-  const V jyy = jy * jy, jzz = jz * jz;
-  const V meq9 = rho0_inv * fma_(bc<V>(2) * jx, jx, -(jyy + jzz));
-  const V meq11 = rho0_inv * (jyy - jzz);
-  V dm[Q];
-  static_for<1, Q>([&](auto kc) {
-    constexpr int k = decltype(kc)::value;
-    if constexpr (mrt_relaxed<k>()) {
-      V m;
-      bool first = true;
-      static_for<0, Q>([&](auto jc) {
-        constexpr int j = decltype(jc)::value;
-        constexpr int c = mrt_m(k, j);
-        if constexpr (c != 0) {
-          if (first) m = first_term<c>(f[j]);
-          else m = acc_term<c>(m, f[j]);
-          first = false;
-        }
-      });
-      V meq;
-      if constexpr (k == 1) meq = fma_(bc<V>(19), jj0, bc<V>(-11) * rho);
-      if constexpr (k == 2) meq = fma_(bcast_param<V>(p.wepsj), jj0, bcast_param<V>(p.weps) * rho);
-      if constexpr (k == 4) meq = bc<V>(-2.0 / 3.0) * jx;
-      if constexpr (k == 6) meq = bc<V>(-2.0 / 3.0) * jy;
-      if constexpr (k == 8) meq = bc<V>(-2.0 / 3.0) * jz;
-      if constexpr (k == 9) meq = meq9;
-      if constexpr (k == 10) meq = bcast_param<V>(p.wxx) * meq9;
-      if constexpr (k == 11) meq = meq11;
-      if constexpr (k == 12) meq = bcast_param<V>(p.wxx) * meq11;
-      if constexpr (k == 13) meq = jx * jy * rho0_inv;
-      if constexpr (k == 14) meq = jy * jz * rho0_inv;
-      if constexpr (k == 15) meq = jz * jx * rho0_inv;
-      constexpr double inv_n2 = 1.0 / (double)mrt_norm2(k);
-      if constexpr (mrt_rate_const<k>() != 0.0) {
-        // constant rate: fold 1/|row|^2 into it at compile time
-        constexpr double sk = mrt_rate_const<k>() * inv_n2;
-        if constexpr (k >= 16)
-          dm[k] = bc<V>(sk) * m;
-        else
-          dm[k] = bc<V>(sk) * (m - meq);
-      } else {
-        dm[k] = (s_nu * bc<V>(inv_n2)) * (m - meq);
-      }
-    }
-  });
-  static_for<0, Q>([&](auto ic) {
-    constexpr int i = decltype(ic)::value;
-    V acc;
-    bool first = true;
-    static_for<1, Q>([&](auto kc) {
-      constexpr int k = decltype(kc)::value;
-      constexpr int c = mrt_m(k, i);
-      if constexpr (mrt_relaxed<k>() && c != 0) {
-        if (first) acc = first_term<c>(dm[k]);
-        else acc = acc_term<c>(acc, dm[k]);
-        first = false;
-      }
-    });
-    f[i] = f[i] - acc;
-  });
-}
 
 
 // ------------------------------------------------------------------ //
@@ -479,13 +298,18 @@ __host__ __device__ constexpr int pair_a(int p) {
   return t[p];
 }
 
+// rho is the sum of the internal values (the density for populations f,
+// rho - 1 for deviations g, as sum w = 1); rho_full is the density itself.
+// j = sum c f = sum c g (sum c w = 0).
 template <class V>
 struct PairState {
   V f0, s[9], d[9];
-  V rho, jx, jy, jz;  // rho and momentum sum c f
+  V rho, jx, jy, jz;  // sum of the internal values and momentum sum c f
+  V rho_full;
 };
 
-template <class V>
+// DEV: f holds deviations g = f - w (16-bit shifted storage)
+template <class V, bool DEV = false>
 __host__ __device__ __forceinline__ void make_pairs(const V (&f)[Q], PairState<V>& ps) {
   ps.f0 = f[0];
   static_for<0, 9>([&](auto pc) {
@@ -502,6 +326,10 @@ __host__ __device__ __forceinline__ void make_pairs(const V (&f)[Q], PairState<V
   diag = diag + ps.s[7];
   diag = diag + ps.s[8];
   ps.rho = ps.f0 + (acc + diag);
+  if constexpr (DEV)
+    ps.rho_full = ps.rho + bc<V>(1);
+  else
+    ps.rho_full = ps.rho;
   V jx = ps.d[0] + ps.d[3];
   jx = jx - ps.d[4];
   jx = jx + ps.d[5];
@@ -559,16 +387,21 @@ __host__ __device__ __forceinline__ V les_tau_eddy_pairs(const PairState<V>& ps,
 // post-collision population.  FROM_PAIRS: rebuild f_a, f_abar from s, d
 // (f is not read after make_pairs, which shortens its register lifetime);
 // otherwise f is updated in place.
-template <bool FROM_PAIRS, class V, class Emit>
+template <bool FROM_PAIRS, class V, bool DEV = false, class Emit>
 __host__ __device__ __forceinline__ void collide_srt_pairs(const V (&f)[Q], const PairState<V>& ps,
                                                            V ux, V uy, V uz, V inv_tau,
                                                            Emit&& emit) {
   V usq = ux * ux;
   usq = fma_(uy, uy, usq);
   usq = fma_(uz, uz, usq);
-  const V c0 = fma_(bc<V>(-1.5), usq, bc<V>(1));
-  const V rho = ps.rho;
-  emit(0, fma_((rho * bc<V>(1.0 / 3.0)) * c0 - ps.f0, inv_tau, ps.f0));
+  // DEV: feq - w = w (rho_int + rho (3 c.u + 4.5 (c.u)^2 - 1.5 u^2)) with
+  // rho_int = rho - 1, so that no term of size w is formed
+  const V c0 = DEV ? bc<V>(-1.5) * usq : fma_(bc<V>(-1.5), usq, bc<V>(1));
+  const V rho = ps.rho_full;
+  if constexpr (DEV)
+    emit(0, fma_(bc<V>(1.0 / 3.0) * fma_(rho, c0, ps.rho) - ps.f0, inv_tau, ps.f0));
+  else
+    emit(0, fma_((rho * bc<V>(1.0 / 3.0)) * c0 - ps.f0, inv_tau, ps.f0));
   const V wr1 = rho * bc<V>(1.0 / 18.0), wr2 = rho * bc<V>(1.0 / 36.0);
   static_for<0, 9>([&](auto pc) {
     constexpr int p = decltype(pc)::value;
@@ -589,7 +422,12 @@ __host__ __device__ __forceinline__ void collide_srt_pairs(const V (&f)[Q], cons
       else eu = acc_term<cz(a)>(eu, uz);
     }
     const V wr = wclass(a) == 1 ? wr1 : wr2;
-    const V even = wr * fma_(bc<V>(4.5) * eu, eu, c0);
+    V even;
+    if constexpr (DEV)
+      even = bc<V>(wclass(a) == 1 ? 1.0 / 18.0 : 1.0 / 36.0) *
+             fma_(rho, fma_(bc<V>(4.5) * eu, eu, c0), ps.rho);
+    else
+      even = wr * fma_(bc<V>(4.5) * eu, eu, c0);
     const V odd = (bc<V>(3) * wr) * eu;
     if constexpr (FROM_PAIRS) {
       // s* = s + (2 even - s) inv,  d* = d + (2 odd - d) inv
@@ -608,7 +446,11 @@ __host__ __device__ __forceinline__ void collide_srt_pairs(const V (&f)[Q], cons
 // formed from s/d, relaxation dm'_k = s_k (m_k - meq_k) / |row_k|^2, back
 // transform f_a -= E_p + O_p, f_abar -= E_p - O_p (or, FROM_PAIRS, the same
 // rebuilt from s - 2E and d - 2O).  emit(q, value) receives the results.
-template <bool FROM_PAIRS, class V, class R, class Emit>
+// DEV: f, s, d hold deviations g = f - w and ps.rho = rho - 1; every
+// equilibrium moment but meq_2 is then the same expression in ps.rho (the
+// rest state's moments M w are (1, -11, 3, 0, ...) and meq_1 = -11 rho + ...
+// is linear in rho), meq_2 adds the constant p.e2c.
+template <bool FROM_PAIRS, class V, class R, bool DEV = false, class Emit>
 __host__ __device__ __forceinline__ void collide_mrt_pairs(const V (&f)[Q], const PairState<V>& ps,
                                                            V s_nu, const MrtParams<R>& p,
                                                            Emit&& emit) {
@@ -649,8 +491,14 @@ __host__ __device__ __forceinline__ void collide_mrt_pairs(const V (&f)[Q], cons
   const V meq11 = rho0_inv * (jyy - jzz);
   // ---- relaxed, pre-scaled differences dm'_k = s_k (m_k - meq_k)/|row|^2 ----
   const V e1 = bc<V>(1.19 / 2394.0) * (m1 - fma_(bc<V>(19), jj0, bc<V>(-11) * rho));
-  const V e2 = bc<V>(1.4 / 252.0) *
-               (m2 - fma_(bcast_param<V>(p.wepsj), jj0, bcast_param<V>(p.weps) * rho));
+  V e2;
+  if constexpr (DEV)
+    e2 = bc<V>(1.4 / 252.0) *
+         ((m2 - fma_(bcast_param<V>(p.wepsj), jj0, bcast_param<V>(p.weps) * rho)) +
+          bcast_param<V>(p.e2c));
+  else
+    e2 = bc<V>(1.4 / 252.0) *
+         (m2 - fma_(bcast_param<V>(p.wepsj), jj0, bcast_param<V>(p.weps) * rho));
   const V e4 = bc<V>(1.2 / 40.0) * fma_(bc<V>(2.0 / 3.0), jx, m4);
   const V e6 = bc<V>(1.2 / 40.0) * fma_(bc<V>(2.0 / 3.0), jy, m6);
   const V e8 = bc<V>(1.2 / 40.0) * fma_(bc<V>(2.0 / 3.0), jz, m8);

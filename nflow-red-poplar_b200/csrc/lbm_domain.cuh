@@ -216,12 +216,9 @@ StepArgs<S> make_args(const lbm_domain* d, const void* src, void* dst, long long
   a.mp.weps = R(d->in.dWeps);
   a.mp.wepsj = R(d->in.dWepsj);
   a.mp.wxx = R(d->in.dWXX);
+  a.mp.e2c = kDev<S> ? R(3) - a.mp.weps : R(0);
   a.scale = d->scale;
   a.inv_scale = d->inv_scale;
-  for (int c = 0; c < 3; ++c) {
-    const float w = c == 0 ? 1.0f / 3.0f : (c == 1 ? 1.0f / 18.0f : 1.0f / 36.0f);
-    a.nws[c] = -w * d->scale;
-  }
   a.inlet_u = d->inlet_u;
   a.init_kind = d->opt.init_kind;
   a.noise_amp = d->opt.noise_amp;

@@ -33,6 +33,21 @@ namespace lbm {
 
 template <class S>
 using RealOf = typename StoreTraits<S>::R;
+// the node arithmetic of storage S works on deviations g = f - w
+template <class S>
+constexpr bool kDev = StoreTraits<S>::dev;
+
+// internal value of population q from the population f, and back
+template <class S, int q>
+__device__ __forceinline__ RealOf<S> to_internal(RealOf<S> f) {
+  if constexpr (kDev<S>) return f - weight<RealOf<S>>(q);
+  else return f;
+}
+template <class S, int q>
+__device__ __forceinline__ RealOf<S> to_population(RealOf<S> v) {
+  if constexpr (kDev<S>) return v + weight<RealOf<S>>(q);
+  else return v;
+}
 
 // round-to-nearest primitives that the compiler may not contract into FMA;
 // used where the reference's own rounding sequence is reproduced
@@ -103,7 +118,6 @@ struct StepArgs {
   const S* srcd[Q];            // srcq[q] - off[q]: the donor of a node is srcd[q][cell]
   S* dstq[Q];
   int off[Q];
-  float nws[3];                // -w * scale per weight class (16-bit stores)
   Geometry g;
   R tau, les_c, rho0;
   R ulx, uly, ulz;            // lid velocity (cavity)
@@ -127,15 +141,15 @@ struct StepArgs {
   int aa_step;
 };
 
+// internal value of a stored population
 template <class S>
-__device__ __forceinline__ RealOf<S> ld(const S* p, int q, float inv_scale) {
-  return StoreTraits<S>::load(p, weight<RealOf<S>>(q), inv_scale);
+__device__ __forceinline__ RealOf<S> ld(const S* p, int, float inv_scale) {
+  return StoreTraits<S>::load(p, inv_scale);
 }
 
 // Where the populations of a node live (cell = in-plane index of the node)
-// and the storage scales of the shifted 16-bit forms (f = h * inv_scale + w
-// on load, h = f * scale - w * scale on store, nws[c] = -w * scale for the
-// weight class c).  PlaneAddr takes the per-population plane pointers and
+// and the storage scales of the shifted 16-bit forms (g = h * inv_scale on
+// load, h = g * scale on store).  PlaneAddr takes the per-population plane pointers and
 // scales of StepArgs, wherever the arguments are held: in the kernel
 // parameter space (single-domain kernels) every pointer is a free operand;
 // in shared memory (the batched kernel) each is one broadcast load, issued
@@ -150,7 +164,6 @@ struct PlaneAddr {
   __device__ __forceinline__ S* out(int q) const { return a.dstq[q] + cell; }
   __device__ __forceinline__ float inv_scale() const { return a.inv_scale; }
   __device__ __forceinline__ float scale() const { return a.scale; }
-  __device__ __forceinline__ float nws(int c) const { return a.nws[c]; }
 };
 
 // Boundary value of population q at a node whose donor x - c_q is outside
@@ -196,6 +209,8 @@ __device__ __forceinline__ RealOf<S> boundary_value(const StepArgs<S>& a, int t,
     const R eu = R(cx(d)) * bx + R(cy(d)) * by + R(cz(d)) * bz;
     const double v = -(double)fo + 2.0 * (double)weight<R>(d) * (double)a.rho0 *
                                        (1.0 + 4.5 * ((double)eu * (double)eu) - 1.5 * (double)usq);
+    // deviations: g_q = f_q - w = -(g_d + w) + X - w (w_q = w_d)
+    if constexpr (kDev<S>) return R(v - 2.0 * (double)weight<R>(d));
     return R(v);
   }
   return fo;  // no rule for this node type: plain bounce-back
@@ -282,7 +297,7 @@ __device__ __forceinline__ void pull_struct(RealOf<S> (&f)[Q], const StepArgs<S>
       const R fo = ld(ad.own(opp(q)), opp(q), ad.inv_scale());
       f[q] = boundary_value<S, q>(a, t, fo, y, z);
     } else {
-      f[q] = initial_feq<R, q>(R(is.den), R(is.ux), R(is.uy), R(is.uz));
+      f[q] = to_internal<S, q>(initial_feq<R, q>(R(is.den), R(is.ux), R(is.uy), R(is.uz)));
     }
   });
 }
@@ -332,15 +347,15 @@ __device__ __forceinline__ void collide_node(const V (&f)[Q], const PairState<V>
     te = les_tau_eddy_pairs<V>(ps, ux, uy, uz, inv_rho, tau, bcast_param<V>(a.les_c));
   const V inv = vrcp(tau + te);
   if constexpr (COLL == COLL_SRT)
-    collide_srt_pairs<FROM_PAIRS, V>(f, ps, ux, uy, uz, inv, emit);
+    collide_srt_pairs<FROM_PAIRS, V, kDev<S>>(f, ps, ux, uy, uz, inv, emit);
   else
-    collide_mrt_pairs<FROM_PAIRS, V>(f, ps, inv, a.mp, emit);
+    collide_mrt_pairs<FROM_PAIRS, V, RealOf<S>, kDev<S>>(f, ps, inv, a.mp, emit);
 }
 
 // u = j * (1/rho); returns 1/rho
 template <class V>
 __device__ __forceinline__ V velocity(const PairState<V>& ps, V& ux, V& uy, V& uz) {
-  const V inv = vrcp(ps.rho);
+  const V inv = vrcp(ps.rho_full);
   ux = ps.jx * inv;
   uy = ps.jy * inv;
   uz = ps.jz * inv;
@@ -380,7 +395,7 @@ __device__ __forceinline__ void store_all(const StepArgs<S>& a, const RealOf<S> 
                                           long long cell) {
   static_for<0, Q>([&](auto qc) {
     constexpr int q = decltype(qc)::value;
-    StoreTraits<S>::store(a.dst + q * a.qs + cell, f[q], weight<RealOf<S>>(q), a.scale);
+    StoreTraits<S>::store(a.dst + q * a.qs + cell, f[q], a.scale);
   });
 }
 
@@ -392,7 +407,7 @@ struct StoreNode {
   long long cell;
   float scale;
   __device__ __forceinline__ void operator()(int q, RealOf<S> v) const {
-    StoreTraits<S>::store(base + q * qs + cell, v, weight<RealOf<S>>(q), scale);
+    StoreTraits<S>::store(base + q * qs + cell, v, scale);
   }
 };
 
@@ -403,12 +418,12 @@ __device__ __forceinline__ void finish_node(const RealOf<S> (&f)[Q], const StepA
                                             const Addr& ad, int x, int y, int z) {
   using R = RealOf<S>;
   PairState<R> ps;
-  make_pairs<R>(f, ps);
+  make_pairs<R, kDev<S>>(f, ps);
   R ux, uy, uz;
   const R inv_rho = velocity<R>(ps, ux, uy, uz);
-  write_macro<S>(a, x, y, z, ps.rho, ux, uy, uz);
+  write_macro<S>(a, x, y, z, ps.rho_full, ux, uy, uz);
   collide_node<S, COLL, LES, false, R>(f, ps, ux, uy, uz, inv_rho, a, [&](int q, R v) {
-    StoreTraits<S>::store_fma(ad.out(q), v, ad.scale(), ad.nws(wclass(q)));
+    StoreTraits<S>::store(ad.out(q), v, ad.scale());
   });
 }
 
@@ -473,15 +488,16 @@ __global__ void __launch_bounds__(128)
   const R rd = R(is.den), ux = R(is.ux), uy = R(is.uy), uz = R(is.uz);
   static_for<0, Q>([&](auto qc) {
     constexpr int q = decltype(qc)::value;
-    f[q] = initial_feq<R, q>(rd, ux, uy, uz);
+    f[q] = to_internal<S, q>(initial_feq<R, q>(rd, ux, uy, uz));
   });
   store_all<S>(a, f, cell);  // post-stream lattice
   write_macro<S>(a, x, y, z, rd, ux, uy, uz);
   if (!collided) return;  // AA streaming: the first step collides
   // the first step collides with the rho, u that Initialize stored
   PairState<R> ps;
-  make_pairs<R>(f, ps);
-  ps.rho = rd;
+  make_pairs<R, kDev<S>>(f, ps);
+  ps.rho = kDev<S> ? rd - R(1) : rd;
+  ps.rho_full = rd;
   ps.jx = mul_rn(rd, ux);  // rounded products: the AA form repeats them exactly
   ps.jy = mul_rn(rd, uy);
   ps.jz = mul_rn(rd, uz);
@@ -510,7 +526,7 @@ __global__ void __launch_bounds__(128)
   R f[Q];
   static_for<0, Q>([&](auto qc) {
     constexpr int q = decltype(qc)::value;
-    f[q] = R(aos[q + node * Q]);
+    f[q] = to_internal<S, q>(R(aos[q + node * Q]));
   });
   store_all<S>(a, f, cell);
   // re-read through the storage format so that the collided state starts
@@ -523,12 +539,18 @@ __global__ void __launch_bounds__(128)
     write_macro<S>(a, x, y, z, R(0), R(0), R(0), R(0));
     return;
   }
-  R rho, ux, uy, uz;
-  macroscopic<R>(f, rho, ux, uy, uz);  // CurrDen / CurrVel in the codelet's order
-  write_macro<S>(a, x, y, z, rho, ux, uy, uz);
-  if (!collided) return;  // AA streaming: the next step collides
+  R ux, uy, uz;
   PairState<R> ps;
-  make_pairs<R>(f, ps);
+  make_pairs<R, kDev<S>>(f, ps);
+  if constexpr (kDev<S>) {
+    velocity<R>(ps, ux, uy, uz);
+    write_macro<S>(a, x, y, z, ps.rho_full, ux, uy, uz);
+  } else {
+    R rho;
+    macroscopic<R>(f, rho, ux, uy, uz);  // CurrDen / CurrVel in the codelet's order
+    write_macro<S>(a, x, y, z, rho, ux, uy, uz);
+  }
+  if (!collided) return;  // AA streaming: the next step collides
   const R inv_rho = velocity<R>(ps, ux, uy, uz);
   collide_node<S, COLL, LES, false, R>(f, ps, ux, uy, uz, inv_rho, a,
                                        StoreNode<S>{collided, a.qs, cell, a.scale});
@@ -635,7 +657,6 @@ struct AADst {
   int cell;
   __device__ __forceinline__ S* out(int q) const { return a.dstq[q] + cell; }
   __device__ __forceinline__ float scale() const { return a.scale; }
-  __device__ __forceinline__ float nws(int c) const { return a.nws[c]; }
 };
 
 // One AA step of node (x, y, z) (shared by the single-domain and batched
@@ -672,13 +693,14 @@ __device__ __forceinline__ void aa_step_node(const StepArgs<S>& a, int x, int y,
       const R rd = R(is.den), ux = R(is.ux), uy = R(is.uy), uz = R(is.uz);
       write_macro<S>(a, x, y, z, rd, ux, uy, uz);
       PairState<R> ps;
-      make_pairs<R>(f, ps);
-      ps.rho = rd;
+      make_pairs<R, kDev<S>>(f, ps);
+      ps.rho = kDev<S> ? rd - R(1) : rd;
+      ps.rho_full = rd;
       ps.jx = mul_rn(rd, ux);
       ps.jy = mul_rn(rd, uy);
       ps.jz = mul_rn(rd, uz);
       collide_node<S, COLL, LES, false, R>(f, ps, ux, uy, uz, vrcp(rd), a, [&](int q, R v) {
-        StoreTraits<S>::store_fma(ad.out(q), v, ad.scale(), ad.nws(wclass(q)));
+        StoreTraits<S>::store(ad.out(q), v, ad.scale());
       });
     }
     return;
@@ -698,19 +720,18 @@ __device__ __forceinline__ void aa_step_node(const StepArgs<S>& a, int x, int y,
     }
   });
   PairState<R> ps;
-  make_pairs<R>(f, ps);
+  make_pairs<R, kDev<S>>(f, ps);
   R ux, uy, uz;
   const R inv_rho = velocity<R>(ps, ux, uy, uz);
-  write_macro<S>(a, x, y, z, ps.rho, ux, uy, uz);
+  write_macro<S>(a, x, y, z, ps.rho_full, ux, uy, uz);
   collide_node<S, COLL, LES, false, R>(f, ps, ux, uy, uz, inv_rho, a, [&](int q, R v) {
     const int xt = x + cx(q), yt = y + cy(q), zt = z + cz(q);
     const bool inside = (unsigned)xt < (unsigned)a.g.nx && (unsigned)yt < (unsigned)a.g.ny &&
                         (unsigned)zt < (unsigned)a.g.nz;
     if (inside)
-      StoreTraits<S>::store_fma(a.dstq[q] + cell, v, a.scale, a.nws[wclass(q)]);
+      StoreTraits<S>::store(a.dstq[q] + cell, v, a.scale);
     else
-      StoreTraits<S>::store_fma(a.dst + (opp(q) * a.qs + cell), aa_wall<S>(a, t, v, q),
-                                a.scale, a.nws[wclass(q)]);
+      StoreTraits<S>::store(a.dst + (opp(q) * a.qs + cell), aa_wall<S>(a, t, v, q), a.scale);
   });
 }
 
@@ -751,10 +772,10 @@ __global__ void __launch_bounds__(128) k_aa_macro(const __grid_constant__ StepAr
     if (layout == kAANaturalPending) aa_open_face_rules<S>(f, a, x, y, z);
   }
   PairState<R> ps;
-  make_pairs<R>(f, ps);
+  make_pairs<R, kDev<S>>(f, ps);
   R ux, uy, uz;
   velocity<R>(ps, ux, uy, uz);
-  write_macro<S>(a, x, y, z, ps.rho, ux, uy, uz);
+  write_macro<S>(a, x, y, z, ps.rho_full, ux, uy, uz);
 }
 
 enum { kExportPull = 0, kExportDirect = 1, kExportAASwapped = 2, kExportAANaturalPending = 3 };
@@ -795,9 +816,10 @@ __global__ void __launch_bounds__(128)
     node = (x + 1) + (long long)(a.g.nx + 2) * ((z + 1) + (long long)(a.g.nz + 2) * (y + 1));
   else
     node = x + (long long)a.g.nx * (z + (long long)a.g.nz * y);
+  const bool solid = has_struct(a.g) && node_type(a.g, x, y, z) == NODE_STRUCT;
   static_for<0, Q>([&](auto qc) {
     constexpr int q = decltype(qc)::value;
-    aos[q + node * Q] = (float)f[q];
+    aos[q + node * Q] = solid ? 0.0f : (float)to_population<S, q>(f[q]);
   });
 }
 
@@ -815,17 +837,15 @@ __device__ __forceinline__ F2 ld_pair<float>(const float* p, int, float) {
   return F2{*reinterpret_cast<const float2*>(p)};
 }
 template <>
-__device__ __forceinline__ F2 ld_pair<__half>(const __half* p, int q, float inv_scale) {
+__device__ __forceinline__ F2 ld_pair<__half>(const __half* p, int, float inv_scale) {
   const float2 h = __half22float2(*reinterpret_cast<const __half2*>(p));
-  const float w = weight<float>(q);
-  return F2{__ffma2_rn(h, make_float2(inv_scale, inv_scale), make_float2(w, w))};
+  return F2{__fmul2_rn(h, make_float2(inv_scale, inv_scale))};
 }
 template <>
-__device__ __forceinline__ F2 ld_pair<__nv_bfloat16>(const __nv_bfloat16* p, int q,
+__device__ __forceinline__ F2 ld_pair<__nv_bfloat16>(const __nv_bfloat16* p, int,
                                                      float inv_scale) {
   const float2 h = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(p));
-  const float w = weight<float>(q);
-  return F2{__ffma2_rn(h, make_float2(inv_scale, inv_scale), make_float2(w, w))};
+  return F2{__fmul2_rn(h, make_float2(inv_scale, inv_scale))};
 }
 
 template <class S>
@@ -835,16 +855,14 @@ __device__ __forceinline__ void st_pair<float>(float* p, F2 v, int, float) {
   *reinterpret_cast<float2*>(p) = v.v;
 }
 template <>
-__device__ __forceinline__ void st_pair<__half>(__half* p, F2 v, int q, float scale) {
-  const float w = weight<float>(q);
-  const float2 d = __fmul2_rn(__fadd2_rn(v.v, make_float2(-w, -w)), make_float2(scale, scale));
+__device__ __forceinline__ void st_pair<__half>(__half* p, F2 v, int, float scale) {
+  const float2 d = __fmul2_rn(v.v, make_float2(scale, scale));
   *reinterpret_cast<__half2*>(p) = __float22half2_rn(d);
 }
 template <>
-__device__ __forceinline__ void st_pair<__nv_bfloat16>(__nv_bfloat16* p, F2 v, int q,
+__device__ __forceinline__ void st_pair<__nv_bfloat16>(__nv_bfloat16* p, F2 v, int,
                                                        float scale) {
-  const float w = weight<float>(q);
-  const float2 d = __fmul2_rn(__fadd2_rn(v.v, make_float2(-w, -w)), make_float2(scale, scale));
+  const float2 d = __fmul2_rn(v.v, make_float2(scale, scale));
   *reinterpret_cast<__nv_bfloat162*>(p) = __float22bfloat162_rn(d);
 }
 
@@ -889,18 +907,18 @@ __global__ void __launch_bounds__(64, LBM_PACKED_MIN_BLOCKS) k_step2(const __gri
     });
   }
   PairState<F2> ps;
-  make_pairs<F2>(f, ps);
+  make_pairs<F2, kDev<S>>(f, ps);
   F2 ux, uy, uz;
   const F2 inv_rho = velocity<F2>(ps, ux, uy, uz);
   if (a.den_out || a.ux_out || a.g.casetype == CHANNEL) {
-    write_macro<S>(a, x0, y, z, ps.rho.v.x, ux.v.x, uy.v.x, uz.v.x);
-    if (two) write_macro<S>(a, x0 + 1, y, z, ps.rho.v.y, ux.v.y, uy.v.y, uz.v.y);
+    write_macro<S>(a, x0, y, z, ps.rho_full.v.x, ux.v.x, uy.v.x, uz.v.x);
+    if (two) write_macro<S>(a, x0 + 1, y, z, ps.rho_full.v.y, ux.v.y, uy.v.y, uz.v.y);
   }
   collide_node<S, COLL, LES, true, F2>(f, ps, ux, uy, uz, inv_rho, a, [&](int q, F2 v) {
     if (two)
       st_pair<S>(a.dstq[q] + cell, v, q, a.scale);
     else
-      StoreTraits<S>::store(a.dstq[q] + cell, v.v.x, weight<float>(q), a.scale);
+      StoreTraits<S>::store(a.dstq[q] + cell, v.v.x, a.scale);
   });
 }
 

@@ -108,17 +108,15 @@ __device__ __forceinline__ F2 lds_pair<float>(const float* p, int, float) {
   return F2{*reinterpret_cast<const float2*>(p)};
 }
 template <>
-__device__ __forceinline__ F2 lds_pair<__half>(const __half* p, int q, float inv_scale) {
+__device__ __forceinline__ F2 lds_pair<__half>(const __half* p, int, float inv_scale) {
   const float2 h = __half22float2(*reinterpret_cast<const __half2*>(p));
-  const float w = weight<float>(q);
-  return F2{__ffma2_rn(h, make_float2(inv_scale, inv_scale), make_float2(w, w))};
+  return F2{__fmul2_rn(h, make_float2(inv_scale, inv_scale))};
 }
 template <>
-__device__ __forceinline__ F2 lds_pair<__nv_bfloat16>(const __nv_bfloat16* p, int q,
+__device__ __forceinline__ F2 lds_pair<__nv_bfloat16>(const __nv_bfloat16* p, int,
                                                       float inv_scale) {
   const float2 h = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(p));
-  const float w = weight<float>(q);
-  return F2{__ffma2_rn(h, make_float2(inv_scale, inv_scale), make_float2(w, w))};
+  return F2{__fmul2_rn(h, make_float2(inv_scale, inv_scale))};
 }
 
 template <class S, int COLL, bool LES>
@@ -227,17 +225,17 @@ __global__ void __launch_bounds__(TmaCfg<S>::THREADS, 1)
           if constexpr (cx(q) == 0) {
             f[q] = lds_pair<S>(p, q, a.inv_scale);
           } else {
-            f[q] = mk2(StoreTraits<S>::load(p, weight<float>(q), a.inv_scale),
-                       StoreTraits<S>::load(p + 1, weight<float>(q), a.inv_scale));
+            f[q] = mk2(StoreTraits<S>::load(p, a.inv_scale),
+                       StoreTraits<S>::load(p + 1, a.inv_scale));
           }
         });
         PairState<F2> ps;
-        make_pairs<F2>(f, ps);
+        make_pairs<F2, kDev<S>>(f, ps);
         F2 ux, uy, uz;
         const F2 inv_rho = velocity<F2>(ps, ux, uy, uz);
         if (a.den_out || a.ux_out || a.g.casetype == CHANNEL) {
-          write_macro<S>(a, x, y, z, ps.rho.v.x, ux.v.x, uy.v.x, uz.v.x);
-          write_macro<S>(a, x + 1, y, z, ps.rho.v.y, ux.v.y, uy.v.y, uz.v.y);
+          write_macro<S>(a, x, y, z, ps.rho_full.v.x, ux.v.x, uy.v.x, uz.v.x);
+          write_macro<S>(a, x + 1, y, z, ps.rho_full.v.y, ux.v.y, uy.v.y, uz.v.y);
         }
         collide_node<S, COLL, LES, true, F2>(f, ps, ux, uy, uz, inv_rho, a, [&](int q, F2 v) {
           st_pair<S>(a.dstq[q] + cell, v, q, a.scale);

@@ -198,7 +198,7 @@ def test_autotune_keeps_results():
     b = pkg.Batch(hbm_budget=512 << 20, chunk_steps=8)
     ids = [b.add(iv, opts(st, k, a), 10 ** 6) for iv, st, k, a in CASES]
     cfg = b.autotune(trial_steps=8)
-    assert cfg["block"] in (128, 256) and cfg["nodes_per_thread"] in (1, 2, 4)
+    assert cfg["block"] in (128, 256) and cfg["nodes_per_thread"] in (1, 2, 4, 8, 16)
     done = b.member(ids[0]).steps()
     b.step(8)
     b.sync()

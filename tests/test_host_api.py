@@ -193,3 +193,15 @@ def test_no_device_is_reported_not_faked():
     with pytest.raises(pkg.LbmError) as e:
         pkg.Domain(iv)
     assert e.value.code in (pkg.LBM_ERR_NO_DEVICE, pkg.LBM_ERR_CUDA)
+
+
+def test_pattern_ceiling_rejects_bad_arguments():
+    """Argument checks of lbm_pattern_ceiling happen before any device call."""
+    m, g = C.c_double(), C.c_double()
+    L = pkg.lib()
+    for args in ((99, pkg.STORE_F32, 64, 2), (pkg.PATTERN_PULL, pkg.STORE_F64, 64, 2),
+                 (pkg.PATTERN_PULL_PAIRED, pkg.STORE_F32, 64, 2), (pkg.PATTERN_PULL, pkg.STORE_F32, 48, 2),
+                 (pkg.PATTERN_PULL, pkg.STORE_F32, 1024, 2), (pkg.PATTERN_PULL, pkg.STORE_F32, 64, 0)):
+        assert L.lbm_pattern_ceiling(*args, C.byref(m), C.byref(g)) == pkg.LBM_ERR_INVALID, args
+    assert L.lbm_pattern_ceiling(pkg.PATTERN_PULL, pkg.STORE_F32, 64, 2, None, None) == \
+        pkg.LBM_ERR_INVALID

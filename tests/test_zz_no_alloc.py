@@ -70,3 +70,26 @@ def test_static_diagnostics_without_previous_density_and_size_limit():
                                                 big.ctypes.data_as(C.c_void_p), None)
     assert rc == pkg.LBM_ERR_INVALID
     assert b"capacity" in pkg.lib().lbm_last_error()
+
+
+def test_static_diagnostics_on_the_256_cube_cavity_fields():
+    """The 256^3 MRT+LES cavity (Cs 0.1, Re 5000): 16,777,216 nodes, i.e.
+    1,024 partial-sum blocks reduced by the fixed-order final pass, checked
+    against lbm_diagnostics on the same state, twice in a row."""
+    torch = pytest.importorskip("torch")
+    iv = pkg.make_inputval(256, casetype=pkg.CAVITY, re=5000.0, u=0.1, mrt=True, les=True,
+                           cs=0.1)
+    dom = pkg.Domain(iv, pkg.default_options(init_kind=pkg.INIT_DENSITY_NOISE, noise_amp=1e-6))
+    assert 256 ** 3 // (256 * 64) == 1024
+    for _ in range(2):
+        dom.run(4)
+        prev = dom.macroscopic()[0]
+        dom.run(1)
+        den, ux, uy, uz = dom.macroscopic()
+        want = dom.diagnostics()
+        got = _static(torch, _dev(torch, den), _dev(torch, prev), _dev(torch, ux),
+                      _dev(torch, uy), _dev(torch, uz))
+        for k in (0, 1, 2, 3, 4, 5):
+            assert abs(got[k] - want[k]) <= 1e-12 * max(1.0, abs(want[k])), (k, got[k], want[k])
+        assert got[6] == want[6] and got[7] == want[7] == 0
+    dom.close()
