@@ -167,7 +167,11 @@ enum {
   LBM_KERNEL_AUTO = 0,    /* the fastest variant for the format             */
   LBM_KERNEL_SCALAR = 1,  /* one node per thread                            */
   LBM_KERNEL_PACKED = 2,  /* two nodes per thread, packed FP32 arithmetic   */
-  LBM_KERNEL_TMA = 3      /* TMA-staged tiles, persistent producer/consumer */
+  LBM_KERNEL_TMA = 3,     /* TMA-staged tiles, persistent producer/consumer */
+  LBM_KERNEL_PAIRED = 4   /* 16-bit pull form: rows stored as 32-bit words of
+                             the node pairs (x, x + px/2), two nodes per thread
+                             with packed FP32 arithmetic; the default (AUTO)
+                             of FP16/BF16 shifted storage with LBM_STREAM_AB  */
 };
 
 typedef struct lbm_options {

@@ -41,7 +41,7 @@ SAVE_VTU, SAVE_CSV = 0, 1
 STORE_F32, STORE_F16_SHIFT, STORE_BF16_SHIFT, STORE_F64 = 0, 1, 2, 3
 INIT_REFERENCE, INIT_DENSITY_NOISE, INIT_CHANNEL = 0, 1, 2
 STREAM_AB, STREAM_AA = 0, 1
-KERNEL_AUTO, KERNEL_SCALAR, KERNEL_PACKED, KERNEL_TMA = 0, 1, 2, 3
+KERNEL_AUTO, KERNEL_SCALAR, KERNEL_PACKED, KERNEL_TMA, KERNEL_PAIRED = 0, 1, 2, 3, 4
 (PATTERN_COPY, PATTERN_PULL, PATTERN_PULL_PAIRED, PATTERN_AA_LOCAL, PATTERN_AA_NEIGHBOR,
  PATTERN_AA_LOCAL_V8, PATTERN_AA_LOCAL_V16) = range(7)
 

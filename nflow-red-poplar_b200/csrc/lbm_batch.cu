@@ -521,12 +521,13 @@ int lbm_batch_add(lbm_batch* b, const Inputval* pinput, const lbm_options* opt,
   if (target_steps < 0) return set_error(LBM_ERR_INVALID, "negative step target");
   if (opt && opt->storage == LBM_STORE_F64)
     return set_error(LBM_ERR_INVALID, "FP64 storage is not supported in batches");
-  if (opt && opt->kernel == LBM_KERNEL_PACKED)
+  if (opt && (opt->kernel == LBM_KERNEL_PACKED || opt->kernel == LBM_KERNEL_PAIRED))
     return set_error(LBM_ERR_INVALID, "batches use the one-node-per-thread kernel");
   CK(cudaSetDevice(b->opt.device));
   if (b->free_images.empty() && (rc = grow_images(b))) return rc;
   lbm_domain* d = new lbm_domain();
   domain_prepare(d, pinput, opt);
+  d->g.paired = 0;  // the batched kernel steps plain rows
   d->opt.device = b->opt.device;
   d->pooled = true;
   d->stream = b->stream;

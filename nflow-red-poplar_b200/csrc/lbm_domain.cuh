@@ -143,8 +143,14 @@ inline int validate(const Inputval* in, const lbm_options* opt) {
                        "AA streaming is implemented for the cavity (casetype %d) and the channel "
                        "(casetype %d) only",
                        CAVITY, CHANNEL);
-    if (opt->kernel < LBM_KERNEL_AUTO || opt->kernel > LBM_KERNEL_TMA)
+    if (opt->kernel < LBM_KERNEL_AUTO || opt->kernel > LBM_KERNEL_PAIRED)
       return set_error(LBM_ERR_INVALID, "unknown kernel %d", opt->kernel);
+    if (opt->kernel == LBM_KERNEL_PAIRED &&
+        ((opt->storage != LBM_STORE_F16_SHIFT && opt->storage != LBM_STORE_BF16_SHIFT) ||
+         opt->stream_mode != LBM_STREAM_AB))
+      return set_error(LBM_ERR_INVALID,
+                       "the paired kernel is the 16-bit pull (A/B) form: FP16/BF16 shifted "
+                       "storage with LBM_STREAM_AB");
     if (!std::isfinite(opt->noise_amp) || !std::isfinite(opt->store_scale) ||
         opt->store_scale < 0.0f)
       return set_error(LBM_ERR_INVALID, "bad noise_amp/store_scale");
@@ -199,7 +205,8 @@ StepArgs<S> make_args(const lbm_domain* d, const void* src, void* dst, long long
   a.dst = (S*)dst;
   a.qs = d->qs;
   for (int q = 0; q < Q; ++q) {
-    a.off[q] = cx(q) + d->g.px * (cz(q) + d->g.nz * cy(q));
+    // paired rows: a node one step away in x is two elements away
+    a.off[q] = (d->g.paired ? 2 : 1) * cx(q) + d->g.px * (cz(q) + d->g.nz * cy(q));
     a.srcq[q] = src ? (const S*)src + q * d->qs : nullptr;
     a.srcd[q] = src ? (const S*)src + (q * d->qs - a.off[q]) : nullptr;
     a.dstq[q] = dst ? (S*)dst + q * d->qs : nullptr;
@@ -268,6 +275,17 @@ int with_model(const lbm_domain* d, F&& f) {
 // the scalar kernel for the FP64 build
 template <class S, int COLL, bool LES>
 void launch_step(const lbm_domain* d, const StepArgs<S>& a, cudaStream_t st) {
+  if constexpr (kDev<S>) {
+    if (d->g.paired) {
+      if (paired_kernel_applies(d->g))
+        k_step_paired<S, COLL, LES>
+            <<<dim3((d->g.px / 2 + 127) / 128, d->g.nz, d->g.ny), dim3(128), 0, st>>>(a);
+      else
+        k_step_rows<S, COLL, LES><<<grid_of(d->g, block_of(d->g.nx)), block_of(d->g.nx), 0,
+                                    st>>>(a);
+      return;
+    }
+  }
   if constexpr (!std::is_same<S, double>::value) {
     if (has_struct(d->g)) {
       // struct geometry: the per-node kernel (its pull checks every donor)
@@ -314,7 +332,8 @@ inline TensorMapEncodeFn tensor_map_encoder() {
 // kernel option then falls back to the scalar kernel) for FP64 storage.
 template <class S>
 int domain_tensor_maps(lbm_domain* d, int sm_count) {
-  if (d->opt.stream_mode == LBM_STREAM_AA) {  // the TMA kernel is a pull (A/B) kernel
+  if (d->opt.stream_mode == LBM_STREAM_AA || d->g.paired) {
+    // the TMA kernel is a pull (A/B) kernel over plain rows
     d->tmap_ok = false;
     return LBM_OK;
   }
@@ -437,6 +456,11 @@ inline void domain_prepare(lbm_domain* d, const Inputval* pinput, const lbm_opti
   d->g.px = s.px;
   d->g.casetype = pinput->casetype;
   d->g.solid = nullptr;
+  // 16-bit pull (A/B) domains use paired rows unless another kernel is asked for
+  const bool b16 =
+      d->opt.storage == LBM_STORE_F16_SHIFT || d->opt.storage == LBM_STORE_BF16_SHIFT;
+  d->g.paired = b16 && d->opt.stream_mode == LBM_STREAM_AB &&
+                (d->opt.kernel == LBM_KERNEL_AUTO || d->opt.kernel == LBM_KERNEL_PAIRED);
   d->N = s.N;
   d->qs = s.qs;
   d->elem = storage_bytes(d->opt.storage);

@@ -26,6 +26,8 @@
 // the other lattice (k_export), what it holds in arFTemp (post-collision)
 // is the lattice this kernel writes.
 #pragma once
+#include <cstring>
+
 #include "lbm_d3q19.cuh"
 #include "../../include/lbm_b200.h"
 
@@ -36,6 +38,12 @@ using RealOf = typename StoreTraits<S>::R;
 // the node arithmetic of storage S works on deviations g = f - w
 template <class S>
 constexpr bool kDev = StoreTraits<S>::dev;
+
+// The collision of the 16-bit forms rebuilds f*_a, f*_abar from the pair
+// sums (FROM_PAIRS in collide_node), in the per-node kernels as in the
+// two-node kernels, so that a node gets the same bits from either.
+template <class S>
+constexpr bool kFromPairs = StoreTraits<S>::dev;
 
 // internal value of population q from the population f, and back
 template <class S, int q>
@@ -61,8 +69,24 @@ __device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(
 struct Geometry {
   int nx, ny, nz, px;
   int casetype;
+  // paired rows (16-bit storage, pull form): element 2w of a row holds node
+  // w and element 2w + 1 node w + px/2, so that the 32-bit word w holds the
+  // node pair (w, w + px/2) and a donor one node away in x is one word away
+  // for both nodes of the pair (k_step_paired)
+  int paired;
   const unsigned char* solid;  // [ny][nz][nx], nonzero = STRUCT; may be null
 };
+
+// element of node x within its row (plain or paired rows)
+__host__ __device__ __forceinline__ int row_slot(int x, int px, bool paired) {
+  if (!paired) return x;
+  const int h = px >> 1;
+  return x < h ? 2 * x : 2 * (x - h) + 1;
+}
+// in-plane element index of node (x, y, z)
+__host__ __device__ __forceinline__ int cell_of(const Geometry& g, int x, int y, int z) {
+  return row_slot(x, g.px, g.paired != 0) + g.px * (z + g.nz * y);
+}
 
 // the geometry holds STRUCT nodes: POISEUILLE, or any case with a solid mask
 __host__ __device__ __forceinline__ bool has_struct(const Geometry& g) {
@@ -162,6 +186,25 @@ struct PlaneAddr {
   __device__ __forceinline__ const S* donor(int q) const { return a.srcd[q] + cell; }
   __device__ __forceinline__ const S* own(int q) const { return a.srcq[q] + cell; }
   __device__ __forceinline__ S* out(int q) const { return a.dstq[q] + cell; }
+  __device__ __forceinline__ float inv_scale() const { return a.inv_scale; }
+  __device__ __forceinline__ float scale() const { return a.scale; }
+};
+
+// The same per-node addressing for either row layout (a.g.paired): the
+// donor x - c_q of population q is addressed through its own row slot.
+// Used by the per-node kernels of paired domains (edge words, initial
+// state, import, export); a donor outside the box is never formed.
+template <class S>
+struct RowAddr {
+  const StepArgs<S>& a;
+  int x, y, z;
+  __device__ __forceinline__ RowAddr(const StepArgs<S>& args, int x_, int y_, int z_)
+      : a(args), x(x_), y(y_), z(z_) {}
+  __device__ __forceinline__ const S* donor(int q) const {
+    return a.srcq[q] + cell_of(a.g, x - cx(q), y - cy(q), z - cz(q));
+  }
+  __device__ __forceinline__ const S* own(int q) const { return a.srcq[q] + cell_of(a.g, x, y, z); }
+  __device__ __forceinline__ S* out(int q) const { return a.dstq[q] + cell_of(a.g, x, y, z); }
   __device__ __forceinline__ float inv_scale() const { return a.inv_scale; }
   __device__ __forceinline__ float scale() const { return a.scale; }
 };
@@ -422,7 +465,7 @@ __device__ __forceinline__ void finish_node(const RealOf<S> (&f)[Q], const StepA
   R ux, uy, uz;
   const R inv_rho = velocity<R>(ps, ux, uy, uz);
   write_macro<S>(a, x, y, z, ps.rho_full, ux, uy, uz);
-  collide_node<S, COLL, LES, false, R>(f, ps, ux, uy, uz, inv_rho, a, [&](int q, R v) {
+  collide_node<S, COLL, LES, kFromPairs<S>, R>(f, ps, ux, uy, uz, inv_rho, a, [&](int q, R v) {
     StoreTraits<S>::store(ad.out(q), v, ad.scale());
   });
 }
@@ -431,16 +474,20 @@ __device__ __forceinline__ void finish_node(const RealOf<S> (&f)[Q], const StepA
 // LES, collision, store.  Shared by the single-domain and batched kernels,
 // so a domain gets the same bits alone and in a batch (only where the
 // arguments are held differs, not the arithmetic).
-template <class S, int COLL, bool LES>
-__device__ __forceinline__ void step_node(const StepArgs<S>& a, int x, int y, int z) {
+template <class S, int COLL, bool LES, class Addr>
+__device__ __forceinline__ void step_node_at(const StepArgs<S>& a, const Addr& ad, int x, int y,
+                                             int z) {
   using R = RealOf<S>;
   // STRUCT nodes are never streamed, collided or measured (kernel.cu:294,
   // 323, 362, 464, 495, 1105)
   if (has_struct(a.g) && node_type(a.g, x, y, z) == NODE_STRUCT) return;
-  const PlaneAddr<S> ad(a, x + a.g.px * (z + a.g.nz * y));
   R f[Q];
   pull<S>(f, a, ad, x, y, z);
   finish_node<S, COLL, LES>(f, a, ad, x, y, z);
+}
+template <class S, int COLL, bool LES>
+__device__ __forceinline__ void step_node(const StepArgs<S>& a, int x, int y, int z) {
+  step_node_at<S, COLL, LES>(a, PlaneAddr<S>(a, x + a.g.px * (z + a.g.nz * y)), x, y, z);
 }
 
 // The fused step.  grid = (ceil(nx/blockDim.x), nz, ny), one thread per node.
@@ -473,7 +520,7 @@ __global__ void __launch_bounds__(128)
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int z = blockIdx.y, y = blockIdx.z;
   if (x >= a.g.nx) return;
-  const long long cell = x + (long long)a.g.px * (z + (long long)a.g.nz * y);
+  const long long cell = cell_of(a.g, x, y, z);
   const int t = node_type(a.g, x, y, z);
   R f[Q];
   if (t == NODE_STRUCT) {
@@ -501,7 +548,7 @@ __global__ void __launch_bounds__(128)
   ps.jx = mul_rn(rd, ux);  // rounded products: the AA form repeats them exactly
   ps.jy = mul_rn(rd, uy);
   ps.jz = mul_rn(rd, uz);
-  collide_node<S, COLL, LES, false, R>(f, ps, ux, uy, uz, vrcp(rd), a,
+  collide_node<S, COLL, LES, kFromPairs<S>, R>(f, ps, ux, uy, uz, vrcp(rd), a,
                                        StoreNode<S>{collided, a.qs, cell, a.scale});
 }
 
@@ -517,7 +564,7 @@ __global__ void __launch_bounds__(128)
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int z = blockIdx.y, y = blockIdx.z;
   if (x >= a.g.nx) return;
-  const long long cell = x + (long long)a.g.px * (z + (long long)a.g.nz * y);
+  const long long cell = cell_of(a.g, x, y, z);
   long long node;
   if (padded)
     node = (x + 1) + (long long)(a.g.nx + 2) * ((z + 1) + (long long)(a.g.nz + 2) * (y + 1));
@@ -552,7 +599,7 @@ __global__ void __launch_bounds__(128)
   }
   if (!collided) return;  // AA streaming: the next step collides
   const R inv_rho = velocity<R>(ps, ux, uy, uz);
-  collide_node<S, COLL, LES, false, R>(f, ps, ux, uy, uz, inv_rho, a,
+  collide_node<S, COLL, LES, kFromPairs<S>, R>(f, ps, ux, uy, uz, inv_rho, a,
                                        StoreNode<S>{collided, a.qs, cell, a.scale});
 }
 
@@ -699,7 +746,7 @@ __device__ __forceinline__ void aa_step_node(const StepArgs<S>& a, int x, int y,
       ps.jx = mul_rn(rd, ux);
       ps.jy = mul_rn(rd, uy);
       ps.jz = mul_rn(rd, uz);
-      collide_node<S, COLL, LES, false, R>(f, ps, ux, uy, uz, vrcp(rd), a, [&](int q, R v) {
+      collide_node<S, COLL, LES, kFromPairs<S>, R>(f, ps, ux, uy, uz, vrcp(rd), a, [&](int q, R v) {
         StoreTraits<S>::store(ad.out(q), v, ad.scale());
       });
     }
@@ -724,7 +771,7 @@ __device__ __forceinline__ void aa_step_node(const StepArgs<S>& a, int x, int y,
   R ux, uy, uz;
   const R inv_rho = velocity<R>(ps, ux, uy, uz);
   write_macro<S>(a, x, y, z, ps.rho_full, ux, uy, uz);
-  collide_node<S, COLL, LES, false, R>(f, ps, ux, uy, uz, inv_rho, a, [&](int q, R v) {
+  collide_node<S, COLL, LES, kFromPairs<S>, R>(f, ps, ux, uy, uz, inv_rho, a, [&](int q, R v) {
     const int xt = x + cx(q), yt = y + cy(q), zt = z + cz(q);
     const bool inside = (unsigned)xt < (unsigned)a.g.nx && (unsigned)yt < (unsigned)a.g.ny &&
                         (unsigned)zt < (unsigned)a.g.nz;
@@ -796,7 +843,7 @@ __global__ void __launch_bounds__(128)
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int z = blockIdx.y, y = blockIdx.z;
   if (x >= a.g.nx) return;
-  const long long cell = x + (long long)a.g.px * (z + (long long)a.g.nz * y);
+  const long long cell = cell_of(a.g, x, y, z);
   R f[Q];
   if (has_struct(a.g) && node_type(a.g, x, y, z) == NODE_STRUCT) {
     static_for<0, Q>([&](auto qc) { f[decltype(qc)::value] = R(0); });
@@ -808,6 +855,8 @@ __global__ void __launch_bounds__(128)
     if (mode == kExportAANaturalPending) aa_open_face_rules<S>(f, a, x, y, z);
   } else if (mode == kExportAASwapped) {
     aa_pull_swapped<S>(f, a, x, y, z, (int)cell);
+  } else if (a.g.paired) {
+    pull<S>(f, a, RowAddr<S>(a, x, y, z), x, y, z);
   } else {
     pull<S>(f, a, PlaneAddr<S>(a, (int)cell), x, y, z);
   }
@@ -920,6 +969,176 @@ __global__ void __launch_bounds__(64, LBM_PACKED_MIN_BLOCKS) k_step2(const __gri
     else
       StoreTraits<S>::store(a.dstq[q] + cell, v.v.x, a.scale);
   });
+}
+
+// ------------------------------------------------------------------ //
+// Paired rows: the 16-bit pull step with two nodes per thread and 32-bit
+// accesses only.
+//
+// With Geometry::paired, word w of a row holds the nodes (w, w + H),
+// H = px / 2.  The donors x - c_q of both nodes of a pair then lie in one
+// word of the donor row, shifted by c_x, so a thread loads one aligned
+// 32-bit word per population for two nodes (a warp reads 128 contiguous
+// bytes, as the FP32 kernel does for one node per thread), converts it with
+// one packed conversion and runs the node arithmetic on F2 lanes (packed
+// FP32: one instruction for both nodes).  Per pair: 19 word loads, 19 word
+// stores, one F2 collision.
+//
+// k_step_paired takes every word.  A thread loads, for each population,
+// the word beside its own (w - c_x) in the donor row, which holds the x
+// donors of both lanes except in the special words:
+//   - the seam: node H - 1 (lo of word H - 1) and node H (hi of word 0) are
+//     x neighbours held in different words;
+//   - x faces (x = 0, lo of word 0; x = nx - 1, a hi lane): the populations
+//     whose donor lies outside take the node's boundary rule from the
+//     node's own f*_{opp q};
+// where the beside word (read past the row end: the neighbouring row's
+// word, inside the allocation) is replaced lane by lane in a branch that
+// only those threads take (two or three per row).  Rows on a y or z face
+// take, for the populations whose donor row is outside, the wall rule of
+// each lane's node (the test is uniform along the row).  Hi lanes past the
+// last node (x >= nx when nx < px) compute on padding slots, which no real
+// node reads and nothing exports.  The node types and rules are those of
+// the per-node path, which steps the geometries with STRUCT nodes
+// (k_step_rows); the 16-bit units are built without multiply-add
+// contraction and both paths rebuild f* from the pair sums, so a node gets
+// the same bits from either.
+// ------------------------------------------------------------------ //
+template <class S>
+__device__ __forceinline__ F2 unpack_pair(uint32_t word, float inv_scale);
+template <>
+__device__ __forceinline__ F2 unpack_pair<__half>(uint32_t word, float inv_scale) {
+  __half2 h;
+  memcpy(&h, &word, 4);
+  return F2{__fmul2_rn(__half22float2(h), make_float2(inv_scale, inv_scale))};
+}
+template <>
+__device__ __forceinline__ F2 unpack_pair<__nv_bfloat16>(uint32_t word, float inv_scale) {
+  __nv_bfloat162 h;
+  memcpy(&h, &word, 4);
+  return F2{__fmul2_rn(__bfloat1622float2(h), make_float2(inv_scale, inv_scale))};
+}
+template <class S>
+__device__ __forceinline__ uint32_t pack_pair(F2 v, float scale);
+template <>
+__device__ __forceinline__ uint32_t pack_pair<__half>(F2 v, float scale) {
+  const __half2 h = __float22half2_rn(__fmul2_rn(v.v, make_float2(scale, scale)));
+  uint32_t word;
+  memcpy(&word, &h, 4);
+  return word;
+}
+template <>
+__device__ __forceinline__ uint32_t pack_pair<__nv_bfloat16>(F2 v, float scale) {
+  const __nv_bfloat162 h = __float22bfloat162_rn(__fmul2_rn(v.v, make_float2(scale, scale)));
+  uint32_t word;
+  memcpy(&word, &h, 4);
+  return word;
+}
+// the paired step kernel applies to the domain (else: k_step_rows); nx >=
+// 11 keeps both x faces out of each other's words and every hi lane's x + 1
+// donor of a real node inside the row
+__host__ __device__ __forceinline__ bool paired_kernel_applies(const Geometry& g) {
+  return !has_struct(g) && (g.px >> 1) <= g.nx - 2;
+}
+
+// Resident threads per SM the register budget is sized for: 1024 (64
+// registers per thread) measured fastest on the 256^3 cavity (55k MLUPS
+// against 48k at 768 and 50k at 896; more warps hide more load latency,
+// which outweighs the few spilled registers).
+#ifndef LBM_PAIRED_THREADS_PER_SM
+#define LBM_PAIRED_THREADS_PER_SM 1024
+#endif
+
+// grid = (ceil(H / 128), nz, ny), 128 threads, one word (two nodes) per
+// thread; a.srcd[q] = plane q minus the donor offset 2 c_x + px (c_z + nz c_y)
+template <class S, int COLL, bool LES>
+__global__ void __launch_bounds__(128, LBM_PAIRED_THREADS_PER_SM / 128)
+    k_step_paired(const __grid_constant__ StepArgs<S> a) {
+  static_assert(kDev<S>, "paired rows are a 16-bit layout");
+  const int H = a.g.px >> 1;
+  const int w = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int z = blockIdx.y, y = blockIdx.z;
+  if (w >= H) return;
+  const int xh = w + H;                             // node of the hi lane
+  const int e = 2 * w + a.g.px * (z + a.g.nz * y);  // the pair's word (lo slot)
+  const bool face_row = y == 0 || y == a.g.ny - 1 || z == 0 || z == a.g.nz - 1;
+  F2 f[Q];
+  if (!face_row) {
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      f[q] = unpack_pair<S>(*reinterpret_cast<const uint32_t*>(a.srcd[q] + e), a.inv_scale);
+    });
+  } else {
+    const int t_lo = node_type(a.g, w, y, z);
+    const int t_hi = xh < a.g.nx ? node_type(a.g, xh, y, z) : NODE_FLUID;
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      const bool inside = (unsigned)(y - cy(q)) < (unsigned)a.g.ny &&
+                          (unsigned)(z - cz(q)) < (unsigned)a.g.nz;
+      if (inside) {
+        f[q] = unpack_pair<S>(*reinterpret_cast<const uint32_t*>(a.srcd[q] + e), a.inv_scale);
+      } else {
+        const F2 fo = unpack_pair<S>(*reinterpret_cast<const uint32_t*>(a.srcq[opp(q)] + e),
+                                     a.inv_scale);
+        f[q] = mk2(boundary_value<S, q>(a, t_lo, fo.v.x, y, z),
+                   boundary_value<S, q>(a, t_hi, fo.v.y, y, z));
+      }
+    });
+  }
+  if (w == 0 || w == H - 1 || xh == a.g.nx - 1) {
+    // the seam and the x faces (see above), lane by lane
+    const int e0 = e - 2 * w;  // row start
+    const int t_lo = node_type(a.g, w, y, z);
+    const int t_hi = xh < a.g.nx ? node_type(a.g, xh, y, z) : NODE_FLUID;
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      if constexpr (cx(q) != 0) {
+        const bool inside = !face_row || ((unsigned)(y - cy(q)) < (unsigned)a.g.ny &&
+                                          (unsigned)(z - cz(q)) < (unsigned)a.g.nz);
+        if (inside) {
+          const int ws = cx(q) == 1 ? H - 1 : 0;  // the word across the seam
+          if ((cx(q) == 1 && w == 0) || (cx(q) == -1 && w == H - 1)) {
+            const uint32_t sw =
+                *reinterpret_cast<const uint32_t*>(a.srcd[q] + (e0 + 2 * ws + 2 * cx(q)));
+            const F2 v = unpack_pair<S>(sw, a.inv_scale);
+            if (cx(q) == 1)
+              f[q].v.y = v.v.x;  // x = H takes node H - 1
+            else
+              f[q].v.x = v.v.y;  // x = H - 1 takes node H
+          }
+          const bool lo_out = cx(q) == 1 && w == 0;
+          const bool hi_out = cx(q) == -1 && xh == a.g.nx - 1;
+          if (lo_out || hi_out) {
+            const F2 fo = unpack_pair<S>(*reinterpret_cast<const uint32_t*>(a.srcq[opp(q)] + e),
+                                         a.inv_scale);
+            if (lo_out) f[q].v.x = boundary_value<S, q>(a, t_lo, fo.v.x, y, z);
+            if (hi_out) f[q].v.y = boundary_value<S, q>(a, t_hi, fo.v.y, y, z);
+          }
+        }
+      }
+    });
+  }
+  PairState<F2> ps;
+  make_pairs<F2, true>(f, ps);
+  F2 ux, uy, uz;
+  const F2 inv_rho = velocity<F2>(ps, ux, uy, uz);
+  if (a.den_out || a.ux_out || a.g.casetype == CHANNEL) {
+    write_macro<S>(a, w, y, z, ps.rho_full.v.x, ux.v.x, uy.v.x, uz.v.x);
+    if (xh < a.g.nx) write_macro<S>(a, xh, y, z, ps.rho_full.v.y, ux.v.y, uy.v.y, uz.v.y);
+  }
+  collide_node<S, COLL, LES, true, F2>(f, ps, ux, uy, uz, inv_rho, a, [&](int q, F2 v) {
+    *reinterpret_cast<uint32_t*>(a.dstq[q] + e) = pack_pair<S>(v, a.scale);
+  });
+}
+
+// Paired domains the paired kernel does not apply to (STRUCT nodes, nx <
+// 11): the per-node step over paired rows.  grid = (ceil(nx/128), nz, ny).
+template <class S, int COLL, bool LES>
+__global__ void __launch_bounds__(128) k_step_rows(const __grid_constant__ StepArgs<S> a) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int z = blockIdx.y, y = blockIdx.z;
+  if (x >= a.g.nx) return;
+  step_node_at<S, COLL, LES>(a, RowAddr<S>(a, x, y, z), x, y, z);
 }
 
 // node type and inside mask per node, [ny][nz][nx]
