@@ -30,7 +30,8 @@ import time
 import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
-BYTES = {"f32": 4, "f16_shift": 2, "bf16_shift": 2, "f64": 8}
+BYTES = {"f32": 4, "f16_shift": 2, "bf16_shift": 2, "f64": 8, "f16_shift_sr": 2,
+         "bf16_shift_sr": 2}
 
 
 def load_package():
@@ -275,22 +276,24 @@ def _enstrophy(ux, uy, uz):
     return 0.5 * float(w2.sum())
 
 
-def precision_c3(pkg, steps, kernel, size=None, warmup=0):
+def precision_c3(pkg, steps, kernel, size=None, warmup=0, re=None):
     """Channel 512x128x128 MRT+LES, parabolic inlet u_max=0.05, outlet rho=1,
     walls, 1 % seeded velocity perturbation, Re = u_max ny / nu = 1000; the
     same run with FP16-shift, BF16-shift and FP32 storage against the FP64
     build of the same kernels.  Errors of rho, u (max over nodes, rms and
     relative L2 norm ||u - u64|| / ||u64||), kinetic energy and enstrophy."""
     import torch
-    w = WORKLOADS["channel512x128x128_mrt_les"]
+    w = dict(WORKLOADS["channel512x128x128_mrt_les"])
+    if re:
+        w["re_ch"] = float(re)
     iv = make_case(pkg, w, size)
     out = {"workload": "channel512x128x128_mrt_les", "steps": steps,
            "nx": iv.nx, "ny": iv.ny, "nz": iv.nz, "re": w["re_ch"], "tau": float(iv.m_dTau),
            "data": "synthetic", "forms": {}}
 
-    def run(storage, kern):
+    def run(storage, kern, rounding=0):
         o = pkg.default_options(storage=storage, init_kind=w["init"], noise_amp=w["amp"], seed=1,
-                                kernel=kern)
+                                kernel=kern, rounding=rounding)
         d = pkg.Domain(iv, o)
         d.run(warmup)
         d.sync()
@@ -313,9 +316,11 @@ def precision_c3(pkg, steps, kernel, size=None, warmup=0):
     umax = float(np.sqrt(u2_ref.max()))
     out["fp64"] = {"MLUPS": ref["mlups"], "kinetic_energy": ref["ke"], "enstrophy": ens_ref,
                    "max_u": umax}
-    for name, st in (("f32", pkg.STORE_F32), ("f16_shift", pkg.STORE_F16_SHIFT),
-                     ("bf16_shift", pkg.STORE_BF16_SHIFT)):
-        r = run(st, kernel)
+    for name, st, rnd in (("f32", pkg.STORE_F32, 0), ("f16_shift", pkg.STORE_F16_SHIFT, 0),
+                          ("bf16_shift", pkg.STORE_BF16_SHIFT, 0),
+                          ("f16_shift_sr", pkg.STORE_F16_SHIFT, pkg.ROUND_STOCHASTIC),
+                          ("bf16_shift_sr", pkg.STORE_BF16_SHIFT, pkg.ROUND_STOCHASTIC)):
+        r = run(st, kernel, rnd)
         d2 = sum((r[k].astype(np.float64) - ref[k].astype(np.float64)) ** 2
                  for k in ("ux", "uy", "uz"))
         ens = _enstrophy(r["ux"], r["uy"], r["uz"])
@@ -329,7 +334,7 @@ def precision_c3(pkg, steps, kernel, size=None, warmup=0):
             "enstrophy_rel_err": abs(ens - ens_ref) / abs(ens_ref),
             "nonfinite_nodes": r["nonfinite"]}
     f32 = out["forms"]["f32"]["MLUPS"]
-    for name in ("f16_shift", "bf16_shift"):
+    for name in ("f16_shift", "bf16_shift", "f16_shift_sr", "bf16_shift_sr"):
         out["forms"][name]["speedup_vs_f32"] = out["forms"][name]["MLUPS"] / f32
     return out
 
@@ -338,7 +343,7 @@ def report_precision(args, pkg):
     """--report precision: precision_c3 with --steps steps as one JSON line."""
     kern = {"auto": pkg.KERNEL_AUTO, "scalar": pkg.KERNEL_SCALAR, "packed": pkg.KERNEL_PACKED,
             "tma": pkg.KERNEL_TMA}[args.kernel]
-    out = precision_c3(pkg, args.steps, kern, args.size or None, args.warmup)
+    out = precision_c3(pkg, args.steps, kern, args.size or None, args.warmup, args.re or None)
     out["report"] = "precision"
     print(json.dumps(out), flush=True)
 
@@ -557,7 +562,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="cavity256_mrt_les", choices=sorted(WORKLOADS))
-    ap.add_argument("--storage", default="f32", choices=["f32", "f16_shift", "bf16_shift", "f64"])
+    ap.add_argument("--storage", default="f32",
+                    choices=["f32", "f16_shift", "bf16_shift", "f64", "f16_shift_sr",
+                             "bf16_shift_sr"])
     ap.add_argument("--size", type=int, default=0, help="scale the workload to this nx (profiling)")
     ap.add_argument("--kernel", default="auto", choices=["auto", "scalar", "packed", "tma"])
     ap.add_argument("--streaming", default="ab", choices=["ab", "aa"],
@@ -577,6 +584,8 @@ def main():
                          "of work at --nominal-mlups (0 = HBM budget only)")
     ap.add_argument("--nominal-mlups", type=float, default=30000.0,
                     help="serving: throughput the backlog horizon is converted with")
+    ap.add_argument("--re", type=float, default=0.0,
+                    help="precision report: Reynolds number of the channel (0 = 1000)")
     ap.add_argument("--c3-steps", type=int, default=20000,
                     help="steps of the precision comparison on the 512x128x128 channel that the "
                          "default run reports (precision_c3)")
@@ -615,7 +624,8 @@ def main():
         return max_over_ranks(v, world)
 
     storage_id = {"f32": pkg.STORE_F32, "f16_shift": pkg.STORE_F16_SHIFT,
-                  "bf16_shift": pkg.STORE_BF16_SHIFT, "f64": pkg.STORE_F64}
+                  "bf16_shift": pkg.STORE_BF16_SHIFT, "f64": pkg.STORE_F64,
+                  "f16_shift_sr": pkg.STORE_F16_SHIFT, "bf16_shift_sr": pkg.STORE_BF16_SHIFT}
     iv = make_case(pkg, w, args.size or None)
     cells = iv.nx * iv.ny * iv.nz
     # a dedicated stream: the library launches on it and the CUDA events
@@ -629,7 +639,9 @@ def main():
                                           "packed": pkg.KERNEL_PACKED,
                                           "tma": pkg.KERNEL_TMA}[args.kernel],
                                   stream_mode=pkg.STREAM_AA if args.streaming == "aa"
-                                  else pkg.STREAM_AB)
+                                  else pkg.STREAM_AB,
+                                  rounding=pkg.ROUND_STOCHASTIC if storage.endswith("_sr")
+                                  else pkg.ROUND_NEAREST)
         dom = pkg.Domain(iv, opt)
         dom.set_stream(stream.cuda_stream)
         dom.run(warm)
@@ -717,12 +729,14 @@ def main():
         dom.close()
         # storage forms of the same workload (precision form: throughput)
         forms = {}
-        for st in ("f32", "f16_shift", "bf16_shift"):
+        for st in ("f32", "f16_shift", "bf16_shift", "f16_shift_sr", "bf16_shift_sr"):
             d2, ms2 = timed_steps(st, args.steps, args.warmup)
             d2.close()
             ms2 = allmax(ms2)
             forms[st] = {"MLUPS": world * cells * args.steps / (ms2 / 1e3) / 1e6,
                          "GB_s": 2 * 19 * BYTES[st] * cells / (ms2 / args.steps / 1e3) / 1e9}
+        for st in forms:
+            forms[st]["vs_f32"] = forms[st]["MLUPS"] / forms["f32"]["MLUPS"]
         line["storage_forms"] = forms
         if rank == 0 and world == 1:
             line["cpu_baseline"] = cpu_baseline(pkg, w)

@@ -183,8 +183,21 @@ typedef struct lbm_options {
   int stream_mode;      /* LBM_STREAM_*                                    */
   int device;           /* CUDA device ordinal                             */
   int kernel;           /* LBM_KERNEL_*                                    */
-  int reserved[7];
+  int rounding;         /* LBM_ROUND_*: rounding of the 16-bit stores      */
+  int reserved[6];
 } lbm_options;
+
+/* Rounding of the shifted 16-bit stores.  NEAREST: round to nearest even.
+ * STOCHASTIC: each stored deviation rounds up or down with probability
+ * given by its position between the two neighbouring 16-bit values
+ * (unbiased: the expected stored value is the exact one), with random bits
+ * from a hash of (node pair, step, seed), so runs are reproducible.  In a
+ * steady flow round-to-nearest rounds the same value the same way every
+ * step, a bias that accumulates; stochastic rounding turns it into noise.
+ * STOCHASTIC needs FP16/BF16 shifted storage with LBM_STREAM_AB and kernel
+ * AUTO, PAIRED or SCALAR (single domains; batch members round to nearest).
+ * The initial state and imports round to nearest. */
+enum { LBM_ROUND_NEAREST = 0, LBM_ROUND_STOCHASTIC = 1 };
 
 /* Fill *opt with the defaults: FP32, reference init, A/B streaming. */
 void lbm_default_options(lbm_options* opt);

@@ -42,6 +42,7 @@ STORE_F32, STORE_F16_SHIFT, STORE_BF16_SHIFT, STORE_F64 = 0, 1, 2, 3
 INIT_REFERENCE, INIT_DENSITY_NOISE, INIT_CHANNEL = 0, 1, 2
 STREAM_AB, STREAM_AA = 0, 1
 KERNEL_AUTO, KERNEL_SCALAR, KERNEL_PACKED, KERNEL_TMA, KERNEL_PAIRED = 0, 1, 2, 3, 4
+ROUND_NEAREST, ROUND_STOCHASTIC = 0, 1
 (PATTERN_COPY, PATTERN_PULL, PATTERN_PULL_PAIRED, PATTERN_AA_LOCAL, PATTERN_AA_NEIGHBOR,
  PATTERN_AA_LOCAL_V8, PATTERN_AA_LOCAL_V16) = range(7)
 
@@ -66,7 +67,8 @@ class Options(C.Structure):
     _fields_ = [
         ("storage", C.c_int), ("init_kind", C.c_int), ("seed", C.c_uint64),
         ("noise_amp", C.c_float), ("store_scale", C.c_float), ("stream_mode", C.c_int),
-        ("device", C.c_int), ("kernel", C.c_int), ("reserved", C.c_int * 7),
+        ("device", C.c_int), ("kernel", C.c_int), ("rounding", C.c_int),
+        ("reserved", C.c_int * 6),
     ]
 
 

@@ -145,9 +145,10 @@ int lbm_create(const Inputval* pinput, const lbm_options* opt, lbm_domain** out)
     d->bytes += b;
     return LBM_OK;
   };
-  if ((rc = domain_alloc_state(d, alloc)) || (rc = alloc((void**)&d->flag, 2 * sizeof(int))))
+  // device words: [0] input check, [1] kernel error, [2..3] step counter
+  if ((rc = domain_alloc_state(d, alloc)) || (rc = alloc((void**)&d->flag, 4 * sizeof(int))))
     return fail(rc);
-  if (cudaMemset(d->flag, 0, 2 * sizeof(int)) != cudaSuccess)
+  if (cudaMemset(d->flag, 0, 4 * sizeof(int)) != cudaSuccess)
     return fail(set_error(LBM_ERR_CUDA, "flag reset failed"));
   rc = storage_ops(d->opt.storage).tensor_maps(d, prop.multiProcessorCount);
   if (rc) return fail(rc);
@@ -282,6 +283,7 @@ int lbm_import_arF(lbm_domain* d, const float* arF, int padded) {
   if (rc) return rc;
   d->cur = 0;
   d->post_direct = true;
+  CK(cudaMemsetAsync(d->flag + 2, 0, 2 * sizeof(int), d->stream));  // step counter
   d->aa_first = false;
   d->step = 0;
   d->initialized = true;

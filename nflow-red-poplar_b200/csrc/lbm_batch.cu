@@ -561,10 +561,12 @@ int lbm_batch_add(lbm_batch* b, const Inputval* pinput, const lbm_options* opt,
   // diagnostics / staging buffers of a member come from cudaMalloc on first
   // use (lbm_diagnostics, lbm_export_arF)
   d->diag_blocks = 4 * b->sm_count;
-  d->flag = (int*)b->pool.alloc(2 * sizeof(int));
+  if (opt && opt->rounding != LBM_ROUND_NEAREST)
+    return undo(set_error(LBM_ERR_INVALID, "batch members round to nearest"));
+  d->flag = (int*)b->pool.alloc(4 * sizeof(int));
   if (!d->flag) return undo(set_error(LBM_ERR_BUDGET, "pool full"));
   d->bytes += 256;
-  if (cudaMemsetAsync(d->flag, 0, 2 * sizeof(int), b->stream) != cudaSuccess ||
+  if (cudaMemsetAsync(d->flag, 0, 4 * sizeof(int), b->stream) != cudaSuccess ||
       cudaEventCreate(&d->ev0) != cudaSuccess || cudaEventCreate(&d->ev1) != cudaSuccess)
     return undo(set_error(LBM_ERR_CUDA, "member set-up"));
   if ((rc = domain_upload_profile(d, b->stream)) || (rc = domain_launch_init(d, b->stream)) ||

@@ -71,6 +71,9 @@ __host__ __device__ constexpr int mrt_norm2(int k) {
   return s;
 }
 
+template <int N>
+using IC = std::integral_constant<int, N>;
+
 // compile-time loop: f(std::integral_constant<int, I>) for I in [B, E)
 template <int B, int E, class F>
 __host__ __device__ __forceinline__ void static_for(F&& f) {
@@ -124,6 +127,17 @@ struct StoreTraits<__half> {
   __device__ static __forceinline__ void store(__half* p, float g, float scale) {
     *p = __float2half_rn(g * scale);
   }
+  // h = g * scale, rounded stochastically (cvt.rs, sm_100a) as the `half`
+  // (0 lower, 1 upper) element of a 16x2 conversion with random bits rbits
+  __device__ static __forceinline__ void store_sr(__half* p, float g, float scale,
+                                                  uint32_t rbits, int half) {
+    const float x = g * scale;
+    uint32_t d;
+    asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;"
+        : "=r"(d)
+        : "f"(half ? x : 0.0f), "f"(half ? 0.0f : x), "r"(rbits));
+    *reinterpret_cast<unsigned short*>(p) = (unsigned short)(half ? d >> 16 : d & 0xffffu);
+  }
 };
 template <>
 struct StoreTraits<__nv_bfloat16> {
@@ -137,6 +151,15 @@ struct StoreTraits<__nv_bfloat16> {
   }
   __device__ static __forceinline__ void store(__nv_bfloat16* p, float g, float scale) {
     *p = __float2bfloat16_rn(g * scale);
+  }
+  __device__ static __forceinline__ void store_sr(__nv_bfloat16* p, float g, float scale,
+                                                  uint32_t rbits, int half) {
+    const float x = g * scale;
+    uint32_t d;
+    asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;"
+        : "=r"(d)
+        : "f"(half ? x : 0.0f), "f"(half ? 0.0f : x), "r"(rbits));
+    *reinterpret_cast<unsigned short*>(p) = (unsigned short)(half ? d >> 16 : d & 0xffffu);
   }
 };
 
@@ -399,9 +422,9 @@ __host__ __device__ __forceinline__ void collide_srt_pairs(const V (&f)[Q], cons
   const V c0 = DEV ? bc<V>(-1.5) * usq : fma_(bc<V>(-1.5), usq, bc<V>(1));
   const V rho = ps.rho_full;
   if constexpr (DEV)
-    emit(0, fma_(bc<V>(1.0 / 3.0) * fma_(rho, c0, ps.rho) - ps.f0, inv_tau, ps.f0));
+    emit(IC<0>{}, fma_(bc<V>(1.0 / 3.0) * fma_(rho, c0, ps.rho) - ps.f0, inv_tau, ps.f0));
   else
-    emit(0, fma_((rho * bc<V>(1.0 / 3.0)) * c0 - ps.f0, inv_tau, ps.f0));
+    emit(IC<0>{}, fma_((rho * bc<V>(1.0 / 3.0)) * c0 - ps.f0, inv_tau, ps.f0));
   const V wr1 = rho * bc<V>(1.0 / 18.0), wr2 = rho * bc<V>(1.0 / 36.0);
   static_for<0, 9>([&](auto pc) {
     constexpr int p = decltype(pc)::value;
@@ -433,11 +456,11 @@ __host__ __device__ __forceinline__ void collide_srt_pairs(const V (&f)[Q], cons
       // s* = s + (2 even - s) inv,  d* = d + (2 odd - d) inv
       const V ss = fma_(fma_(bc<V>(2), even, -ps.s[p]), inv_tau, ps.s[p]);
       const V dd = fma_(fma_(bc<V>(2), odd, -ps.d[p]), inv_tau, ps.d[p]);
-      emit(a, bc<V>(0.5) * (ss + dd));
-      emit(b, bc<V>(0.5) * (ss - dd));
+      emit(IC<a>{}, bc<V>(0.5) * (ss + dd));
+      emit(IC<b>{}, bc<V>(0.5) * (ss - dd));
     } else {
-      emit(a, fma_((even + odd) - f[a], inv_tau, f[a]));
-      emit(b, fma_((even - odd) - f[b], inv_tau, f[b]));
+      emit(IC<a>{}, fma_((even + odd) - f[a], inv_tau, f[a]));
+      emit(IC<b>{}, fma_((even - odd) - f[b], inv_tau, f[b]));
     }
   });
 }
@@ -514,7 +537,7 @@ __host__ __device__ __forceinline__ void collide_mrt_pairs(const V (&f)[Q], cons
   const V e17 = bc<V>(1.98 / 8.0) * m17;
   const V e18 = bc<V>(1.98 / 8.0) * m18;
   // ---- back transform, f -= M^T dm' ----
-  emit(0, ps.f0 - fma_(bc<V>(-30), e1, bc<V>(12) * e2));
+  emit(IC<0>{}, ps.f0 - fma_(bc<V>(-30), e1, bc<V>(12) * e2));
   const V eax = fma_(bc<V>(-11), e1, bc<V>(-4) * e2);  // rows 1,2 on axis directions
   const V edg = fma_(bc<V>(8), e1, e2);                 // rows 1,2 on diagonals
   const V g910 = e9 + e10;
@@ -548,11 +571,11 @@ __host__ __device__ __forceinline__ void collide_mrt_pairs(const V (&f)[Q], cons
     if constexpr (FROM_PAIRS) {
       const V ss = fma_(bc<V>(-2), E[q], s[q]);
       const V dd = fma_(bc<V>(-2), O[q], d[q]);
-      emit(a, bc<V>(0.5) * (ss + dd));
-      emit(b, bc<V>(0.5) * (ss - dd));
+      emit(IC<a>{}, bc<V>(0.5) * (ss + dd));
+      emit(IC<b>{}, bc<V>(0.5) * (ss - dd));
     } else {
-      emit(a, f[a] - (E[q] + O[q]));
-      emit(b, f[b] - (E[q] - O[q]));
+      emit(IC<a>{}, f[a] - (E[q] + O[q]));
+      emit(IC<b>{}, f[b] - (E[q] - O[q]));
     }
   });
 }

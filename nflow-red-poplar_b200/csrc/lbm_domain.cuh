@@ -151,6 +151,16 @@ inline int validate(const Inputval* in, const lbm_options* opt) {
       return set_error(LBM_ERR_INVALID,
                        "the paired kernel is the 16-bit pull (A/B) form: FP16/BF16 shifted "
                        "storage with LBM_STREAM_AB");
+    if (opt->rounding != LBM_ROUND_NEAREST && opt->rounding != LBM_ROUND_STOCHASTIC)
+      return set_error(LBM_ERR_INVALID, "unknown rounding %d", opt->rounding);
+    if (opt->rounding == LBM_ROUND_STOCHASTIC &&
+        ((opt->storage != LBM_STORE_F16_SHIFT && opt->storage != LBM_STORE_BF16_SHIFT) ||
+         opt->stream_mode != LBM_STREAM_AB ||
+         (opt->kernel != LBM_KERNEL_AUTO && opt->kernel != LBM_KERNEL_PAIRED &&
+          opt->kernel != LBM_KERNEL_SCALAR)))
+      return set_error(LBM_ERR_INVALID,
+                       "stochastic rounding needs FP16/BF16 shifted storage with LBM_STREAM_AB "
+                       "and kernel AUTO, PAIRED or SCALAR");
     if (!std::isfinite(opt->noise_amp) || !std::isfinite(opt->store_scale) ||
         opt->store_scale < 0.0f)
       return set_error(LBM_ERR_INVALID, "bad noise_amp/store_scale");
@@ -224,6 +234,12 @@ StepArgs<S> make_args(const lbm_domain* d, const void* src, void* dst, long long
   a.mp.wepsj = R(d->in.dWepsj);
   a.mp.wxx = R(d->in.dWXX);
   a.mp.e2c = kDev<S> ? R(3) - a.mp.weps : R(0);
+  // step counter of the stochastic rounding: step k reads kctr[(k-1) & 1]
+  // and writes kctr[k & 1] (d->flag[2..3])
+  a.kctr = (unsigned*)(d->flag + 2);
+  a.kpar = (int)((k - 1) & 1);
+  a.sr = d->opt.rounding == LBM_ROUND_STOCHASTIC;
+  a.sr_seed = (unsigned)(d->opt.seed * 0x9E3779B97F4A7C15ull >> 32);
   a.scale = d->scale;
   a.inv_scale = d->inv_scale;
   a.inlet_u = d->inlet_u;
@@ -277,12 +293,17 @@ template <class S, int COLL, bool LES>
 void launch_step(const lbm_domain* d, const StepArgs<S>& a, cudaStream_t st) {
   if constexpr (kDev<S>) {
     if (d->g.paired) {
-      if (paired_kernel_applies(d->g))
-        k_step_paired<S, COLL, LES>
-            <<<dim3((d->g.px / 2 + 127) / 128, d->g.nz, d->g.ny), dim3(128), 0, st>>>(a);
+      const dim3 gr((d->g.px / 2 + 127) / 128, d->g.nz, d->g.ny);
+      if (paired_kernel_applies(d->g) && a.sr)
+        k_step_paired<S, COLL, LES, true><<<gr, dim3(128), 0, st>>>(a);
+      else if (paired_kernel_applies(d->g))
+        k_step_paired<S, COLL, LES, false><<<gr, dim3(128), 0, st>>>(a);
+      else if (a.sr)
+        k_step_rows<S, COLL, LES, true><<<grid_of(d->g, block_of(d->g.nx)), block_of(d->g.nx),
+                                          0, st>>>(a);
       else
-        k_step_rows<S, COLL, LES><<<grid_of(d->g, block_of(d->g.nx)), block_of(d->g.nx), 0,
-                                    st>>>(a);
+        k_step_rows<S, COLL, LES, false><<<grid_of(d->g, block_of(d->g.nx)),
+                                           block_of(d->g.nx), 0, st>>>(a);
       return;
     }
   }
@@ -304,7 +325,13 @@ void launch_step(const lbm_domain* d, const StepArgs<S>& a, cudaStream_t st) {
     }
   }
   const dim3 b = block_of(d->g.nx), gr = grid_of(d->g, b);
-  k_step<S, COLL, LES><<<gr, b, 0, st>>>(a);
+  if constexpr (kDev<S>) {
+    if (a.sr) {
+      k_step<S, COLL, LES, true><<<gr, b, 0, st>>>(a);
+      return;
+    }
+  }
+  k_step<S, COLL, LES, false><<<gr, b, 0, st>>>(a);
 }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link
@@ -588,6 +615,7 @@ inline int domain_launch_init(lbm_domain* d, cudaStream_t st) {
   const size_t nb = (size_t)d->N * sizeof(float);
   CK(cudaMemsetAsync(d->den[0], 0, nb, st));
   CK(cudaMemsetAsync(d->den[1], 0, nb, st));
+  CK(cudaMemsetAsync(d->flag + 2, 0, 2 * sizeof(int), st));  // step counter
   int rc = storage_ops(d->opt.storage).launch_init(d, st);
   if (rc) return rc;
   d->cur = 0;

@@ -163,6 +163,12 @@ struct StepArgs {
   unsigned long long seed;
   // batched kernel: 0 pull step, 1 AA local step, 2 AA neighbour step
   int aa_step;
+  // stochastic rounding of the 16-bit stores (paired kernel): step counter
+  // pair (the step reads kctr[kpar], writes kctr[kpar ^ 1]) and seed
+  unsigned* kctr;
+  int kpar;
+  int sr;
+  unsigned sr_seed;
 };
 
 // internal value of a stored population
@@ -454,9 +460,37 @@ struct StoreNode {
   }
 };
 
+// Stochastic rounding (LBM_ROUND_STOCHASTIC).  cvt.rs rounds each FP32
+// input to one of its two neighbouring 16-bit values, up with probability
+// equal to the input's distance from the lower one in units of the spacing,
+// using the caller's random bits (sm_100a).  The bits of a store are a hash
+// of (pair word, step, seed, population), so a run is reproducible and a
+// node gets the same bits whichever kernel stores it.  The pair word of node
+// (x, y, z) is that of the paired rows, (x mod H) + H (z + nz y) with
+// H = px / 2, and its half is x >= H, whatever the layout of the domain.
+__device__ __forceinline__ uint32_t sr_hash(uint32_t word, uint32_t k, uint32_t seed) {
+  uint32_t h = word * 0x9E3779B1u ^ (k * 0x85EBCA77u + seed);
+  h ^= h >> 16;
+  h *= 0x7FEB352Du;
+  h ^= h >> 15;
+  h *= 0x846CA68Bu;
+  h ^= h >> 16;
+  return h;
+}
+template <int q>
+__device__ __forceinline__ uint32_t sr_bits(uint32_t h) {
+  uint32_t r = h * (0x2C1B3C6Du + 2u * (uint32_t)q * 0x9E3779B9u);  // odd multiplier per q
+  return r ^ (r >> 16);
+}
+__device__ __forceinline__ uint32_t sr_word(const Geometry& g, int x, int y, int z) {
+  const int h = g.px >> 1;
+  return (uint32_t)((x < h ? x : x - h) + h * (z + g.nz * y));
+}
+
 // Steps 3-6 of a node whose post-stream populations f are known:
-// macroscopic, side outputs, LES, collision, store of f*.
-template <class S, int COLL, bool LES, class Addr>
+// macroscopic, side outputs, LES, collision, store of f* (SR: stochastic
+// rounding of the 16-bit stores, step number from a.kctr[a.kpar]).
+template <class S, int COLL, bool LES, bool SR = false, class Addr>
 __device__ __forceinline__ void finish_node(const RealOf<S> (&f)[Q], const StepArgs<S>& a,
                                             const Addr& ad, int x, int y, int z) {
   using R = RealOf<S>;
@@ -465,16 +499,28 @@ __device__ __forceinline__ void finish_node(const RealOf<S> (&f)[Q], const StepA
   R ux, uy, uz;
   const R inv_rho = velocity<R>(ps, ux, uy, uz);
   write_macro<S>(a, x, y, z, ps.rho_full, ux, uy, uz);
-  collide_node<S, COLL, LES, kFromPairs<S>, R>(f, ps, ux, uy, uz, inv_rho, a, [&](int q, R v) {
-    StoreTraits<S>::store(ad.out(q), v, ad.scale());
-  });
+  if constexpr (SR) {
+    static_assert(kDev<S>, "stochastic rounding is a 16-bit store");
+    const uint32_t h = sr_hash(sr_word(a.g, x, y, z), a.kctr[a.kpar], a.sr_seed);
+    const int half = x >= (a.g.px >> 1);
+    collide_node<S, COLL, LES, kFromPairs<S>, R>(f, ps, ux, uy, uz, inv_rho, a,
+                                                 [&](auto qc, R v) {
+      constexpr int q = decltype(qc)::value;
+      StoreTraits<S>::store_sr(ad.out(q), v, ad.scale(), sr_bits<q>(h), half);
+    });
+  } else {
+    collide_node<S, COLL, LES, kFromPairs<S>, R>(f, ps, ux, uy, uz, inv_rho, a,
+                                                 [&](int q, R v) {
+      StoreTraits<S>::store(ad.out(q), v, ad.scale());
+    });
+  }
 }
 
 // One fused step of the node (x, y, z): pull + boundary rules, macroscopic,
 // LES, collision, store.  Shared by the single-domain and batched kernels,
 // so a domain gets the same bits alone and in a batch (only where the
 // arguments are held differs, not the arithmetic).
-template <class S, int COLL, bool LES, class Addr>
+template <class S, int COLL, bool LES, bool SR = false, class Addr>
 __device__ __forceinline__ void step_node_at(const StepArgs<S>& a, const Addr& ad, int x, int y,
                                              int z) {
   using R = RealOf<S>;
@@ -483,7 +529,17 @@ __device__ __forceinline__ void step_node_at(const StepArgs<S>& a, const Addr& a
   if (has_struct(a.g) && node_type(a.g, x, y, z) == NODE_STRUCT) return;
   R f[Q];
   pull<S>(f, a, ad, x, y, z);
-  finish_node<S, COLL, LES>(f, a, ad, x, y, z);
+  finish_node<S, COLL, LES, SR>(f, a, ad, x, y, z);
+}
+
+// stochastic rounding: the first thread of a step's grid leaves the next
+// step number for the next step (the others read only kctr[kpar])
+template <bool SR, class S>
+__device__ __forceinline__ void bump_step_counter(const StepArgs<S>& a) {
+  if constexpr (SR) {
+    if ((blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x | threadIdx.y) == 0)
+      a.kctr[a.kpar ^ 1] = a.kctr[a.kpar] + 1;
+  }
 }
 template <class S, int COLL, bool LES>
 __device__ __forceinline__ void step_node(const StepArgs<S>& a, int x, int y, int z) {
@@ -491,12 +547,13 @@ __device__ __forceinline__ void step_node(const StepArgs<S>& a, int x, int y, in
 }
 
 // The fused step.  grid = (ceil(nx/blockDim.x), nz, ny), one thread per node.
-template <class S, int COLL, bool LES>
+template <class S, int COLL, bool LES, bool SR = false>
 __global__ void __launch_bounds__(128) k_step(const __grid_constant__ StepArgs<S> a) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int z = blockIdx.y, y = blockIdx.z;
+  bump_step_counter<SR>(a);
   if (x >= a.g.nx) return;
-  step_node<S, COLL, LES>(a, x, y, z);
+  step_node_at<S, COLL, LES, SR>(a, PlaneAddr<S>(a, x + a.g.px * (z + a.g.nz * y)), x, y, z);
 }
 
 // ------------------------------------------------------------------ //
@@ -1034,6 +1091,24 @@ __device__ __forceinline__ uint32_t pack_pair<__nv_bfloat16>(F2 v, float scale) 
   memcpy(&word, &h, 4);
   return word;
 }
+template <class S>
+__device__ __forceinline__ uint32_t pack_pair_sr(F2 v, float scale, uint32_t rbits);
+template <>
+__device__ __forceinline__ uint32_t pack_pair_sr<__half>(F2 v, float scale, uint32_t rbits) {
+  const float2 x = __fmul2_rn(v.v, make_float2(scale, scale));
+  uint32_t d;  // a (the hi lane) goes to the upper half, b (lo) to the lower
+  asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(x.y), "f"(x.x), "r"(rbits));
+  return d;
+}
+template <>
+__device__ __forceinline__ uint32_t pack_pair_sr<__nv_bfloat16>(F2 v, float scale,
+                                                               uint32_t rbits) {
+  const float2 x = __fmul2_rn(v.v, make_float2(scale, scale));
+  uint32_t d;
+  asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(x.y), "f"(x.x), "r"(rbits));
+  return d;
+}
+
 // the paired step kernel applies to the domain (else: k_step_rows); nx >=
 // 11 keeps both x faces out of each other's words and every hi lane's x + 1
 // donor of a real node inside the row
@@ -1051,7 +1126,7 @@ __host__ __device__ __forceinline__ bool paired_kernel_applies(const Geometry& g
 
 // grid = (ceil(H / 128), nz, ny), 128 threads, one word (two nodes) per
 // thread; a.srcd[q] = plane q minus the donor offset 2 c_x + px (c_z + nz c_y)
-template <class S, int COLL, bool LES>
+template <class S, int COLL, bool LES, bool SR>
 __global__ void __launch_bounds__(128, LBM_PAIRED_THREADS_PER_SM / 128)
     k_step_paired(const __grid_constant__ StepArgs<S> a) {
   static_assert(kDev<S>, "paired rows are a 16-bit layout");
@@ -1126,19 +1201,31 @@ __global__ void __launch_bounds__(128, LBM_PAIRED_THREADS_PER_SM / 128)
     write_macro<S>(a, w, y, z, ps.rho_full.v.x, ux.v.x, uy.v.x, uz.v.x);
     if (xh < a.g.nx) write_macro<S>(a, xh, y, z, ps.rho_full.v.y, ux.v.y, uy.v.y, uz.v.y);
   }
-  collide_node<S, COLL, LES, true, F2>(f, ps, ux, uy, uz, inv_rho, a, [&](int q, F2 v) {
-    *reinterpret_cast<uint32_t*>(a.dstq[q] + e) = pack_pair<S>(v, a.scale);
-  });
+  if constexpr (!SR) {
+    collide_node<S, COLL, LES, true, F2>(f, ps, ux, uy, uz, inv_rho, a, [&](int q, F2 v) {
+      *reinterpret_cast<uint32_t*>(a.dstq[q] + e) = pack_pair<S>(v, a.scale);
+    });
+  } else {
+    // the step number: this step reads kctr[kpar] and leaves its successor
+    // in kctr[kpar ^ 1] for the next step
+    bump_step_counter<SR>(a);
+    const uint32_t h = sr_hash((uint32_t)(e >> 1), a.kctr[a.kpar], a.sr_seed);
+    collide_node<S, COLL, LES, true, F2>(f, ps, ux, uy, uz, inv_rho, a, [&](auto qc, F2 v) {
+      constexpr int q = decltype(qc)::value;
+      *reinterpret_cast<uint32_t*>(a.dstq[q] + e) = pack_pair_sr<S>(v, a.scale, sr_bits<q>(h));
+    });
+  }
 }
 
 // Paired domains the paired kernel does not apply to (STRUCT nodes, nx <
 // 11): the per-node step over paired rows.  grid = (ceil(nx/128), nz, ny).
-template <class S, int COLL, bool LES>
+template <class S, int COLL, bool LES, bool SR = false>
 __global__ void __launch_bounds__(128) k_step_rows(const __grid_constant__ StepArgs<S> a) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int z = blockIdx.y, y = blockIdx.z;
+  bump_step_counter<SR>(a);
   if (x >= a.g.nx) return;
-  step_node_at<S, COLL, LES>(a, RowAddr<S>(a, x, y, z), x, y, z);
+  step_node_at<S, COLL, LES, SR>(a, RowAddr<S>(a, x, y, z), x, y, z);
 }
 
 // node type and inside mask per node, [ny][nz][nx]

@@ -149,3 +149,85 @@ def test_paired_option_rejected_where_it_does_not_apply():
         with pytest.raises(pkg.LbmError) as e:
             pkg.Domain(iv, o)
         assert e.value.code == pkg.LBM_ERR_INVALID
+
+
+# ---------------------------------------------------------------------------
+# Stochastic rounding (LBM_ROUND_STOCHASTIC): the random bits of a store
+# depend on the node's pair word, the step and the seed only, and cvt.rs
+# rounds each element of a 16x2 conversion with its own bits, so the paired
+# kernel (both elements real) and the per-node kernel over plain rows (the
+# other element 0) give the same bits.
+# ---------------------------------------------------------------------------
+def sr_opts(storage, kernel, kind=pkg.INIT_DENSITY_NOISE, amp=1e-4, seed=7):
+    return pkg.default_options(storage=storage, kernel=kernel, init_kind=kind, noise_amp=amp,
+                               seed=seed, rounding=pkg.ROUND_STOCHASTIC)
+
+
+def run_arF(iv, o, steps, mask=None):
+    d = pkg.Domain(iv, o)
+    if mask is not None:
+        d.set_solid_mask(mask)
+    d.run(steps)
+    out = (d.export_arF(), d.macroscopic())
+    d.close()
+    return out
+
+
+@pytest.mark.parametrize("storage", STORES)
+@pytest.mark.parametrize("shape", [(64, 20, 18), (130, 9, 11), (17, 16, 3), (9, 8, 7)])
+def test_stochastic_rounding_same_bits_paired_and_per_node(storage, shape):
+    iv = cavity(*shape)
+    a = run_arF(iv, sr_opts(storage, pkg.KERNEL_PAIRED), 70)
+    b = run_arF(iv, sr_opts(storage, pkg.KERNEL_SCALAR), 70)
+    assert_same(a, b)
+
+
+@pytest.mark.parametrize("storage", STORES)
+def test_stochastic_rounding_channel_and_mask(storage):
+    iv = channel(48, 12, 14)
+    a = run_arF(iv, sr_opts(storage, pkg.KERNEL_PAIRED, pkg.INIT_CHANNEL, 0.01), 66)
+    b = run_arF(iv, sr_opts(storage, pkg.KERNEL_SCALAR, pkg.INIT_CHANNEL, 0.01), 66)
+    assert_same(a, b)
+    iv = cavity(40, 16, 18)
+    mask = np.zeros((16, 18, 40), np.uint8)
+    mask[5:10, 6:12, 15:22] = 1
+    a = run_arF(iv, sr_opts(storage, pkg.KERNEL_PAIRED), 30, mask)
+    b = run_arF(iv, sr_opts(storage, pkg.KERNEL_SCALAR), 30, mask)
+    assert_same(a, b)
+
+
+def test_stochastic_rounding_is_reproducible_and_seeded():
+    iv = cavity(48, 14, 12)
+    st = pkg.STORE_F16_SHIFT
+    a = run_arF(iv, sr_opts(st, pkg.KERNEL_AUTO), 70)   # graph chunks + single steps
+    b = run_arF(iv, sr_opts(st, pkg.KERNEL_AUTO), 70)
+    assert_same(a, b)
+    c = run_arF(iv, sr_opts(st, pkg.KERNEL_AUTO, seed=8), 70)
+    n = run_arF(iv, opts(st, pkg.KERNEL_AUTO), 70)
+    assert not np.array_equal(a[0], c[0]) and not np.array_equal(a[0], n[0])
+    # the same physics: every variant within a few storage quanta of the others
+    assert np.abs(a[0] - n[0]).max() < 2e-4
+    # 70 steps in one call equal 33 + 37 steps (the step counter carries over)
+    d = pkg.Domain(iv, sr_opts(st, pkg.KERNEL_AUTO))
+    d.run(33)
+    d.run(37)
+    np.testing.assert_array_equal(d.export_arF(), a[0])
+    d.close()
+
+
+def test_stochastic_rounding_rejected_where_not_built():
+    iv = cavity(16, 12, 10)
+    for o in (pkg.default_options(storage=pkg.STORE_F32, rounding=pkg.ROUND_STOCHASTIC),
+              pkg.default_options(storage=pkg.STORE_F16_SHIFT, rounding=pkg.ROUND_STOCHASTIC,
+                                  stream_mode=pkg.STREAM_AA),
+              pkg.default_options(storage=pkg.STORE_F16_SHIFT, rounding=pkg.ROUND_STOCHASTIC,
+                                  kernel=pkg.KERNEL_TMA),
+              pkg.default_options(storage=pkg.STORE_F16_SHIFT, rounding=5)):
+        with pytest.raises(pkg.LbmError) as e:
+            pkg.Domain(iv, o)
+        assert e.value.code == pkg.LBM_ERR_INVALID
+    b = pkg.Batch(hbm_budget=64 << 20)
+    with pytest.raises(pkg.LbmError):
+        b.add(iv, pkg.default_options(storage=pkg.STORE_F16_SHIFT,
+                                      rounding=pkg.ROUND_STOCHASTIC), 4)
+    b.close()

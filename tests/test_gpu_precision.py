@@ -1,0 +1,74 @@
+"""The precision form against the FP64 build (shortened channel).
+
+The 512x128x128 channel of the precision comparison, scaled to 128x32x32
+with the same relaxation time (tau = 0.5192, Re 1000 at full size), MRT +
+LES, parabolic inlet u_max = 0.05, outlet rho = 1, 1 % seeded velocity
+perturbation, 8,000 steps (past the time the perturbation needs to cross
+the channel).  The velocity error of the 16-bit forms is measured against
+the FP64 build of the same kernels as the relative L2 norm
+||u - u64|| / ||u64|| and as the largest nodal error relative to max |u64|.
+Stochastic rounding of the FP16 stores must keep the relative L2 error
+within 1e-3 (the precision target) and below round-to-nearest, whose error
+in this steady, pressure-driven flow is a rounding bias that accumulates
+(measured at this size: 3.5e-4 against 7.8e-4; on the full 512x128x128
+channel after 20,000 steps: 3.6e-4 against 1.4e-2).
+"""
+import numpy as np
+import pytest
+
+import oracle_lib as O
+
+pkg = O.pkg
+pytestmark = pytest.mark.gpu
+
+STEPS = 8000
+
+
+def channel():
+    nu = (0.5192 - 0.5) / 3.0
+    return pkg.make_inputval(128, 32, 32, casetype=pkg.CHANNEL, tau=3.0 * nu + 0.5, u=0.05,
+                             mrt=True, les=True, cs=0.1)
+
+
+def run(storage, rounding=pkg.ROUND_NEAREST):
+    o = pkg.default_options(storage=storage, init_kind=pkg.INIT_CHANNEL, noise_amp=0.01, seed=1,
+                            rounding=rounding)
+    d = pkg.Domain(channel(), o)
+    d.run(STEPS)
+    den, ux, uy, uz = d.macroscopic()
+    d.close()
+    return np.stack([ux, uy, uz]).astype(np.float64), den.astype(np.float64)
+
+
+@pytest.fixture(scope="module")
+def ref():
+    return run(pkg.STORE_F64)
+
+
+def errors(u, u64):
+    d2 = ((u - u64) ** 2).sum(0)
+    n2 = (u64 ** 2).sum(0)
+    return float(np.sqrt(d2.sum() / n2.sum())), float(np.sqrt(d2.max() / n2.max()))
+
+
+def test_fp32_matches_fp64(ref):
+    u, _ = run(pkg.STORE_F32)
+    l2, mx = errors(u, ref[0])
+    assert l2 < 1e-4 and mx < 1e-4, (l2, mx)
+
+
+def test_fp16_stochastic_rounding_meets_the_target(ref):
+    u_sr, _ = run(pkg.STORE_F16_SHIFT, pkg.ROUND_STOCHASTIC)
+    u_rn, _ = run(pkg.STORE_F16_SHIFT)
+    l2_sr, mx_sr = errors(u_sr, ref[0])
+    l2_rn, mx_rn = errors(u_rn, ref[0])
+    assert l2_sr <= 1e-3, (l2_sr, mx_sr, l2_rn, mx_rn)
+    assert l2_sr < 0.7 * l2_rn, (l2_sr, l2_rn)
+
+
+def test_bf16_stochastic_rounding_beats_nearest(ref):
+    u_sr, _ = run(pkg.STORE_BF16_SHIFT, pkg.ROUND_STOCHASTIC)
+    u_rn, _ = run(pkg.STORE_BF16_SHIFT)
+    l2_sr, _ = errors(u_sr, ref[0])
+    l2_rn, _ = errors(u_rn, ref[0])
+    assert l2_sr < l2_rn / 2, (l2_sr, l2_rn)
