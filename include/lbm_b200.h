@@ -184,7 +184,11 @@ typedef struct lbm_options {
   int device;           /* CUDA device ordinal                             */
   int kernel;           /* LBM_KERNEL_*                                    */
   int rounding;         /* LBM_ROUND_*: rounding of the 16-bit stores      */
-  int reserved[6];
+  int wait_test;        /* test of the bounded waits, LBM_KERNEL_TMA only:
+                           k > 0 makes the TMA producer withhold the copies
+                           of tile k-1 and every wait give up after ~1 ms,
+                           so that the step reports LBM_ERR_TIMEOUT; 0 off */
+  int reserved[5];
 } lbm_options;
 
 /* Rounding of the shifted 16-bit stores.  NEAREST: round to nearest even.
@@ -419,6 +423,17 @@ int lbm_sync(lbm_domain* d);
 
 /* Device bytes held by the handle. */
 int lbm_device_bytes(const lbm_domain* d, size_t* bytes);
+
+/* The device arrays of the macroscopic state after the last step, as the
+ * reference's LBMSolver::m_DeviceNode exposes them (m_dCurrDen, m_dPrevDen,
+ * m_dCurrVelx/y/z; struct.h:30-50): [ny][nz][nx] FP32 each, owned by the
+ * handle, written by the handle's stream; valid until its next step,
+ * import or destroy.  prev_den holds the density of the step before (0
+ * right after initialize / import).  Any pointer may be NULL.  (The
+ * populations are in the library's private layout; lbm_export_arF reads
+ * them as the reference's arF.) */
+int lbm_device_fields(lbm_domain* d, float** den, float** prev_den, float** velx, float** vely,
+                      float** velz);
 
 /* Bytes a domain of this case would hold (for admission control). */
 int lbm_estimate_bytes(const Inputval* pinput, const lbm_options* opt,

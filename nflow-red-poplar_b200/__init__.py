@@ -68,7 +68,7 @@ class Options(C.Structure):
         ("storage", C.c_int), ("init_kind", C.c_int), ("seed", C.c_uint64),
         ("noise_amp", C.c_float), ("store_scale", C.c_float), ("stream_mode", C.c_int),
         ("device", C.c_int), ("kernel", C.c_int), ("rounding", C.c_int),
-        ("reserved", C.c_int * 6),
+        ("wait_test", C.c_int), ("reserved", C.c_int * 5),
     ]
 
 
@@ -180,6 +180,7 @@ def lib():
         L.lbm_batch_last_step_ms.argtypes = [vp, C.POINTER(C.c_float), C.POINTER(C.c_longlong)]
         L.lbm_pattern_ceiling.argtypes = [i32, i32, i32, i32, C.POINTER(C.c_double),
                                           C.POINTER(C.c_double)]
+        L.lbm_device_fields.argtypes = [vp] + [C.POINTER(vp)] * 5
         _lib = L
     return _lib
 

@@ -370,4 +370,16 @@ int lbm_device_bytes(const lbm_domain* d, size_t* bytes) {
   return LBM_OK;
 }
 
+int lbm_device_fields(lbm_domain* d, float** den, float** prev_den, float** velx, float** vely,
+                      float** velz) {
+  if (!d) return set_error(LBM_ERR_INVALID, "NULL domain");
+  if (!d->initialized) return set_error(LBM_ERR_STATE, "domain not initialized");
+  if (den) *den = d->den[d->step & 1];
+  if (prev_den) *prev_den = d->den[(d->step + 1) & 1];
+  if (velx) *velx = d->ux;
+  if (vely) *vely = d->uy;
+  if (velz) *velz = d->uz;
+  return LBM_OK;
+}
+
 }  // extern "C"

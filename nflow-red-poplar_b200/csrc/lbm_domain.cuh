@@ -151,6 +151,8 @@ inline int validate(const Inputval* in, const lbm_options* opt) {
       return set_error(LBM_ERR_INVALID,
                        "the paired kernel is the 16-bit pull (A/B) form: FP16/BF16 shifted "
                        "storage with LBM_STREAM_AB");
+    if (opt->wait_test < 0 || (opt->wait_test > 0 && opt->kernel != LBM_KERNEL_TMA))
+      return set_error(LBM_ERR_INVALID, "wait_test applies to the TMA kernel only");
     if (opt->rounding != LBM_ROUND_NEAREST && opt->rounding != LBM_ROUND_STOCHASTIC)
       return set_error(LBM_ERR_INVALID, "unknown rounding %d", opt->rounding);
     if (opt->rounding == LBM_ROUND_STOCHASTIC &&
@@ -319,8 +321,10 @@ void launch_step(const lbm_domain* d, const StepArgs<S>& a, cudaStream_t st) {
     else if (d->opt.kernel == LBM_KERNEL_TMA && d->tmap_ok) {
       using Cfg = TmaCfg<S>;
       const int which = (a.src == (const S*)d->lat[0]) ? 0 : 1;
-      k_step_tma<S, COLL, LES><<<d->tma_grid, Cfg::THREADS, Cfg::SMEM, st>>>(a, d->tmap[which],
-                                                                            d->flag + 1);
+      // the wait test withholds one tile and bounds every wait to ~1 ms
+      const int stall = d->opt.wait_test > 0 ? d->opt.wait_test - 1 : -1;
+      k_step_tma<S, COLL, LES><<<d->tma_grid, Cfg::THREADS, Cfg::SMEM, st>>>(
+          a, d->tmap[which], d->flag + 1, stall, stall >= 0 ? 1000 : kWaitIters);
       return;
     }
   }

@@ -1,26 +1,24 @@
-// lbm_main.cpp — C++ driver with the behaviour of the reference main.cpp:
+// lbm_main.cpp — C++ driver with the behaviour of the reference main.cpp,
+// written against the reference's own host spelling (lbm_b200_compat.hpp):
 // build the case of main.cpp:59-85, report the tile decomposition
-// (main.cpp:256-261), initialise and run maxitr steps on the GPU timed with
-// std::chrono around the run (main.cpp:308-314), read arF back
-// (main.cpp:317) and print direction 9 of the plane k=2 (main.cpp:321-347).
+// (decomposition(), main.cpp:256-261), run the Initialize program and
+// maxitr steps on the GPU timed with std::chrono around the run
+// (main.cpp:308-314), read arF back (main.cpp:317) and print direction 9 of
+// the plane k=2 (main.cpp:321-347).
 //
-//   lbm_main [h] [maxitr] [Cs] [srt|mrt] [nwrite] [savetype] [outdir]
+//   lbm_main [h] [maxitr] [Cs] [srt|mrt] [nwrite] [savetype]
 // Defaults are main.cpp's: h=10, maxitr=199, MRT+LES, Re=1000, u_lid=0.1,
 // Smagorinsky constant 0 (main.cpp never assigns it), no result files.
-// With nwrite > 0 it also writes the result files of kernel.cu's loop
-// (kernel.cu:203-228, savetype 0 = VTU, 1 = CSV, into outdir, default
-// ./result/) every nwrite steps and prints kernel.cu's residual line every
-// 100 steps (kernel.cu:232-248).  Each file is written by a host thread from
-// a snapshot while the GPU keeps stepping.
-#include <algorithm>
+// The steps run through runSimulation(Inputval*, LBMSolver*), kernel.cu's
+// loop: a residual line every 100 cycles and, with nwrite > 0, a result
+// file every nwrite cycles (savetype 0 = VTU, 1 = CSV, into ./result/).
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
-#include <thread>
 #include <vector>
 
-#include "../../include/lbm_b200.h"
+#include "../../include/lbm_b200_compat.hpp"
 
 int main(int argc, char** argv) {
   Inputval in;
@@ -39,7 +37,6 @@ int main(int argc, char** argv) {
   in.nu = in.m_dRefVelx * in.h / in.Re;
   in.nwrite = argc > 5 ? std::atoi(argv[5]) : 0;
   in.savetype = argc > 6 ? std::atoi(argv[6]) : 1;
-  const char* outdir = argc > 7 ? argv[7] : nullptr;
   in.casetype = CAVITY;
   in.m_dTau = 3.0f * in.m_dRefVelx * in.h / in.Re + 0.50f;
   in.dWeps = 3.0f;
@@ -47,73 +44,40 @@ int main(int argc, char** argv) {
   in.dWXX = -0.5f;
 
   static int Slice[TILE_NUM][DIMENSION][2];
-  int ntile = lbm_decomposition(&in, Slice);
-  std::printf("Number of Tiles participating = %d\n", ntile);
+  LBMSolver* psolver = new LBMSolver();
+  int rc = 0;
+  try {
+    const int ntile = decomposition(&in, Slice);
+    std::printf("Number of Tiles participating = %d\n", ntile);
+    initialize(&in, psolver);  // the Initialize program (main.cpp:280-282)
+    lbm_b200::check(lbm_sync(psolver->m_pDomain));
+    const auto t0 = std::chrono::high_resolution_clock::now();
+    std::printf(" - Running program\n");
+    runSimulation(&in, psolver);  // Repeat(maxitr, runSimulation) (main.cpp:283-291)
+    lbm_b200::check(lbm_sync(psolver->m_pDomain));
+    const auto t1 = std::chrono::high_resolution_clock::now();
+    const std::chrono::duration<double> el = t1 - t0;
+    std::printf(" - Elapsed time(GPU) = %fs | h=%d | %.1f MLUPS\n", el.count(), in.h,
+                (double)in.nx * in.ny * in.nz * in.maxitr / el.count() / 1e6);
 
-  lbm_domain* d = nullptr;
-  if (lbm_create(&in, nullptr, &d) != LBM_OK || lbm_initialize(d) != LBM_OK) {
-    std::fprintf(stderr, " - Error: %s\n", lbm_last_error());
-    if (d) lbm_destroy(d);
-    return 1;
-  }
-  lbm_sync(d);
-  auto t0 = std::chrono::high_resolution_clock::now();
-  std::printf(" - Running program\n");
-  bool ok = true;
-  if (in.nwrite <= 0) {
-    ok = lbm_run_simulation(d, in.maxitr) == LBM_OK && lbm_sync(d) == LBM_OK;
-  } else {
-    // kernel.cu's loop: a residual line every 100 steps, a file every nwrite
-    std::thread writer;
-    int write_rc = LBM_OK;
-    for (int icycle = 0; ok && icycle < in.maxitr;) {
-      const int next_print = (icycle / 100 + 1) * 100, next_write = (icycle / in.nwrite + 1) * in.nwrite;
-      int k = std::min(std::min(next_print, next_write), in.maxitr) - icycle;
-      ok = lbm_run_simulation(d, k) == LBM_OK;
-      icycle += k;
-      if (ok && icycle % 100 == 0) {
-        double diag[8];
-        ok = lbm_diagnostics(d, diag) == LBM_OK;
-        if (ok) std::printf("ITER=%d | ERROR=%.5e\n", icycle, diag[4]);
+    std::vector<float>& arF = psolver->m_HostNode.m_arF;  // engine.readTensor("D2H-arF")
+    arF.resize((size_t)in.nx * in.ny * in.nz * DIRECTION_SIZE);
+    lbm_b200::check(lbm_export_arF(psolver->m_pDomain, arF.data(), 0));
+    std::printf("---------------------------------\n");
+    const int k = in.nz > 2 ? 2 : 0;
+    for (int j = in.ny - 1; j >= 0; j--) {
+      for (int i = 0; i < in.nx; i++) {
+        const size_t id =
+            9 + DIRECTION_SIZE * ((size_t)i + (size_t)k * in.nx + (size_t)j * in.nx * in.nz);
+        std::printf("%8.6f ", arF[id]);
       }
-      if (ok && icycle % in.nwrite == 0) {
-        if (writer.joinable()) writer.join();
-        ok = write_rc == LBM_OK && lbm_snapshot(d) == LBM_OK;
-        const int index = icycle / in.nwrite, type = in.savetype;
-        if (ok) writer = std::thread([&write_rc, d, type, outdir, index] {
-            write_rc = lbm_save_snapshot(d, type, outdir, index);
-          });
-      }
+      std::printf("\n");
     }
-    if (writer.joinable()) writer.join();
-    ok = ok && write_rc == LBM_OK && lbm_sync(d) == LBM_OK;
+    std::printf("\n---------------------------------\n");
+  } catch (const lbm_b200::Error& e) {
+    std::fprintf(stderr, " - Error: %s\n", e.what());
+    rc = 1;
   }
-  if (!ok) {
-    std::fprintf(stderr, " - Error: %s\n", lbm_last_error());
-    lbm_destroy(d);
-    return 1;
-  }
-  auto t1 = std::chrono::high_resolution_clock::now();
-  std::chrono::duration<double> el = t1 - t0;
-  std::printf(" - Elapsed time(GPU) = %fs | h=%d | %.1f MLUPS\n", el.count(), in.h,
-              (double)in.nx * in.ny * in.nz * in.maxitr / el.count() / 1e6);
-
-  std::vector<float> arF((size_t)in.nx * in.ny * in.nz * DIRECTION_SIZE);
-  if (lbm_export_arF(d, arF.data(), 0) != LBM_OK) {
-    std::fprintf(stderr, " - Error: %s\n", lbm_last_error());
-    lbm_destroy(d);
-    return 1;
-  }
-  std::printf("---------------------------------\n");
-  const int k = in.nz > 2 ? 2 : 0;
-  for (int j = in.ny - 1; j >= 0; j--) {
-    for (int i = 0; i < in.nx; i++) {
-      size_t id = 9 + DIRECTION_SIZE * ((size_t)i + (size_t)k * in.nx + (size_t)j * in.nx * in.nz);
-      std::printf("%8.6f ", arF[id]);
-    }
-    std::printf("\n");
-  }
-  std::printf("\n---------------------------------\n");
-  lbm_destroy(d);
-  return 0;
+  delete psolver;
+  return rc;
 }

@@ -86,8 +86,8 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (int i = 0; i < kWaitIters; ++i)
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int iters) {
+  for (int i = 0; i < iters; ++i)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
@@ -119,10 +119,15 @@ __device__ __forceinline__ F2 lds_pair<__nv_bfloat16>(const __nv_bfloat16* p, in
   return F2{__fmul2_rn(h, make_float2(inv_scale, inv_scale))};
 }
 
+// stall_tile >= 0 (the wait test of lbm_options.wait_test): the producer
+// issues no copy for that tile and stops there, and every wait gives up after
+// wait_iters tries; the copies it issued before are all drained by the
+// consumers ahead of the withheld tile, so none is in flight when the
+// consumers give up and the CTA exits.
 template <class S, int COLL, bool LES>
 __global__ void __launch_bounds__(TmaCfg<S>::THREADS, 1)
     k_step_tma(const __grid_constant__ StepArgs<S> a, const __grid_constant__ CUtensorMap src_map,
-               int* __restrict__ err) {
+               int* __restrict__ err, int stall_tile, int wait_iters) {
   using C = TmaCfg<S>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   // 128-byte aligned stage base, derived by pointer arithmetic on the
@@ -152,7 +157,8 @@ __global__ void __launch_bounds__(TmaCfg<S>::THREADS, 1)
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
       const int s = i % C::STAGES;
       const uint32_t ph = (uint32_t)(i / C::STAGES) & 1u;
-      if (!mbar_wait(smem_addr(&empty[s]), ph ^ 1u)) {
+      if (t == stall_tile) break;  // the wait test: this tile's copies are withheld
+      if (!mbar_wait(smem_addr(&empty[s]), ph ^ 1u, wait_iters)) {
         atomicExch(err, kErrProducerWait);
         break;
       }
@@ -201,7 +207,7 @@ __global__ void __launch_bounds__(TmaCfg<S>::THREADS, 1)
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
     const int s = i % C::STAGES;
     const uint32_t ph = (uint32_t)(i / C::STAGES) & 1u;
-    if (!mbar_wait(smem_addr(&full[s]), ph)) {
+    if (!mbar_wait(smem_addr(&full[s]), ph, wait_iters)) {
       atomicExch(err, kErrConsumerWait);
       return;
     }

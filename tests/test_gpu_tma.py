@@ -72,3 +72,31 @@ def test_tma_matches_scalar_kernel_closely():
     b = run(iv, 200, kernel=pkg.KERNEL_SCALAR)
     fa, fb = a.export_arF(), b.export_arF()
     assert O.rel_field_err(fa, fb) <= 1e-6
+
+
+def test_bounded_wait_gives_up_with_timeout_and_the_device_stays_usable():
+    """The failure path of the TMA kernel's bounded mbarrier waits: with
+    wait_test the producer withholds the copies of one tile (a barrier that
+    nothing completes) and the waits give up after ~1 ms; the step reports
+    LBM_ERR_TIMEOUT at the next synchronising call instead of hanging, and a
+    fresh domain on the same device then steps normally."""
+    iv = pkg.make_inputval(64, 32, 32, casetype=pkg.CAVITY, re=100.0, u=0.1, mrt=True, les=True,
+                           cs=0.1, h=64)
+    d = pkg.Domain(iv, pkg.default_options(kernel=pkg.KERNEL_TMA, wait_test=3))
+    d.run(1)
+    with pytest.raises(pkg.LbmError) as e:
+        d.sync()
+    assert e.value.code == pkg.LBM_ERR_TIMEOUT
+    d.close()
+    good = pkg.Domain(iv, pkg.default_options(kernel=pkg.KERNEL_TMA))
+    good.run(5)
+    good.sync()
+    plain = pkg.Domain(iv, pkg.default_options(kernel=pkg.KERNEL_SCALAR))
+    plain.run(5)
+    a, b = good.macroscopic(), plain.macroscopic()
+    good.close()
+    plain.close()
+    assert O.rel_field_err(a[0], b[0]) <= 1e-6
+    with pytest.raises(pkg.LbmError) as e:
+        pkg.Domain(iv, pkg.default_options(kernel=pkg.KERNEL_SCALAR, wait_test=1))
+    assert e.value.code == pkg.LBM_ERR_INVALID

@@ -205,3 +205,47 @@ def test_pattern_ceiling_rejects_bad_arguments():
         assert L.lbm_pattern_ceiling(*args, C.byref(m), C.byref(g)) == pkg.LBM_ERR_INVALID, args
     assert L.lbm_pattern_ceiling(pkg.PATTERN_PULL, pkg.STORE_F32, 64, 2, None, None) == \
         pkg.LBM_ERR_INVALID
+
+
+def test_compat_header_compiles_and_runs_the_host_functions(tmp_path):
+    """include/lbm_b200_compat.hpp compiled by a C++ caller that uses the
+    reference's spelling: LBMSolver's tables, decomposition, inverseMRT
+    (host numerics only, no device needed)."""
+    src = tmp_path / "caller.cpp"
+    src.write_text(r'''
+#include <cstdio>
+#include "lbm_b200_compat.hpp"
+int main() {
+  LBMSolver s;
+  Inputval in{};
+  in.h = in.nx = in.ny = in.nz = 10;
+  static int Slice[TILE_NUM][DIMENSION][2];
+  int n = decomposition(&in, Slice);
+  std::vector<std::vector<float>> m(DIRECTION_SIZE, std::vector<float>(DIRECTION_SIZE)), inv;
+  float M[DIRECTION_SIZE * DIRECTION_SIZE];
+  lbm_d3q19_tables(nullptr, nullptr, nullptr, M);
+  for (int i = 0; i < DIRECTION_SIZE; ++i)
+    for (int j = 0; j < DIRECTION_SIZE; ++j) m[i][j] = M[i * DIRECTION_SIZE + j];
+  inverseMRT(m, inv);
+  double e = 0;
+  for (int i = 0; i < DIRECTION_SIZE; ++i)
+    for (int j = 0; j < DIRECTION_SIZE; ++j) {
+      double acc = 0;
+      for (int k = 0; k < DIRECTION_SIZE; ++k) acc += m[i][k] * inv[k][j];
+      e += acc - (i == j);
+    }
+  std::printf("%d %d %.6f %.6f %d %g\n", n, s.m_HostOppIndex[7], s.m_HostW[0], s.m_HostW[18],
+              s.m_pDomain == nullptr, e);
+  return 0;
+}
+''')
+    exe = tmp_path / "caller"
+    pkgdir = os.path.join(O.ROOT if hasattr(O, "ROOT") else os.path.dirname(os.path.dirname(
+        os.path.abspath(__file__))), "nflow-red-poplar_b200")
+    inc = os.path.join(os.path.dirname(pkgdir), "include")
+    subprocess.run(["g++", "-std=c++17", "-O1", "-I", inc, str(src), "-L", pkgdir, "-llbm_b200",
+                    "-Wl,-rpath," + pkgdir, "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
+    assert out[0] == "27" and out[1] == "10"
+    assert abs(float(out[2]) - 1 / 3) < 1e-6 and abs(float(out[3]) - 1 / 36) < 1e-6
+    assert out[4] == "1" and abs(float(out[5])) < 1e-3
