@@ -477,10 +477,11 @@ __device__ __forceinline__ uint32_t sr_hash(uint32_t word, uint32_t k, uint32_t 
   h ^= h >> 16;
   return h;
 }
+// bits of population q: h times an odd constant per q (a bijection of h,
+// so each population's bits are uniform, and one multiply per store)
 template <int q>
 __device__ __forceinline__ uint32_t sr_bits(uint32_t h) {
-  uint32_t r = h * (0x2C1B3C6Du + 2u * (uint32_t)q * 0x9E3779B9u);  // odd multiplier per q
-  return r ^ (r >> 16);
+  return h * (0x2C1B3C6Du + 2u * (uint32_t)q * 0x9E3779B9u);
 }
 __device__ __forceinline__ uint32_t sr_word(const Geometry& g, int x, int y, int z) {
   const int h = g.px >> 1;
@@ -1126,8 +1127,12 @@ __host__ __device__ __forceinline__ bool paired_kernel_applies(const Geometry& g
 
 // grid = (ceil(H / 128), nz, ny), 128 threads, one word (two nodes) per
 // thread; a.srcd[q] = plane q minus the donor offset 2 c_x + px (c_z + nz c_y)
+#ifndef LBM_PAIRED_SR_THREADS_PER_SM
+#define LBM_PAIRED_SR_THREADS_PER_SM 768
+#endif
 template <class S, int COLL, bool LES, bool SR>
-__global__ void __launch_bounds__(128, LBM_PAIRED_THREADS_PER_SM / 128)
+__global__ void __launch_bounds__(128, (SR ? LBM_PAIRED_SR_THREADS_PER_SM
+                                           : LBM_PAIRED_THREADS_PER_SM) / 128)
     k_step_paired(const __grid_constant__ StepArgs<S> a) {
   static_assert(kDev<S>, "paired rows are a 16-bit layout");
   const int H = a.g.px >> 1;
