@@ -400,16 +400,20 @@ def _case_iv(pkg, c):
                               les=c["mrt"], cs=0.1), pkg.INIT_CHANNEL, 0.01)
 
 
-def report_batch(args, pkg):
+def batch_c4(pkg, ndom=256, steps=64, warmup=4, streaming="ab", batch_shape="",
+             storages=("f32", "f16_shift")):
     """256 independent domains in one persistent launch per step
     (CUDA-graph chunks, autotuned launch shape) vs each domain launched
-    alone, for FP32 and FP16-shift storage; --streaming aa keeps every
-    domain in one lattice (AA pattern), ab in two (pull)."""
-    ndom = args.domains
-    mode = pkg.STREAM_AA if args.streaming == "aa" else pkg.STREAM_AB
-    res = {"report": "batch", "domains": ndom, "steps": args.steps, "data": "synthetic (seeded)",
-           "streaming": args.streaming, "forms": {}}
-    for sname, st in (("f32", pkg.STORE_F32), ("f16_shift", pkg.STORE_F16_SHIFT)):
+    alone, for FP32 and FP16-shift storage; streaming "aa" keeps every
+    domain in one lattice (AA pattern), "ab" in two (pull).  Batched MLUPS
+    are device time (CUDA events on the batch stream) of `steps` steps;
+    alone MLUPS sum the device time of each domain's own `steps` steps."""
+    mode = pkg.STREAM_AA if streaming == "aa" else pkg.STREAM_AB
+    sid = {"f32": pkg.STORE_F32, "f16_shift": pkg.STORE_F16_SHIFT}
+    res = {"domains": ndom, "steps": steps, "data": "synthetic (seeded)",
+           "streaming": streaming, "forms": {}}
+    for sname in storages:
+        st = sid[sname]
         cases = _c4_domains(7, ndom, st)
         ivs = [_case_iv(pkg, c) for c in cases]
         opts = [pkg.default_options(storage=st, init_kind=k, noise_amp=a, seed=i + 1,
@@ -417,8 +421,8 @@ def report_batch(args, pkg):
                 for i, (iv, k, a) in enumerate(ivs)]
         need = sum(pkg.batch_domain_bytes(iv, o) for (iv, _, _), o in zip(ivs, opts))
         shape = {}
-        if args.batch_shape:  # fixed launch shape, no autotuning (profiling)
-            sc, rg, bl, npt = (int(v) for v in args.batch_shape.split(","))
+        if batch_shape:  # fixed launch shape, no autotuning (profiling)
+            sc, rg, bl, npt = (int(v) for v in batch_shape.split(","))
             shape = dict(schedule=sc, regs=rg, block=bl, nodes_per_thread=npt)
         b = pkg.Batch(hbm_budget=int(need * 1.02) + (64 << 20), chunk_steps=32, **shape)
         t0 = time.perf_counter()
@@ -427,12 +431,12 @@ def report_batch(args, pkg):
         b.sync()
         t_admit = time.perf_counter() - t0
         cfg = b.autotune(trial_steps=32) if not shape else dict(shape, fixed=True)
-        b.step(args.warmup)
+        b.step(warmup)
         b.sync()
-        b.step(args.steps)
+        b.step(steps)
         ms, lups = b.last_step_ms()
         nodes = sum(iv.nx * iv.ny * iv.nz for iv, _, _ in ivs)
-        batched = lups / (ms * args.steps / 1e3) / 1e6
+        batched = lups / (ms * steps / 1e3) / 1e6
         nonfinite = 0
         steps_done = []
         for i in list(b.ivs):
@@ -445,35 +449,45 @@ def report_batch(args, pkg):
         nonfinite_alone = 0
         for ((iv, _, _), o), sd in zip(zip(ivs, opts), steps_done):
             d = pkg.Domain(iv, o)
-            d.run(args.warmup)
-            d.run(args.steps)
-            t_alone += d.last_run_ms() * args.steps / 1e3
+            d.run(warmup)
+            d.run(steps)
+            t_alone += d.last_run_ms() * steps / 1e3
             # the same step count as in the batch (autotuner trials included)
-            d.run(max(0, sd - args.warmup - args.steps))
+            d.run(max(0, sd - warmup - steps))
             nonfinite_alone += int(d.diagnostics()[7] > 0)
             d.close()
-        alone = nodes * args.steps / t_alone / 1e6
+        alone = nodes * steps / t_alone / 1e6
         bpl = 2 * 19 * BYTES[sname]
+        peak, _ = measured_peak()
         res["forms"][sname] = {"batched_MLUPS": batched, "alone_MLUPS": alone,
                                "batched_over_alone": batched / alone, "nodes": nodes,
                                "pool_GB": need / 1e9, "admit_s": t_admit, "autotuned": cfg,
                                "batched_GB_s": batched * 1e6 * bpl / 1e9,
+                               "batched_frac_of_hbm": batched * 1e6 * bpl / 1e9 / peak,
                                "domains_nonfinite": nonfinite,
                                "domains_nonfinite_alone": nonfinite_alone}
-    print(json.dumps(res), flush=True)
+    return res
 
 
-def report_serving(args, pkg):
-    """Seeded Poisson arrivals, cavity/channel solves with edge
-    32-192, steps U[500, 5000], Re log-U[100, 5000], FP16-shift or FP32 per
-    request (MRT+LES), admitted by an HBM budget and stepped by continuous
-    batching; time-to-solution (arrival -> result on the host) and service
-    time (admission -> result) over a bounded wall-clock window."""
-    rate = args.rate
-    window = args.window
-    budget = int(min(150e9, args.budget_gb * 1e9))
-    rng = np.random.default_rng(11)
-    nreq = 20000
+def report_batch(args, pkg):
+    out = batch_c4(pkg, args.domains, args.steps, args.warmup, args.streaming, args.batch_shape)
+    out["report"] = "batch"
+    print(json.dumps(out), flush=True)
+
+
+def serving_c5(pkg, rate=200.0, window=20.0, budget_gb=150.0, policy="shortest", tol=0.0,
+               streaming="ab", horizon=0.0, nominal_mlups=30000.0, nreq=20000, seed=11):
+    """Seeded Poisson arrivals (mean `rate` req/s, up to `nreq` requests) of
+    cavity/channel solves with edge 32-192, steps U[500, 5000], Re
+    log-U[100, 5000], FP16-shift or FP32 storage per request (MRT+LES).  This
+    function only generates the stream: each request is handed to the
+    library's serving loop (pkg.Server: lbm_server_submit at its arrival
+    time, lbm_server_progress turns in between), which admits by HBM budget
+    (and the backlog horizon), steps by continuous batching, checks residuals
+    and retires.  Over a bounded wall-clock window; the time stamps and
+    percentiles are the library's (lbm_server_stats)."""
+    budget = int(min(150e9, budget_gb * 1e9))
+    rng = np.random.default_rng(seed)
     arrivals = np.cumsum(rng.exponential(1.0 / rate, nreq))
     reqs = []
     for i in range(nreq):
@@ -483,76 +497,54 @@ def report_serving(args, pkg):
         steps = int(rng.integers(500, 5001))
         st = pkg.STORE_F16_SHIFT if rng.random() < 0.5 else pkg.STORE_F32
         reqs.append(dict(t=float(arrivals[i]), e=e, cavity=cav, re=re, steps=steps, storage=st))
-    b = pkg.Batch(hbm_budget=budget, chunk_steps=32)
-    queue, active, tts, service, done_lups = [], {}, [], [], 0
+    mode = pkg.STREAM_AA if streaming == "aa" else pkg.STREAM_AB
+    pol = {"fifo": pkg.SERVE_FIFO, "shortest": pkg.SERVE_SHORTEST}[policy]
+    srv = pkg.Server(hbm_budget=budget, chunk_steps=32, policy=pol, check_every=256,
+                     backlog_horizon_s=horizon, nominal_mlups=nominal_mlups if horizon else 0.0)
     nxt = 0
-    admitted = 0
-    executed = 0   # lattice updates issued to the GPU in the window
-    # admission stops while the resident backlog (remaining lattice updates)
-    # exceeds horizon seconds at the nominal rate: requests then finish in
-    # about their own share instead of all sharing the GPU until the end
-    backlog_cap = args.horizon * args.nominal_mlups * 1e6 if args.horizon > 0 else float("inf")
     t0 = time.perf_counter()
     while True:
         now = time.perf_counter() - t0
         if now > window:
             break
         while nxt < nreq and reqs[nxt]["t"] <= now:
-            queue.append(reqs[nxt])
-            nxt += 1
-        backlog = sum(n * left for (_, _, n, left) in active.values())
-        while queue and backlog < backlog_cap:  # FIFO while the head fits the budget
-            r = queue[0]
+            r = reqs[nxt]
             iv, k, a = _case_iv(pkg, dict(e=r["e"], cavity=r["cavity"], re=r["re"], mrt=True))
-            o = pkg.default_options(storage=r["storage"], init_kind=k, noise_amp=a, seed=nxt + 1,
-                                    stream_mode=(pkg.STREAM_AA if args.streaming == "aa"
-                                                 else pkg.STREAM_AB))
-            try:
-                i = b.add(iv, o, r["steps"])
-            except pkg.LbmError as ex:
-                if ex.code == pkg.LBM_ERR_BUDGET:
-                    break
-                raise
-            queue.pop(0)
-            nodes = iv.nx * iv.ny * iv.nz
-            active[i] = [r, time.perf_counter() - t0, nodes, r["steps"]]
-            backlog += nodes * r["steps"]
-            admitted += 1
-        if not active:
+            o = pkg.default_options(storage=r["storage"], init_kind=k, noise_amp=a,
+                                    seed=nxt + 1, stream_mode=mode)
+            srv.submit(iv, o, steps=r["steps"], tol=tol)
+            nxt += 1
+        st = srv.stats()
+        if st["queued"] == 0 and st["resident"] == 0:
             if nxt < nreq:
                 time.sleep(max(0.0, min(reqs[nxt]["t"] - now, window - now)))
             continue
-        b.step(32)
-        for v in active.values():
-            took = min(32, v[3])
-            executed += v[2] * took
-            v[3] -= took
-        for i in b.poll():
-            r, t_adm, nodes, _ = active.pop(i)
-            den, ux, uy, uz = b.fetch(i)  # the result reaches the host
-            t_done = time.perf_counter() - t0
-            tts.append(t_done - r["t"])
-            service.append(t_done - t_adm)
-            done_lups += nodes * r["steps"]
-            b.remove(i)
-    elapsed = time.perf_counter() - t0
-    b.close()
-
-    def pct(v, p):
-        return float(np.percentile(v, p)) if v else None
-    print(json.dumps({
-        "report": "serving", "rate_req_s": rate, "window_s": window, "budget_GB": budget / 1e9,
-        "streaming": args.streaming,
-        "arrived": nxt, "admitted": admitted, "completed": len(tts), "queued_at_end": len(queue),
-        "tts_p50_s": pct(tts, 50), "tts_p99_s": pct(tts, 99),
-        "service_p50_s": pct(service, 50), "service_p99_s": pct(service, 99),
-        "completed_MLUPS": done_lups / elapsed / 1e6,
-        "aggregate_MLUPS": executed / elapsed / 1e6,
-        "admission": {"hbm_budget_GB": budget / 1e9, "backlog_horizon_s": args.horizon,
-                      "nominal_MLUPS": args.nominal_mlups},
+        srv.progress()
+    st = srv.stats()
+    srv.close()
+    return {
+        "rate_req_s": rate, "window_s": window, "budget_GB": budget / 1e9, "policy": policy,
+        "residual_tol": tol, "streaming": streaming,
+        "arrived": nxt, "admitted": st["admitted"], "completed": st["completed"],
+        "converged_early": st["converged"], "queued_at_end": st["queued"],
+        "resident_at_end": st["resident"],
+        "tts_p50_s": st["tts_p50_s"], "tts_p99_s": st["tts_p99_s"],
+        "service_p50_s": st["service_p50_s"], "service_p99_s": st["service_p99_s"],
+        "completed_MLUPS": st["completed_lups"] / st["elapsed_s"] / 1e6,
+        "aggregate_MLUPS": st["executed_lups"] / st["elapsed_s"] / 1e6,
+        "admission": {"hbm_budget_GB": budget / 1e9, "backlog_horizon_s": horizon,
+                      "nominal_MLUPS": nominal_mlups},
         "offered_LUPS": float(np.mean([(r["e"] ** 3 if r["cavity"] else 4 * r["e"] ** 3) *
                                        r["steps"] for r in reqs]) * rate),
-        "data": "synthetic (seeded Poisson stream)"}), flush=True)
+        "loop": "lbm_server_* (C++ library); bench.py only generates the arrival stream",
+        "data": "synthetic (seeded Poisson stream)"}
+
+
+def report_serving(args, pkg):
+    out = serving_c5(pkg, args.rate, args.window, args.budget_gb, args.policy, args.tol,
+                     args.streaming, args.horizon, args.nominal_mlups)
+    out["report"] = "serving"
+    print(json.dumps(out), flush=True)
 
 
 def main():
@@ -577,7 +569,15 @@ def main():
                     help="batch: fixed launch shape 'schedule,regs,block,nodes_per_thread' "
                          "instead of autotuning")
     ap.add_argument("--rate", type=float, default=200.0, help="serving: arrivals per second")
-    ap.add_argument("--window", type=float, default=60.0, help="serving: wall-clock window (s)")
+    ap.add_argument("--window", type=float, default=20.0, help="serving: wall-clock window (s)")
+    ap.add_argument("--policy", default="shortest", choices=["fifo", "shortest"],
+                    help="serving: admission order")
+    ap.add_argument("--tol", type=float, default=0.0,
+                    help="serving: residual tolerance for early retirement (0 = full budget)")
+    ap.add_argument("--c4-steps", type=int, default=64,
+                    help="timed steps of the batched comparison the default run reports")
+    ap.add_argument("--c5-window", type=float, default=20.0,
+                    help="wall-clock window of the serving run the default run reports")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="serving: HBM budget")
     ap.add_argument("--horizon", type=float, default=0.0,
                     help="serving: admit while the resident backlog is below this many seconds "
@@ -742,6 +742,9 @@ def main():
             line["cpu_baseline"] = cpu_baseline(pkg, w)
             line["pattern_ceilings"] = pattern_ceilings(pkg)
             line["precision_c3"] = precision_c3(pkg, args.c3_steps, pkg.KERNEL_AUTO)
+            line["batch_c4"] = batch_c4(pkg, 256, args.c4_steps, 4)
+            line["serving_c5"] = serving_c5(pkg, 200.0, args.c5_window, 150.0, "shortest",
+                                            0.0, "ab")
     else:
         dom.close()
 

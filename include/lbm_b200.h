@@ -549,6 +549,91 @@ int lbm_batch_autotune(lbm_batch* b, int trial_steps, lbm_batch_options* chosen)
  * updates issued by that call. */
 int lbm_batch_last_step_ms(lbm_batch* b, float* ms, long long* lups);
 
+/* ------------------------------------------------------------------ */
+/* Serving: a request queue over one batch.  A request is one solve (a  */
+/* case, its options, a step budget and an optional residual            */
+/* tolerance).  lbm_server_progress admits queued requests while their  */
+/* state fits the pool (and the resident backlog stays under a horizon),*/
+/* runs one chunk of steps for every resident request, and retires the  */
+/* requests that reached their budget or whose density residual         */
+/* sum |rho_k - rho_(k-1)| (the quantity kernel.cu:232-248 prints) fell */
+/* to their tolerance at a check, copying rho and u to host memory and  */
+/* returning their device memory to the pool.  No reference             */
+/* counterpart: the reference runs one case per program.                */
+/* ------------------------------------------------------------------ */
+typedef struct lbm_server lbm_server;
+
+enum {
+  LBM_SERVE_FIFO = 0,     /* arrival order; a request that does not fit blocks
+                             the ones behind it (no overtaking)               */
+  LBM_SERVE_SHORTEST = 1  /* least work (nodes x steps) first; requests that
+                             do not fit are skipped                           */
+};
+
+enum { LBM_REQ_QUEUED = 0, LBM_REQ_RESIDENT = 1, LBM_REQ_DONE = 2 };
+
+typedef struct lbm_server_options {
+  lbm_batch_options batch;  /* the batch under the queue (pool, chunk, ...)  */
+  int policy;               /* LBM_SERVE_*                                    */
+  int check_every;          /* steps between residual checks: a positive
+                               multiple of the chunk, default 256              */
+  double backlog_horizon_s; /* > 0: admit while the resident requests owe at
+                               most this many seconds of work at
+                               nominal_mlups; 0 = limited by the pool only    */
+  double nominal_mlups;     /* the rate the horizon is measured in            */
+  int reserved[6];
+} lbm_server_options;
+
+typedef struct lbm_server_request {
+  int state;                /* LBM_REQ_*                                       */
+  int converged;            /* 1: retired early at its residual tolerance      */
+  long long steps_done;
+  double residual;          /* last checked residual, -1 if never checked      */
+  double t_arrive, t_admit, t_done;  /* seconds since the server was created,
+                                        -1 where not reached                 */
+} lbm_server_request;
+
+typedef struct lbm_server_summary {
+  long long submitted, admitted, completed, converged, queued, resident;
+  double elapsed_s;                   /* since the server was created          */
+  double tts_p50_s, tts_p99_s;        /* arrival -> result on the host         */
+  double service_p50_s, service_p99_s;/* admission -> result on the host       */
+  double executed_lups;               /* lattice updates run                    */
+  double completed_lups;              /* ... by requests that completed         */
+  double aggregate_mlups;             /* executed_lups / elapsed_s / 1e6        */
+  size_t pool_used_bytes;
+} lbm_server_summary;
+
+void lbm_server_default_options(lbm_server_options* so);
+int lbm_server_create(const lbm_server_options* so, lbm_server** out);
+int lbm_server_destroy(lbm_server* s);
+
+/* Queue a request; *id names it.  LBM_ERR_BUDGET when its state can never
+ * fit the pool.  tol > 0 enables the residual check (domains of at most
+ * 67,108,864 nodes); tol = 0 runs the full budget. */
+int lbm_server_submit(lbm_server* s, const Inputval* pinput, const lbm_options* opt,
+                      long long steps, double tol, int* id);
+
+/* One turn of the loop: admit, one chunk, checks, retire.  *completed (may
+ * be NULL) = requests that completed during the call. */
+int lbm_server_progress(lbm_server* s, int* completed);
+
+/* Turn the loop until request id is done. */
+int lbm_server_wait(lbm_server* s, int id);
+
+/* Status of a request, and (when done) its CurrDen / CurrVel* in
+ * [ny][nz][nx]; any pointer may be NULL. */
+int lbm_server_result(lbm_server* s, int id, float* den, float* velx, float* vely, float* velz,
+                      lbm_server_request* info);
+
+/* Forget a done request and free its host copy. */
+int lbm_server_release(lbm_server* s, int id);
+
+int lbm_server_stats(lbm_server* s, lbm_server_summary* st);
+
+/* The batch under the queue (owned by the server). */
+int lbm_server_batch(lbm_server* s, lbm_batch** b);
+
 #ifdef __cplusplus
 }
 #endif

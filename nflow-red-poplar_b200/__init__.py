@@ -45,6 +45,8 @@ KERNEL_AUTO, KERNEL_SCALAR, KERNEL_PACKED, KERNEL_TMA, KERNEL_PAIRED = 0, 1, 2, 
 ROUND_NEAREST, ROUND_STOCHASTIC = 0, 1
 (PATTERN_COPY, PATTERN_PULL, PATTERN_PULL_PAIRED, PATTERN_AA_LOCAL, PATTERN_AA_NEIGHBOR,
  PATTERN_AA_LOCAL_V8, PATTERN_AA_LOCAL_V16) = range(7)
+SERVE_FIFO, SERVE_SHORTEST = 0, 1
+REQ_QUEUED, REQ_RESIDENT, REQ_DONE = 0, 1, 2
 
 
 class Inputval(C.Structure):
@@ -77,6 +79,33 @@ class BatchOptions(C.Structure):
         ("device", C.c_int), ("hbm_budget", C.c_size_t), ("chunk_steps", C.c_int),
         ("block", C.c_int), ("nodes_per_thread", C.c_int), ("ctas_per_sm", C.c_int),
         ("schedule", C.c_int), ("regs", C.c_int), ("reserved", C.c_int * 6),
+    ]
+
+
+class ServerOptions(C.Structure):
+    _fields_ = [
+        ("batch", BatchOptions), ("policy", C.c_int), ("check_every", C.c_int),
+        ("backlog_horizon_s", C.c_double), ("nominal_mlups", C.c_double),
+        ("reserved", C.c_int * 6),
+    ]
+
+
+class ServerRequest(C.Structure):
+    _fields_ = [
+        ("state", C.c_int), ("converged", C.c_int), ("steps_done", C.c_longlong),
+        ("residual", C.c_double), ("t_arrive", C.c_double), ("t_admit", C.c_double),
+        ("t_done", C.c_double),
+    ]
+
+
+class ServerSummary(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_longlong), ("admitted", C.c_longlong), ("completed", C.c_longlong),
+        ("converged", C.c_longlong), ("queued", C.c_longlong), ("resident", C.c_longlong),
+        ("elapsed_s", C.c_double), ("tts_p50_s", C.c_double), ("tts_p99_s", C.c_double),
+        ("service_p50_s", C.c_double), ("service_p99_s", C.c_double),
+        ("executed_lups", C.c_double), ("completed_lups", C.c_double),
+        ("aggregate_mlups", C.c_double), ("pool_used_bytes", C.c_size_t),
     ]
 
 
@@ -181,6 +210,17 @@ def lib():
         L.lbm_pattern_ceiling.argtypes = [i32, i32, i32, i32, C.POINTER(C.c_double),
                                           C.POINTER(C.c_double)]
         L.lbm_device_fields.argtypes = [vp] + [C.POINTER(vp)] * 5
+        L.lbm_server_default_options.argtypes = [C.POINTER(ServerOptions)]
+        L.lbm_server_create.argtypes = [C.POINTER(ServerOptions), C.POINTER(vp)]
+        L.lbm_server_destroy.argtypes = [vp]
+        L.lbm_server_submit.argtypes = [vp, C.POINTER(Inputval), C.POINTER(Options),
+                                        C.c_longlong, C.c_double, C.POINTER(C.c_int)]
+        L.lbm_server_progress.argtypes = [vp, C.POINTER(C.c_int)]
+        L.lbm_server_wait.argtypes = [vp, i32]
+        L.lbm_server_result.argtypes = [vp, i32, vp, vp, vp, vp, C.POINTER(ServerRequest)]
+        L.lbm_server_release.argtypes = [vp, i32]
+        L.lbm_server_stats.argtypes = [vp, C.POINTER(ServerSummary)]
+        L.lbm_server_batch.argtypes = [vp, C.POINTER(vp)]
         _lib = L
     return _lib
 
@@ -483,6 +523,74 @@ class Batch:
         ms, lups = C.c_float(), C.c_longlong()
         check(lib().lbm_batch_last_step_ms(self.h, C.byref(ms), C.byref(lups)))
         return ms.value, lups.value
+
+
+class Server:
+    """A request queue over one batch: admission into the HBM pool, one chunk
+    of steps per progress() turn, residual checks and early retirement; the
+    loop itself is the C++ library's (lbm_server_*)."""
+
+    def __init__(self, hbm_budget=1 << 30, device=0, chunk_steps=32, policy=SERVE_FIFO,
+                 check_every=256, backlog_horizon_s=0.0, nominal_mlups=0.0, **batch_kw):
+        o = ServerOptions()
+        lib().lbm_server_default_options(C.byref(o))
+        o.batch.device, o.batch.hbm_budget, o.batch.chunk_steps = device, hbm_budget, chunk_steps
+        for k, v in batch_kw.items():
+            setattr(o.batch, k, v)
+        o.policy, o.check_every = policy, check_every
+        o.backlog_horizon_s, o.nominal_mlups = backlog_horizon_s, nominal_mlups
+        h = C.c_void_p()
+        check(lib().lbm_server_create(C.byref(o), C.byref(h)))
+        self.h = h
+        self.ivs = {}
+
+    def close(self):
+        if self.h:
+            check(lib().lbm_server_destroy(self.h))
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, inputval, options=None, steps=1, tol=0.0):
+        opt = options if options is not None else default_options()
+        i = C.c_int()
+        check(lib().lbm_server_submit(self.h, C.byref(inputval), C.byref(opt), int(steps),
+                                      float(tol), C.byref(i)))
+        self.ivs[i.value] = inputval
+        return i.value
+
+    def progress(self):
+        n = C.c_int()
+        check(lib().lbm_server_progress(self.h, C.byref(n)))
+        return n.value
+
+    def wait(self, i):
+        check(lib().lbm_server_wait(self.h, int(i)))
+
+    def info(self, i):
+        r = ServerRequest()
+        check(lib().lbm_server_result(self.h, int(i), None, None, None, None, C.byref(r)))
+        return {k: getattr(r, k) for k, _ in ServerRequest._fields_}
+
+    def result(self, i):
+        """rho, ux, uy, uz [ny][nz][nx] of a done request."""
+        iv = self.ivs[i]
+        out = [np.empty((iv.ny, iv.nz, iv.nx), np.float32) for _ in range(4)]
+        check(lib().lbm_server_result(self.h, int(i), *[_ptr(a) for a in out], None))
+        return tuple(out)
+
+    def release(self, i):
+        check(lib().lbm_server_release(self.h, int(i)))
+        self.ivs.pop(i, None)
+
+    def stats(self):
+        st = ServerSummary()
+        check(lib().lbm_server_stats(self.h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in ServerSummary._fields_}
 
 
 def batch_domain_bytes(inputval, options=None):

@@ -412,6 +412,13 @@ void destroy_member(lbm_batch* b, lbm_batch::Member& m) {
 
 }  // namespace
 
+namespace lbm {
+// the stream every chunk of the batch runs on (the serving loop paces its
+// chunk issue with events on it)
+void* batch_stream(lbm_batch* b) { return b ? (void*)b->stream : nullptr; }
+int batch_device(lbm_batch* b) { return b ? b->opt.device : 0; }
+}  // namespace lbm
+
 extern "C" {
 
 void lbm_batch_default_options(lbm_batch_options* bo) {

@@ -764,6 +764,48 @@ struct AADst {
   __device__ __forceinline__ float scale() const { return a.scale; }
 };
 
+// The neighbour step of a node in a row that is not on a y or z face, for
+// the warps that hold an x face of such rows.  Only the populations whose
+// donor x - c_q or destination x + c_q leaves the box at x = 0 or x = nx-1
+// differ from the interior form, and only in their slot: a donor outside is
+// the node's own slot (x, q) (the wall rule of the node applied to it, which
+// for the cavity's fixed walls is the value itself), a destination outside
+// is the node's own slot (x, opp q) (the plain f*_q: x faces are fixed
+// walls, inlets or outlets, whose rules are applied when the natural slot
+// is read).  The slot is chosen per lane, so the warp does not diverge.
+template <class S, int COLL, bool LES>
+__device__ __forceinline__ void aa_neighbor_xface_node(const StepArgs<S>& a, int x, int y, int z,
+                                                       int cell) {
+  using R = RealOf<S>;
+  const bool xlo = x == 0, xhi = x == a.g.nx - 1;
+  R f[Q];
+  static_for<0, Q>([&](auto qc) {
+    constexpr int q = decltype(qc)::value;
+    const bool out = (cx(q) == 1 && xlo) || (cx(q) == -1 && xhi);
+    f[q] = ld((out ? a.srcq[q] : a.srcd[q]) + cell, q, a.inv_scale);
+  });
+  if (a.g.casetype != CAVITY && (xlo || xhi)) {
+    // inlet / outlet rules on the donors outside (the cavity's walls keep
+    // the value)
+    const int t = node_type(a.g, x, y, z);
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      if ((cx(q) == 1 && xlo) || (cx(q) == -1 && xhi))
+        f[q] = boundary_value<S, q>(a, t, f[q], y, z);
+    });
+  }
+  PairState<R> ps;
+  make_pairs<R, kDev<S>>(f, ps);
+  R ux, uy, uz;
+  const R inv_rho = velocity<R>(ps, ux, uy, uz);
+  write_macro<S>(a, x, y, z, ps.rho_full, ux, uy, uz);
+  collide_node<S, COLL, LES, kFromPairs<S>, R>(f, ps, ux, uy, uz, inv_rho, a, [&](auto qc, R v) {
+    constexpr int q = decltype(qc)::value;
+    const bool out = (cx(q) == -1 && xlo) || (cx(q) == 1 && xhi);
+    StoreTraits<S>::store(out ? a.dst + (opp(q) * a.qs + cell) : a.dstq[q] + cell, v, a.scale);
+  });
+}
+
 // One AA step of node (x, y, z) (shared by the single-domain and batched
 // kernels); neighbor = 0: local step (natural -> swapped), 1: neighbour
 // step (swapped -> natural).  entry (local steps): kAAPending, the natural
@@ -778,9 +820,16 @@ __device__ __forceinline__ void aa_step_node(const StepArgs<S>& a, int x, int y,
                                              int neighbor, int entry) {
   using R = RealOf<S>;
   const int cell = x + a.g.px * (z + a.g.nz * y);
-  const bool edge = (x == 0) | (x == a.g.nx - 1) | (y == 0) | (y == a.g.ny - 1) | (z == 0) |
-                    (z == a.g.nz - 1);
+  const bool face_row = (y == 0) | (y == a.g.ny - 1) | (z == 0) | (z == a.g.nz - 1);
+  const bool xface = (x == 0) | (x == a.g.nx - 1);
+  const bool edge = face_row | xface;
   R f[Q];
+  if (neighbor && !face_row && __any_sync(__activemask(), xface)) {
+    // a warp holding an x face of interior rows: every lane takes the
+    // x-face form (no divergence into the per-node face path)
+    aa_neighbor_xface_node<S, COLL, LES>(a, x, y, z, cell);
+    return;
+  }
   if (!neighbor || !edge) {
     static_for<0, Q>([&](auto qc) {
       constexpr int q = decltype(qc)::value;

@@ -249,3 +249,21 @@ int main() {
     assert out[0] == "27" and out[1] == "10"
     assert abs(float(out[2]) - 1 / 3) < 1e-6 and abs(float(out[3]) - 1 / 36) < 1e-6
     assert out[4] == "1" and abs(float(out[5])) < 1e-3
+
+
+def test_server_rejects_bad_options_before_any_device_call():
+    """lbm_server_create checks the policy and the residual-check spacing
+    (a positive multiple of the batch chunk) before it creates the batch."""
+    L = pkg.lib()
+    for policy, every, chunk in ((7, 256, 32), (pkg.SERVE_FIFO, 33, 32), (pkg.SERVE_FIFO, 0, 32),
+                                 (pkg.SERVE_SHORTEST, 48, 32), (pkg.SERVE_FIFO, 16, 32)):
+        o = pkg.ServerOptions()
+        L.lbm_server_default_options(C.byref(o))
+        o.policy, o.check_every, o.batch.chunk_steps = policy, every, chunk
+        h = C.c_void_p()
+        assert L.lbm_server_create(C.byref(o), C.byref(h)) == pkg.LBM_ERR_INVALID
+        assert not h.value
+    o = pkg.ServerOptions()
+    L.lbm_server_default_options(C.byref(o))
+    assert o.policy == pkg.SERVE_FIFO and o.check_every == 256
+    assert L.lbm_server_create(C.byref(o), None) == pkg.LBM_ERR_INVALID
