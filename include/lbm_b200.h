@@ -485,10 +485,10 @@ typedef struct lbm_batch_options {
   size_t hbm_budget;      /* bytes of the device pool holding every domain    */
   int chunk_steps;        /* steps per captured graph chunk (even), 0 = 32    */
   int block;              /* threads per CTA (128 or 256), 0 = autotuned/256  */
-  int nodes_per_thread;   /* nodes per thread per tile (1..16), 0 = 2         */
+  int nodes_per_thread;   /* nodes per lane per warp tile (1..16), 0 = 2      */
   int ctas_per_sm;        /* persistent CTAs per SM, 0 = max resident         */
-  int schedule;           /* 0: each CTA a contiguous range of tiles,
-                             1: grid-stride over the tile list                */
+  int schedule;           /* 0: each warp a contiguous range of tiles,
+                             1: warp-stride over the tile list                */
   int regs;               /* kernel build: 0 = 64 registers, 1 = 80           */
   int reserved[6];
 } lbm_batch_options;

@@ -578,6 +578,8 @@ class Server:
 
     def result(self, i):
         """rho, ux, uy, uz [ny][nz][nx] of a done request."""
+        if i not in self.ivs:  # the library reports the unknown id
+            check(lib().lbm_server_result(self.h, int(i), None, None, None, None, None))
         iv = self.ivs[i]
         out = [np.empty((iv.ny, iv.nz, iv.nx), np.float32) for _ in range(4)]
         check(lib().lbm_server_result(self.h, int(i), *[_ptr(a) for a in out], None))

@@ -5,10 +5,12 @@
 // an autotuner over the launch shape.
 //
 // Work-list.  Every active domain contributes ceil(nodes / tile) tiles, a
-// tile being block*npt consecutive nodes in the domain's [y][z][x] order.
-// tile_off[] is the prefix sum over the active domains; a CTA walks the
-// global tile index t = blockIdx.x, += gridDim.x, finds its domain by binary
-// search and copies that domain's kernel arguments into shared memory.
+// tile (a warp tile) being 32*npt consecutive nodes in the domain's
+// [y][z][x] order.  tile_off[] is the prefix sum over the active domains;
+// each warp walks its own tiles (a contiguous range, or t = warp, += warps
+// in the grid), finds a tile's domain by a search from its current one and
+// copies that domain's kernel arguments into its own shared memory, with
+// no barrier across the warps of a CTA.
 // Each node then runs step_node<S, COLL, LES>() (aa_step_node for members
 // with AA streaming) — the very function of the single-domain kernel — so a
 // domain produces the same bits alone and in a batch, whatever else is
@@ -29,12 +31,12 @@ using namespace lbm::batch;
 
 namespace {
 
-// variant -> kernel: storage = variant >> 3, model = (variant >> 1) & 3,
-// aa = variant & 1
+// variant -> kernel: variant = (storage * 4 + model) * kModes + mode
 BatchKernel batch_kernel(int variant, int regs) {
-  const int st = variant >> 3, model = (variant >> 1) & 3, aa = variant & 1;
+  const int mode = variant % kModes, model = (variant / kModes) % 4,
+            st = variant / (4 * kModes);
   const BatchKernels& t = st == 0 ? kBatch_f32 : (st == 1 ? kBatch_f16 : kBatch_bf16);
-  return t.k[model][regs == 1 ? 1 : 0][aa];
+  return t.k[model][regs == 1 ? 1 : 0][mode];
 }
 
 // First-fit device pool with coalescing (offsets 256-byte aligned).
@@ -172,9 +174,13 @@ int launch_grid(lbm_batch* b, int variant, int block, int* grid) {
   return LBM_OK;
 }
 
+int member_mode(const lbm_domain* d) {
+  return d->opt.stream_mode == LBM_STREAM_AA ? kModeAA
+                                             : (d->g.paired ? kModePaired : kModePull);
+}
+
 int member_variant(const lbm_domain* d) {
-  return (storage_index(d->opt.storage) * 4 + model_of(d->in)) * 2 +
-         (d->opt.stream_mode == LBM_STREAM_AA ? 1 : 0);
+  return (storage_index(d->opt.storage) * 4 + model_of(d->in)) * kModes + member_mode(d);
 }
 
 // Launch groups (variants) of the members that still have steps to take,
@@ -322,7 +328,7 @@ int issue_chunk(lbm_batch* b, int steps_offered, long long* lups) {
   if (groups.empty()) return LBM_OK;
   int rc = ensure_graph(b, groups);
   if (rc) return rc;
-  const int tile = b->graph_block * b->graph_npt;
+  const int tile = 32 * b->graph_npt;  // a warp tile
   CK(cudaEventSynchronize(b->tables_free));  // the pinned tables may be rewritten
   std::memset(b->h_tab->v, 0, sizeof(b->h_tab->v));
   int n = 0, noff = 0;
@@ -340,17 +346,20 @@ int issue_chunk(lbm_batch* b, int steps_offered, long long* lups) {
       if (left <= 0 || member_variant(d) != groups[g]) continue;
       const int active = (int)std::min<long long>(std::min(S, steps_offered), left);
       SlotMeta& sm = b->h_meta[n];
+      // items of a row: its nodes, or the words of a paired row
+      const int row_items = d->g.paired ? d->g.px / 2 : d->g.nx;
+      const long long items = (long long)row_items * d->g.nz * d->g.ny;
       sm.image_base = m.image_slot * kImages;
-      sm.nx = d->g.nx;
+      sm.nx = row_items;
       sm.nz = d->g.nz;
-      sm.mnx = ~0ull / (unsigned long long)d->g.nx + 1;
+      sm.mnx = ~0ull / (unsigned long long)row_items + 1;
       sm.mnz = ~0ull / (unsigned long long)d->g.nz + 1;
-      sm.nodes = d->N;
+      sm.nodes = items;
       sm.active = active;
       sm.cur0 = d->cur;
       sm.entry0 = d->aa_first ? kAAFromInit : (d->post_direct ? kAAComplete : kAAPending);
       b->h_off[noff++] = tiles;
-      tiles += (d->N + tile - 1) / tile;
+      tiles += (items + tile - 1) / tile;
       updates += d->N * active;
       // host bookkeeping of the steps this chunk takes
       d->step += active;
@@ -528,13 +537,17 @@ int lbm_batch_add(lbm_batch* b, const Inputval* pinput, const lbm_options* opt,
   if (target_steps < 0) return set_error(LBM_ERR_INVALID, "negative step target");
   if (opt && opt->storage == LBM_STORE_F64)
     return set_error(LBM_ERR_INVALID, "FP64 storage is not supported in batches");
-  if (opt && (opt->kernel == LBM_KERNEL_PACKED || opt->kernel == LBM_KERNEL_PAIRED))
-    return set_error(LBM_ERR_INVALID, "batches use the one-node-per-thread kernel");
+  if (opt && (opt->kernel == LBM_KERNEL_PACKED || opt->kernel == LBM_KERNEL_TMA))
+    return set_error(LBM_ERR_INVALID,
+                     "batches step one node (or one paired word) per thread: kernel AUTO, "
+                     "SCALAR or PAIRED");
   CK(cudaSetDevice(b->opt.device));
   if (b->free_images.empty() && (rc = grow_images(b))) return rc;
   lbm_domain* d = new lbm_domain();
   domain_prepare(d, pinput, opt);
-  d->g.paired = 0;  // the batched kernel steps plain rows
+  // 16-bit A/B members keep the paired rows of a single domain where the
+  // paired step applies (no STRUCT nodes, nx large enough), else plain rows
+  if (d->g.paired && !paired_kernel_applies(d->g)) d->g.paired = 0;
   d->opt.device = b->opt.device;
   d->pooled = true;
   d->stream = b->stream;

@@ -21,19 +21,21 @@ constexpr int kImages = 6;
 // per active domain, per chunk
 struct SlotMeta {
   int image_base;    // index of the domain's first argument image
-  int nx, nz;
+  int nx, nz;        // items per row (nodes, or words of paired rows), rows per plane
   int active;        // steps the domain takes in this chunk
   unsigned long long mnx, mnz;  // ceil(2^64 / n): exact 32-bit division
-  long long nodes;
+  long long nodes;   // items: nodes, or words of paired rows
   int cur0;          // lattice holding f* (AA: layout) at chunk start
   int entry0;        // AA: entry mode of the chunk's first step (k_aa_step)
 };
 
-// model: 0 SRT, 1 SRT+LES, 2 MRT, 3 MRT+LES; variant = (storage * 4 +
-// model) * 2 + aa (aa: AA streaming).  A launch group is the domains of one
-// variant; each step launches the group's kernel once.  Storage scales travel
-// in the argument images.
+// model: 0 SRT, 1 SRT+LES, 2 MRT, 3 MRT+LES; mode: kModePull (plain rows,
+// A/B), kModeAA (AA streaming), kModePaired (16-bit A/B in paired rows);
+// variant = (storage * 4 + model) * 3 + mode.  A launch group is the
+// domains of one variant; each step launches the group's kernel once.
+// Storage scales travel in the argument images.
 constexpr int kGroups = 32;
+enum { kModePull = 0, kModeAA = 1, kModePaired = 2, kModes = 3 };
 
 // The domains of one group: meta[slot0 .. slot0 + nslots) and their tile
 // prefix sums tile_off[off0 .. off0 + nslots] (tiles of the group's list).
@@ -46,8 +48,8 @@ struct GroupList {
 };
 
 struct BatchTables {
-  int tile;          // nodes per tile = block * npt
-  int schedule;      // 0: contiguous tile range per CTA, 1: grid-stride
+  int tile;          // nodes per tile = 32 * npt (a warp tile)
+  int schedule;      // 0: contiguous tile range per warp, 1: warp-stride
   GroupList v[kGroups];
   const SlotMeta* meta;
   const long long* tile_off;
@@ -58,142 +60,162 @@ __device__ __forceinline__ unsigned fastdiv(unsigned n, unsigned long long m) {
   return (unsigned)__umul64hi(m, (unsigned long long)n);
 }
 
-// the CTA's current domain, in shared memory: everything the tile loop
-// needs besides the tile index itself, so that little stays live in
-// registers across the node step
-struct CurSlot {
+// A warp's current domain, in shared memory (one per warp): everything the
+// tile loop needs besides the tile index, so that little stays live in
+// registers across the node step.
+struct WarpSlot {
   SlotMeta m;
-  long long begin, end;  // the domain's tiles [begin, end) in the group list
-  long long ntiles;      // tiles of the group
-  int s;                 // slot index in the group, -1 before the first
-  int ok;                // the domain takes step j
-  int image;             // argument image in img[], -1 = none
-  int fetch;             // image to copy into img[] on entry, -1 = none
+  unsigned begin, end;  // the domain's tiles [begin, end) in the group list
+  int s;                // slot index in the group
+  int ok;               // the domain takes step j
+  int image;            // argument image held in the warp's img[], -1 = none
+  int pad;
 };
 
-// the nodes of local tile lt of the current domain
-template <class S, int COLL, bool LES, bool AA>
-__device__ __forceinline__ void batch_tile(const StepArgs<S>& a, const CurSlot& cur,
-                                           unsigned lt, int npt, int j) {
-  const unsigned base = lt * (unsigned)(blockDim.x * npt);
-  for (int i = 0; i < npt; ++i) {
-    const unsigned n = base + (unsigned)i * blockDim.x + threadIdx.x;
-    if (n >= (unsigned)cur.m.nodes) break;
-    const unsigned r = fastdiv(n, cur.m.mnx);
-    const int x = (int)(n - r * (unsigned)cur.m.nx);
-    const unsigned y = fastdiv(r, cur.m.mnz);
-    const int z = (int)(r - y * (unsigned)cur.m.nz);
-    if constexpr (AA)
-      aa_step_node<S, COLL, LES>(a, x, (int)y, z, a.aa_step - 1,
-                                 j == 0 ? cur.m.entry0 : kAAPending);
-    else
-      step_node<S, COLL, LES>(a, x, (int)y, z);
-  }
-}
+constexpr int kMaxWarps = 8;  // 256-thread CTAs at most
 
-// Make the slot holding tile t (at or after the current one) the CTA's
-// current domain: meta, tile range and, when it takes step j, its argument
-// image for launch j.  All threads of the CTA take the same path.
-__device__ __forceinline__ void enter_slot(CurSlot& cur, unsigned char* img,
-                                           const BatchTables* __restrict__ tab, int g, long long t,
+// Make the slot holding tile t (at or after the warp's current one) the
+// warp's current domain: meta, tile range and, when it takes step j, its
+// argument image for launch j, copied into the warp's own image.  Every
+// lane of the warp takes the same path; no other warp is involved.
+__device__ __forceinline__ void warp_enter(WarpSlot& cur, unsigned char* img,
+                                           const BatchTables* __restrict__ tab, int g, unsigned t,
                                            int j) {
-  __syncthreads();  // every thread is done with the previous domain
-  if (threadIdx.x == 0) {
+  const unsigned lane = threadIdx.x & 31u;
+  __syncwarp();  // every lane is done with the previous domain's image
+  int fetch = -1;
+  if (lane == 0) {
     const GroupList& L = tab->v[g];
     const long long* off = tab->tile_off + L.off0;
-    int lo = cur.s < 0 ? 0 : cur.s, hi = L.nslots;  // off[lo] <= t < off[hi]
-    while (hi - lo > 1) {
-      const int mid = (lo + hi) >> 1;
-      if (off[mid] <= t)
-        lo = mid;
-      else
-        hi = mid;
+    int lo = cur.s, hi = L.nslots;  // off[lo] <= t < off[hi]
+    if (off[lo + 1] > (long long)t) {
+      hi = lo + 1;
+    } else {
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (off[mid] <= (long long)t)
+          lo = mid;
+        else
+          hi = mid;
+      }
     }
     const SlotMeta m = tab->meta[L.slot0 + lo];
     cur.m = m;
     cur.s = lo;
-    cur.begin = off[lo];
-    cur.end = off[lo + 1];
+    cur.begin = (unsigned)off[lo];
+    cur.end = (unsigned)off[lo + 1];
     cur.ok = j < m.active;
     const int image = m.image_base + ((m.cur0 + j) & 1) * 3 +
                       (j >= m.active - 1 ? 2 : (j >= m.active - 2 ? 1 : 0));
-    cur.fetch = cur.ok && image != cur.image ? image : -1;
+    fetch = cur.ok && image != cur.image ? image : -1;
     if (cur.ok) cur.image = image;
   }
-  __syncthreads();
-  const int fetch = cur.fetch;
+  fetch = __shfl_sync(0xffffffffu, fetch, 0);
   if (fetch >= 0) {
     const int4* src = reinterpret_cast<const int4*>(tab->images + (size_t)fetch * kArgsBytes);
     int4* dst = reinterpret_cast<int4*>(img);
-    for (int i = threadIdx.x; i < kArgsBytes / 16; i += blockDim.x) dst[i] = src[i];
-    __syncthreads();
+    for (unsigned i = lane; i < kArgsBytes / 16; i += 32) dst[i] = src[i];
   }
+  __syncwarp();
 }
 
 // One time step (launch j of a chunk) of every active domain of launch
-// group g (one variant).  Schedule 0 gives CTA c the
-// contiguous tiles [c*per, (c+1)*per) of the group's list; schedule 1 walks
-// t = blockIdx.x, += gridDim.x.  Either way the CTA moves forward through the
-// domains and reloads a domain's arguments only when it enters it.  The
-// domain's arguments and meta stay in shared memory (uniform over the CTA).
+// group g (one variant).  The unit of work is a warp tile: 32 x npt
+// consecutive items of one domain (row-major, rows may wrap): nodes, or for
+// members in paired rows (MODE kModePaired) the words of node pairs.  Each warp
+// walks its own tiles: schedule 0, the contiguous range [w*per, (w+1)*per)
+// of the group's list; schedule 1, t = w, += (warps in the grid).  A warp
+// enters a domain (meta and argument image into its own shared memory)
+// only when its next tile lies in another one, without waiting for the
+// other warps of its CTA; the node step reads the arguments from there.
+// Tile indices are 32-bit (the host keeps a group below 2^31 tiles).
 // MINB (resident 256-thread CTAs the register budget must allow: 4 -> 64
 // registers, 3 -> 80) trades occupancy against spills; the autotuner picks.
-template <class S, int COLL, bool LES, int MINB, bool AA>
+template <class S, int COLL, bool LES, int MINB, int MODE>
 __global__ void __launch_bounds__(256, MINB) k_batch_step(const BatchTables* __restrict__ tab,
                                                           int g, int j, int npt) {
-  __shared__ __align__(16) unsigned char img[kArgsBytes];
-  __shared__ CurSlot cur;
-  const StepArgs<S>& a = *reinterpret_cast<const StepArgs<S>*>(img);
-  if (threadIdx.x == 0) {
-    cur.s = -1;
-    cur.image = -1;
-    cur.end = 0;
-    cur.ntiles = tab->v[g].ntiles;
-  }
-  __syncthreads();
+  __shared__ __align__(16) unsigned char img[kMaxWarps][kArgsBytes];
+  __shared__ WarpSlot slots[kMaxWarps];
+  const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const StepArgs<S>& a = *reinterpret_cast<const StepArgs<S>*>(img[warp]);
+  WarpSlot& cur = slots[warp];
+  const unsigned ntiles = (unsigned)tab->v[g].ntiles;
+  const unsigned nw = gridDim.x * (blockDim.x >> 5);
+  const unsigned w = blockIdx.x * (blockDim.x >> 5) + warp;
+  unsigned t, tend, stride;
   if (tab->schedule == 0) {
-    const long long per = (cur.ntiles + gridDim.x - 1) / gridDim.x;
-    const long long t0 = (long long)blockIdx.x * per;
-    for (long long t = t0; t < min(t0 + per, cur.ntiles); ++t) {
-      if (t >= cur.end) enter_slot(cur, img, tab, g, t, j);
-      if (!cur.ok) {
-        t = cur.end - 1;
-        continue;
-      }
-      batch_tile<S, COLL, LES, AA>(a, cur, (unsigned)(t - cur.begin), npt, j);
-    }
+    const unsigned per = (ntiles + nw - 1) / nw;
+    t = w * per;
+    tend = min(t + per, ntiles);
+    stride = 1;
   } else {
-    for (long long t = blockIdx.x; t < cur.ntiles; t += gridDim.x) {
-      if (t >= cur.end) enter_slot(cur, img, tab, g, t, j);
-      if (!cur.ok) continue;
-      batch_tile<S, COLL, LES, AA>(a, cur, (unsigned)(t - cur.begin), npt, j);
+    t = w;
+    tend = ntiles;
+    stride = nw;
+  }
+  if (lane == 0) {
+    cur.s = 0;
+    cur.image = -1;
+    cur.begin = 0;
+    cur.end = 0;
+    cur.ok = 0;
+  }
+  __syncwarp();
+  const unsigned span = 32u * (unsigned)npt;
+  for (; t < tend; t += stride) {
+    if (t >= cur.end) warp_enter(cur, img[warp], tab, g, t, j);
+    if (!cur.ok) {
+      if (stride == 1) t = cur.end - 1;  // skip the domain
+      continue;
+    }
+    const unsigned n0 = (t - cur.begin) * span;
+    const unsigned nend = min(n0 + span, (unsigned)cur.m.nodes);
+    for (unsigned n = n0 + lane; n < nend; n += 32u) {
+      const unsigned r = fastdiv(n, cur.m.mnx);
+      const int x = (int)(n - r * (unsigned)cur.m.nx);
+      const unsigned y = fastdiv(r, cur.m.mnz);
+      const int z = (int)(r - y * (unsigned)cur.m.nz);
+      if constexpr (MODE == kModeAA)
+        aa_step_node<S, COLL, LES>(a, x, (int)y, z, a.aa_step - 1,
+                                   j == 0 ? cur.m.entry0 : kAAPending);
+      else if constexpr (MODE == kModePaired)
+        paired_word<S, COLL, LES, false>(a, x, (int)y, z);  // x: the word
+      else
+        step_node<S, COLL, LES>(a, x, (int)y, z);
     }
   }
 }
 
-// kernel of (model, register build, streaming): k[model][regs][aa];
-// regs 0 -> the 64-register build, 1 -> the 80-register build
+// kernel of (model, register build, mode): k[model][regs][mode];
+// regs 0 -> the 64-register build, 1 -> the 80-register build; the paired
+// mode exists for the 16-bit formats only (nullptr for FP32)
 using BatchKernel = void (*)(const BatchTables*, int, int, int);
 struct BatchKernels {
-  BatchKernel k[4][2][2];
+  BatchKernel k[4][2][kModes];
 };
 
-template <class S, int MINB, bool AA>
+template <class S, int MINB, int MODE>
 constexpr BatchKernel batch_kernel_of(int model) {
-  return model == 0   ? k_batch_step<S, COLL_SRT, false, MINB, AA>
-         : model == 1 ? k_batch_step<S, COLL_SRT, true, MINB, AA>
-         : model == 2 ? k_batch_step<S, COLL_MRT, false, MINB, AA>
-                      : k_batch_step<S, COLL_MRT, true, MINB, AA>;
+  return model == 0   ? k_batch_step<S, COLL_SRT, false, MINB, MODE>
+         : model == 1 ? k_batch_step<S, COLL_SRT, true, MINB, MODE>
+         : model == 2 ? k_batch_step<S, COLL_MRT, false, MINB, MODE>
+                      : k_batch_step<S, COLL_MRT, true, MINB, MODE>;
 }
 
 template <class S>
 BatchKernels make_batch_kernels() {
   BatchKernels t;
   for (int m = 0; m < 4; ++m) {
-    t.k[m][0][0] = batch_kernel_of<S, 4, false>(m);
-    t.k[m][1][0] = batch_kernel_of<S, 3, false>(m);
-    t.k[m][0][1] = batch_kernel_of<S, 4, true>(m);
-    t.k[m][1][1] = batch_kernel_of<S, 3, true>(m);
+    t.k[m][0][kModePull] = batch_kernel_of<S, 4, kModePull>(m);
+    t.k[m][1][kModePull] = batch_kernel_of<S, 3, kModePull>(m);
+    t.k[m][0][kModeAA] = batch_kernel_of<S, 4, kModeAA>(m);
+    t.k[m][1][kModeAA] = batch_kernel_of<S, 3, kModeAA>(m);
+    if constexpr (kDev<S>) {
+      t.k[m][0][kModePaired] = batch_kernel_of<S, 4, kModePaired>(m);
+      t.k[m][1][kModePaired] = batch_kernel_of<S, 3, kModePaired>(m);
+    } else {
+      t.k[m][0][kModePaired] = t.k[m][1][kModePaired] = nullptr;
+    }
   }
   return t;
 }

@@ -815,7 +815,14 @@ __device__ __forceinline__ void aa_neighbor_xface_node(const StepArgs<S>& a, int
 // a.src = a.dst = the lattice.
 enum { kAAPending = 0, kAAFromInit = 1, kAAComplete = 2 };
 
-template <class S, int COLL, bool LES>
+//
+// warp_row: the caller maps the lanes of a warp to the x-consecutive nodes
+// x - lane .. x - lane + 31 of one row (the single-domain kernel), so that
+// "this warp holds an x face" is known to every lane without a vote and a
+// warp of an interior row that holds one takes the x-face form as a whole.
+// Otherwise (the batched kernel, whose warps may span rows) each lane
+// decides for itself.
+template <class S, int COLL, bool LES, bool WARP_ROW = false>
 __device__ __forceinline__ void aa_step_node(const StepArgs<S>& a, int x, int y, int z,
                                              int neighbor, int entry) {
   using R = RealOf<S>;
@@ -823,10 +830,13 @@ __device__ __forceinline__ void aa_step_node(const StepArgs<S>& a, int x, int y,
   const bool face_row = (y == 0) | (y == a.g.ny - 1) | (z == 0) | (z == a.g.nz - 1);
   const bool xface = (x == 0) | (x == a.g.nx - 1);
   const bool edge = face_row | xface;
+  bool xsel = xface;
+  if constexpr (WARP_ROW) {
+    const int x0 = x - (int)(threadIdx.x & 31u);  // the warp's first node
+    xsel = x0 == 0 || (unsigned)(a.g.nx - 1 - x0) < 32u;
+  }
   R f[Q];
-  if (neighbor && !face_row && __any_sync(__activemask(), xface)) {
-    // a warp holding an x face of interior rows: every lane takes the
-    // x-face form (no divergence into the per-node face path)
+  if (neighbor && !face_row && xsel) {
     aa_neighbor_xface_node<S, COLL, LES>(a, x, y, z, cell);
     return;
   }
@@ -898,7 +908,7 @@ __global__ void __launch_bounds__(128, NB ? 8 : 9)
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int z = blockIdx.y, y = blockIdx.z;
   if (x >= a.g.nx) return;
-  aa_step_node<S, COLL, LES>(a, x, y, z, NB, entry);
+  aa_step_node<S, COLL, LES, true>(a, x, y, z, NB, entry);
 }
 
 // rho and u of arF in the current AA layout, written through a.den_out /
@@ -1179,15 +1189,12 @@ __host__ __device__ __forceinline__ bool paired_kernel_applies(const Geometry& g
 #ifndef LBM_PAIRED_SR_THREADS_PER_SM
 #define LBM_PAIRED_SR_THREADS_PER_SM 768
 #endif
+// One word w (0 <= w < px/2) of row (y, z): the step of its two nodes
+// (shared by the single-domain and batched kernels).
 template <class S, int COLL, bool LES, bool SR>
-__global__ void __launch_bounds__(128, (SR ? LBM_PAIRED_SR_THREADS_PER_SM
-                                           : LBM_PAIRED_THREADS_PER_SM) / 128)
-    k_step_paired(const __grid_constant__ StepArgs<S> a) {
+__device__ __forceinline__ void paired_word(const StepArgs<S>& a, int w, int y, int z) {
   static_assert(kDev<S>, "paired rows are a 16-bit layout");
   const int H = a.g.px >> 1;
-  const int w = (int)(blockIdx.x * blockDim.x + threadIdx.x);
-  const int z = blockIdx.y, y = blockIdx.z;
-  if (w >= H) return;
   const int xh = w + H;                             // node of the hi lane
   const int e = 2 * w + a.g.px * (z + a.g.nz * y);  // the pair's word (lo slot)
   const bool face_row = y == 0 || y == a.g.ny - 1 || z == 0 || z == a.g.nz - 1;
@@ -1269,6 +1276,16 @@ __global__ void __launch_bounds__(128, (SR ? LBM_PAIRED_SR_THREADS_PER_SM
       *reinterpret_cast<uint32_t*>(a.dstq[q] + e) = pack_pair_sr<S>(v, a.scale, sr_bits<q>(h));
     });
   }
+}
+
+template <class S, int COLL, bool LES, bool SR>
+__global__ void __launch_bounds__(128, (SR ? LBM_PAIRED_SR_THREADS_PER_SM
+                                           : LBM_PAIRED_THREADS_PER_SM) / 128)
+    k_step_paired(const __grid_constant__ StepArgs<S> a) {
+  const int w = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int z = blockIdx.y, y = blockIdx.z;
+  if (w >= (a.g.px >> 1)) return;
+  paired_word<S, COLL, LES, SR>(a, w, y, z);
 }
 
 // Paired domains the paired kernel does not apply to (STRUCT nodes, nx <

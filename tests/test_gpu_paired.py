@@ -231,3 +231,37 @@ def test_stochastic_rounding_rejected_where_not_built():
         b.add(iv, pkg.default_options(storage=pkg.STORE_F16_SHIFT,
                                       rounding=pkg.ROUND_STOCHASTIC), 4)
     b.close()
+
+
+@pytest.mark.parametrize("storage", STORES)
+@pytest.mark.parametrize("shape", [(0, 0, 256, 2), (1, 1, 128, 1), (0, 1, 128, 16),
+                                   (1, 0, 256, 3)])
+def test_batch_members_in_paired_rows_match_alone(storage, shape):
+    """16-bit A/B batch members keep the paired rows (the batched kernel
+    steps their words), except where the paired step does not apply (tiny
+    rows: plain rows); a mix of both, of both collision models and of the
+    channel, against each domain alone, over warp tiles that wrap rows."""
+    sched, regs, block, npt = shape
+    cases = [(cavity(64, 20, 18), pkg.INIT_DENSITY_NOISE, 1e-4),
+             (cavity(9, 8, 7), pkg.INIT_DENSITY_NOISE, 1e-4),
+             (cavity(130, 9, 11, mrt=False, les=False), pkg.INIT_DENSITY_NOISE, 1e-4),
+             (channel(48, 12, 14), pkg.INIT_CHANNEL, 0.01),
+             (cavity(41, 10, 7, mrt=True, les=False), pkg.INIT_DENSITY_NOISE, 1e-4)]
+    kerns = [pkg.KERNEL_AUTO, pkg.KERNEL_AUTO, pkg.KERNEL_PAIRED, pkg.KERNEL_AUTO,
+             pkg.KERNEL_SCALAR]
+    want = []
+    for (iv, kind, amp), k in zip(cases, kerns):
+        d = pkg.Domain(iv, opts(storage, k, kind, amp))
+        d.run(45)
+        want.append((d.export_arF(), d.macroscopic()))
+        d.close()
+    b = pkg.Batch(hbm_budget=256 << 20, chunk_steps=16, schedule=sched, regs=regs, block=block,
+                  nodes_per_thread=npt)
+    ids = [b.add(iv, opts(storage, k, kind, amp), 45)
+           for (iv, kind, amp), k in zip(cases, kerns)]
+    b.step(45)
+    b.sync()
+    for i, w in zip(ids, want):
+        m = b.member(i)
+        assert_same((m.export_arF(), m.macroscopic()), w)
+    b.close()
