@@ -579,7 +579,7 @@ def main():
     ap.add_argument("--c5-window", type=float, default=20.0,
                     help="wall-clock window of the serving run the default run reports")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="serving: HBM budget")
-    ap.add_argument("--horizon", type=float, default=0.0,
+    ap.add_argument("--horizon", type=float, default=2.0,
                     help="serving: admit while the resident backlog is below this many seconds "
                          "of work at --nominal-mlups (0 = HBM budget only)")
     ap.add_argument("--nominal-mlups", type=float, default=30000.0,
@@ -744,7 +744,7 @@ def main():
             line["precision_c3"] = precision_c3(pkg, args.c3_steps, pkg.KERNEL_AUTO)
             line["batch_c4"] = batch_c4(pkg, 256, args.c4_steps, 4)
             line["serving_c5"] = serving_c5(pkg, 200.0, args.c5_window, 150.0, "shortest",
-                                            0.0, "ab")
+                                            0.0, "ab", args.horizon, args.nominal_mlups)
     else:
         dom.close()
 

@@ -487,8 +487,12 @@ typedef struct lbm_batch_options {
   int block;              /* threads per CTA (128 or 256), 0 = autotuned/256  */
   int nodes_per_thread;   /* nodes per lane per warp tile (1..16), 0 = 2      */
   int ctas_per_sm;        /* persistent CTAs per SM, 0 = max resident         */
-  int schedule;           /* 0: each warp a contiguous range of tiles,
-                             1: warp-stride over the tile list                */
+  int schedule;           /* persistent kernel over warp tiles: 0 each warp a
+                             contiguous range, 1 warp-stride; 2: flat grids,
+                             members packed into sets whose arguments travel
+                             as kernel parameters, one launch chain per set
+                             in the chunk graph (block, nodes_per_thread,
+                             ctas_per_sm and regs do not apply); default 2   */
   int regs;               /* kernel build: 0 = 64 registers, 1 = 80           */
   int reserved[6];
 } lbm_batch_options;

@@ -445,7 +445,7 @@ class Batch:
     """Many resident domains stepped together (continuous batching)."""
 
     def __init__(self, hbm_budget=1 << 30, device=0, chunk_steps=32, block=0,
-                 nodes_per_thread=0, ctas_per_sm=0, schedule=0, regs=0):
+                 nodes_per_thread=0, ctas_per_sm=0, schedule=2, regs=0):
         o = BatchOptions()
         lib().lbm_batch_default_options(C.byref(o))
         o.device, o.hbm_budget, o.chunk_steps = device, hbm_budget, chunk_steps

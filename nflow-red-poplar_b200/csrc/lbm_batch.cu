@@ -22,6 +22,7 @@
 // membership changes; only the tables are re-uploaded before each chunk.
 #include <algorithm>
 #include <map>
+#include <memory>
 #include <vector>
 
 #include "lbm_batch_kernel.cuh"
@@ -148,6 +149,7 @@ struct lbm_batch {
   // completion tracking
   long long chunks_issued = 0;
   std::vector<std::pair<long long, cudaEvent_t>> chunk_events;
+  std::vector<std::pair<long long, cudaGraphExec_t>> flat_execs;  // schedule 2, per chunk
   long long chunks_completed = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   long long last_lups = 0;
@@ -317,11 +319,181 @@ void retire_completed(lbm_batch* b) {
     cudaEventDestroy(ce.second);
     b->chunk_events.erase(b->chunk_events.begin());
   }
+  while (!b->flat_execs.empty() && b->flat_execs.front().first <= b->chunks_completed) {
+    cudaGraphExecDestroy(b->flat_execs.front().second);
+    b->flat_execs.erase(b->flat_execs.begin());
+  }
+}
+
+// After a chunk's launches: rho, u of the AA members, the completion event.
+int finish_chunk(lbm_batch* b) {
+  // AA members: rho, u of the state the chunk ends in (a single-domain AA
+  // run ends the same way), before the chunk's completion event
+  int rc;
+  for (auto& kv : b->members) {
+    lbm_domain* d = kv.second.d;
+    if (d->opt.stream_mode == LBM_STREAM_AA && kv.second.last_active > 0 &&
+        (rc = storage_ops(d->opt.storage).aa_macro(d)))
+      return rc;
+  }
+  ++b->chunks_issued;
+  cudaEvent_t ev;
+  CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  CK(cudaEventRecord(ev, b->stream));
+  b->chunk_events.push_back({b->chunks_issued, ev});
+  return LBM_OK;
+}
+
+// Schedule 2.  A member of at least kOwnSetCtas CTAs (of 128 items) is a set
+// of its own; the others are packed, per variant and in admission order,
+// into sets of at most kFlatMax members and kSetCtas CTAs.  Each set is a
+// chain of chunk_steps launches in a graph built for this chunk, with no
+// edge between the chains.  Launch j of a set steps the members that take
+// step j, with the argument image of their parity and output kind at that
+// step: k_batch_flat, or the member's single-domain kernel when one member
+// takes the step.
+constexpr unsigned kOwnSetCtas = 8192;
+constexpr unsigned kSetCtas = 16384;
+
+int issue_chunk_flat(lbm_batch* b, int steps_offered, long long* lups) {
+  const int S = chunk_steps(b);
+  *lups = 0;
+  const std::vector<int> groups = pending_groups(b);
+  if (groups.empty()) return LBM_OK;
+  struct Item {
+    lbm_batch::Member* m;
+    int active, cur0, entry0, row_items;
+    unsigned ctas;
+  };
+  long long updates = 0;
+  for (auto& kv : b->members) kv.second.last_active = 0;
+  std::vector<std::vector<Item>> sets;
+  std::vector<int> set_variant;
+  for (int v : groups) {
+    std::vector<Item> cur;
+    unsigned cur_ctas = 0;
+    for (auto& kv : b->members) {
+      lbm_batch::Member& m = kv.second;
+      lbm_domain* d = m.d;
+      const long long left = m.target - m.issued;
+      if (left <= 0 || member_variant(d) != v) continue;
+      Item it;
+      it.m = &m;
+      it.active = (int)std::min<long long>(std::min(S, steps_offered), left);
+      it.cur0 = d->cur;
+      it.entry0 = d->aa_first ? kAAFromInit : (d->post_direct ? kAAComplete : kAAPending);
+      it.row_items = d->g.paired ? d->g.px / 2 : d->g.nx;
+      const long long items = (long long)it.row_items * d->g.nz * d->g.ny;
+      it.ctas = (unsigned)((items + kFlatBlock - 1) / kFlatBlock);
+      if (it.ctas >= kOwnSetCtas) {
+        sets.push_back({it});  // a large member: a set of its own
+        set_variant.push_back(v);
+      } else {
+        if (!cur.empty() && ((int)cur.size() == kFlatMax || cur_ctas + it.ctas > kSetCtas)) {
+          sets.push_back(std::move(cur));
+          set_variant.push_back(v);
+          cur.clear();
+          cur_ctas = 0;
+        }
+        cur.push_back(it);
+        cur_ctas += it.ctas;
+      }
+      updates += d->N * it.active;
+      // host bookkeeping of the steps this chunk takes
+      d->step += it.active;
+      d->cur ^= (it.active & 1);
+      d->post_direct = false;
+      d->aa_first = false;
+      m.issued += it.active;
+      m.last_active = it.active;
+      if (m.issued >= m.target) m.done_chunk = b->chunks_issued + 1;
+    }
+    if (!cur.empty()) {
+      sets.push_back(std::move(cur));
+      set_variant.push_back(v);
+    }
+  }
+  cudaGraph_t gr = nullptr;
+  CK(cudaGraphCreate(&gr, 0));
+  std::unique_ptr<FlatSet<float>> fs(new FlatSet<float>());
+  cudaError_t e = cudaSuccess;
+  for (size_t k = 0; k < sets.size() && e == cudaSuccess; ++k) {
+    const int v = set_variant[k];
+    const int mode = v % kModes, model = (v / kModes) % 4, st = v / (4 * kModes);
+    const BatchKernels& t = st == 0 ? kBatch_f32 : (st == 1 ? kBatch_f16 : kBatch_bf16);
+    cudaGraphNode_t prev = nullptr;
+    for (int j = 0; j < S && e == cudaSuccess; ++j) {
+      FlatSet<float>& p = *fs;
+      p.n = 0;
+      p.cta_off[0] = 0;
+      const Item* only = nullptr;  // the member, when one takes step j
+      for (const Item& it : sets[k]) {
+        if (j >= it.active) continue;
+        only = &it;
+        const lbm_domain* d = it.m->d;
+        const int kind = j >= it.active - 1 ? 2 : (j >= it.active - 2 ? 1 : 0);
+        const int image = ((it.cur0 + j) & 1) * 3 + kind;
+        std::memcpy(&p.args[p.n],
+                    b->h_images + ((size_t)it.m->image_slot * kImages + image) * kArgsBytes,
+                    sizeof(StepArgs<float>));
+        FlatMeta& fm = p.meta[p.n];
+        fm.nx = it.row_items;
+        fm.nz = d->g.nz;
+        fm.items = (unsigned)((long long)it.row_items * d->g.nz * d->g.ny);
+        fm.entry = j == 0 ? it.entry0 : kAAPending;
+        fm.mnx = ~0ull / (unsigned long long)it.row_items + 1;
+        fm.mnz = ~0ull / (unsigned long long)d->g.nz + 1;
+        p.cta_off[p.n + 1] = p.cta_off[p.n] + it.ctas;
+        ++p.n;
+      }
+      if (p.n == 0) break;  // members only leave a set as j grows
+      cudaKernelNodeParams kp;
+      std::memset(&kp, 0, sizeof(kp));
+      int entry = p.meta[0].entry;
+      void* args[] = {fs.get(), &entry};
+      kp.kernelParams = args;
+      if (p.n == 1) {
+        // one member: its single-domain kernel, launched as alone
+        const lbm_domain* d = only->m->d;
+        const int nb = mode == kModeAA ? p.args[0].aa_step - 1 : 0;
+        kp.func = const_cast<void*>(t.single[model][mode][nb]);
+        kp.blockDim = block_of(mode == kModePaired ? d->g.px / 2 : d->g.nx);
+        kp.gridDim = dim3(((mode == kModePaired ? d->g.px / 2 : d->g.nx) + kp.blockDim.x - 1) /
+                              kp.blockDim.x,
+                          d->g.nz, d->g.ny);
+        args[0] = &p.args[0];
+      } else {
+        kp.func = const_cast<void*>(t.flat[model][mode]);
+        kp.gridDim = dim3(p.cta_off[p.n]);
+        kp.blockDim = dim3(kFlatBlock);
+      }
+      cudaGraphNode_t node;
+      e = cudaGraphAddKernelNode(&node, gr, prev ? &prev : nullptr, prev ? 1 : 0, &kp);
+      prev = node;
+    }
+  }
+  cudaGraphExec_t ex = nullptr;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&ex, gr, 0);
+  cudaGraphDestroy(gr);
+  if (e != cudaSuccess)
+    return set_error(LBM_ERR_CUDA, "flat chunk graph: %s", cudaGetErrorString(e));
+  e = cudaGraphLaunch(ex, b->stream);
+  if (e != cudaSuccess) {
+    cudaGraphExecDestroy(ex);
+    return set_error(LBM_ERR_CUDA, "flat chunk launch: %s", cudaGetErrorString(e));
+  }
+  // released once the chunk is complete (retire_completed)
+  b->flat_execs.push_back({b->chunks_issued + 1, ex});
+  int rc = finish_chunk(b);
+  if (rc) return rc;
+  *lups = updates;
+  return LBM_OK;
 }
 
 // Build and upload the tables of one chunk and launch its graph; returns
 // the lattice updates.  Slots are grouped by variant.
 int issue_chunk(lbm_batch* b, int steps_offered, long long* lups) {
+  if (b->opt.schedule == 2) return issue_chunk_flat(b, steps_offered, lups);
   const int S = chunk_steps(b);
   *lups = 0;
   const std::vector<int> groups = pending_groups(b);
@@ -387,19 +559,7 @@ int issue_chunk(lbm_batch* b, int steps_offered, long long* lups) {
   CK(cudaMemcpyAsync(b->d_tab, b->h_tab, sizeof(BatchTables), cudaMemcpyHostToDevice, b->stream));
   CK(cudaEventRecord(b->tables_free, b->stream));
   CK(cudaGraphLaunch(b->graph, b->stream));
-  // AA members: rho, u of the state the chunk ends in (a single-domain AA
-  // run ends the same way), before the chunk's completion event
-  for (auto& kv : b->members) {
-    lbm_domain* d = kv.second.d;
-    if (d->opt.stream_mode == LBM_STREAM_AA && kv.second.last_active > 0 &&
-        (rc = storage_ops(d->opt.storage).aa_macro(d)))
-      return rc;
-  }
-  ++b->chunks_issued;
-  cudaEvent_t ev;
-  CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-  CK(cudaEventRecord(ev, b->stream));
-  b->chunk_events.push_back({b->chunks_issued, ev});
+  if ((rc = finish_chunk(b))) return rc;
   *lups = updates;
   return LBM_OK;
 }
@@ -437,6 +597,7 @@ void lbm_batch_default_options(lbm_batch_options* bo) {
   bo->chunk_steps = 32;
   bo->block = 256;
   bo->nodes_per_thread = 2;
+  bo->schedule = 2;  // flat grids: the fastest schedule on the mixes measured
 }
 
 int lbm_batch_domain_bytes(const Inputval* pinput, const lbm_options* opt, size_t* bytes) {
@@ -461,7 +622,8 @@ int lbm_batch_create(const lbm_batch_options* bo, lbm_batch** out) {
     return set_error(LBM_ERR_INVALID, "block must be 128 or 256");
   if (o.nodes_per_thread < 0 || o.nodes_per_thread > 16)
     return set_error(LBM_ERR_INVALID, "nodes_per_thread must be 1..16");
-  if (o.schedule < 0 || o.schedule > 1) return set_error(LBM_ERR_INVALID, "schedule must be 0 or 1");
+  if (o.schedule < 0 || o.schedule > 2)
+    return set_error(LBM_ERR_INVALID, "schedule must be 0, 1 or 2");
   if (o.regs < 0 || o.regs > 1) return set_error(LBM_ERR_INVALID, "regs must be 0 or 1");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
@@ -509,6 +671,7 @@ int lbm_batch_destroy(lbm_batch* b) {
   for (auto& kv : b->members) destroy_member(b, kv.second);
   b->members.clear();
   for (auto& ce : b->chunk_events) cudaEventDestroy(ce.second);
+  for (auto& fe : b->flat_execs) cudaGraphExecDestroy(fe.second);
   if (b->graph) cudaGraphExecDestroy(b->graph);
   if (b->d_images) cudaFree(b->d_images);
   if (b->h_images) cudaFreeHost(b->h_images);
@@ -728,7 +891,8 @@ int lbm_batch_autotune(lbm_batch* b, int trial_steps, lbm_batch_options* chosen)
   if (!b) return set_error(LBM_ERR_INVALID, "NULL batch");
   if (trial_steps <= 0) return set_error(LBM_ERR_INVALID, "trial_steps must be positive");
   // coordinate search: register build x schedule x block at 2 nodes per
-  // thread, then nodes per thread, then a cap of 2 CTAs per SM
+  // thread and the flat grids, then (persistent schedules) nodes per thread,
+  // then a cap of 2 CTAs per SM
   lbm_batch_options keep = b->opt, best_opt = b->opt;
   float best = 1e30f;
   bool done = false;
@@ -762,7 +926,17 @@ int lbm_batch_autotune(lbm_batch* b, int trial_steps, lbm_batch_options* chosen)
         o.ctas_per_sm = 0;
         stage.push_back(o);
       }
+  {
+    lbm_batch_options o = keep;  // flat grids (launch shape fixed)
+    o.schedule = 2;
+    o.block = 128;
+    o.nodes_per_thread = 2;
+    o.regs = 0;
+    o.ctas_per_sm = 0;
+    stage.push_back(o);
+  }
   for (int phase = 0; phase < 3 && !done; ++phase) {
+    if (phase > 0 && best_opt.schedule == 2) break;  // nothing further to tune
     if (phase == 1) {
       stage.clear();
       for (int np : {1, 4, 8, 16}) {

@@ -186,12 +186,75 @@ __global__ void __launch_bounds__(256, MINB) k_batch_step(const BatchTables* __r
   }
 }
 
+// ------------------------------------------------------------------ //
+// Schedule 2: flat grids with the arguments in the kernel parameter space.
+// A launch steps one set of at most kFlatMax members of one variant by one
+// time step: one CTA per 128 consecutive items (nodes, or words of paired
+// rows) of a member, the member found by a loop over the set's CTA offsets
+// that depends on blockIdx and parameters only, so it is the same for every
+// thread, and the member's arguments read from the parameter space like
+// those of a single-domain kernel.  Each set is a chain of launches in the
+// chunk graph, independent of the other sets, so the sets' launches overlap
+// on the GPU and fill each other's tails.  A set of one member launches the
+// member's single-domain step kernel instead (its arguments are kernel
+// parameters there as well).
+// ------------------------------------------------------------------ //
+constexpr int kFlatMax = 32;
+constexpr int kFlatBlock = 128;
+
+struct FlatMeta {
+  int nx, nz;        // items per row, rows per plane
+  unsigned items;    // items of the member
+  int entry;         // AA: entry mode of this step (k_aa_step)
+  unsigned long long mnx, mnz;
+};
+
+template <class S>
+struct FlatSet {
+  int n;                           // members of the set taking this step
+  int pad[3];
+  unsigned cta_off[kFlatMax + 1];  // CTAs of members [0, k): cta_off[k]
+  FlatMeta meta[kFlatMax];
+  StepArgs<S> args[kFlatMax];
+};
+static_assert(sizeof(FlatSet<float>) <= 32000, "kernel parameters are limited to 32 KB");
+static_assert(sizeof(FlatSet<__half>) == sizeof(FlatSet<float>) &&
+                  sizeof(FlatSet<__nv_bfloat16>) == sizeof(FlatSet<float>) &&
+                  sizeof(StepArgs<__half>) == sizeof(StepArgs<float>) &&
+                  sizeof(StepArgs<__nv_bfloat16>) == sizeof(StepArgs<float>),
+              "the host fills every format's FlatSet through the FP32 layout");
+
+template <class S, int COLL, bool LES, int MODE>
+__global__ void __launch_bounds__(kFlatBlock, 8)
+    k_batch_flat(const __grid_constant__ FlatSet<S> p) {
+  int s = 0;
+  for (int k = 1; k < p.n; ++k) s += blockIdx.x >= p.cta_off[k];
+  const StepArgs<S>& a = p.args[s];
+  const FlatMeta& m = p.meta[s];
+  const unsigned n = (blockIdx.x - p.cta_off[s]) * (unsigned)kFlatBlock + threadIdx.x;
+  if (n >= m.items) return;
+  const unsigned r = fastdiv(n, m.mnx);
+  const int x = (int)(n - r * (unsigned)m.nx);
+  const unsigned y = fastdiv(r, m.mnz);
+  const int z = (int)(r - y * (unsigned)m.nz);
+  if constexpr (MODE == kModeAA)
+    aa_step_node<S, COLL, LES>(a, x, (int)y, z, a.aa_step - 1, m.entry);
+  else if constexpr (MODE == kModePaired)
+    paired_word<S, COLL, LES, false>(a, x, (int)y, z);
+  else
+    step_node<S, COLL, LES>(a, x, (int)y, z);
+}
+
 // kernel of (model, register build, mode): k[model][regs][mode];
 // regs 0 -> the 64-register build, 1 -> the 80-register build; the paired
 // mode exists for the 16-bit formats only (nullptr for FP32)
 using BatchKernel = void (*)(const BatchTables*, int, int, int);
 struct BatchKernels {
   BatchKernel k[4][2][kModes];
+  const void* flat[4][kModes];  // k_batch_flat<S, ...>: the FlatSet<S> of the format
+  // the single-domain step kernels (a set of one member, schedule 2):
+  // [model][mode][NB], NB the AA step kind (k_aa_step<.., NB>), 0 otherwise
+  const void* single[4][kModes][2];
 };
 
 template <class S, int MINB, int MODE>
@@ -202,19 +265,48 @@ constexpr BatchKernel batch_kernel_of(int model) {
                       : k_batch_step<S, COLL_MRT, true, MINB, MODE>;
 }
 
+template <class S, int MODE>
+const void* flat_kernel_of(int model) {
+  return model == 0   ? (const void*)k_batch_flat<S, COLL_SRT, false, MODE>
+         : model == 1 ? (const void*)k_batch_flat<S, COLL_SRT, true, MODE>
+         : model == 2 ? (const void*)k_batch_flat<S, COLL_MRT, false, MODE>
+                      : (const void*)k_batch_flat<S, COLL_MRT, true, MODE>;
+}
+
+template <class S, int COLL, bool LES>
+void set_single(BatchKernels& t, int m) {
+  t.single[m][kModePull][0] = (const void*)k_step<S, COLL, LES, false>;
+  t.single[m][kModePull][1] = nullptr;
+  t.single[m][kModeAA][0] = (const void*)k_aa_step<S, COLL, LES, 0>;
+  t.single[m][kModeAA][1] = (const void*)k_aa_step<S, COLL, LES, 1>;
+  if constexpr (kDev<S>)
+    t.single[m][kModePaired][0] = (const void*)k_step_paired<S, COLL, LES, false>;
+  else
+    t.single[m][kModePaired][0] = nullptr;
+  t.single[m][kModePaired][1] = nullptr;
+}
+
 template <class S>
 BatchKernels make_batch_kernels() {
   BatchKernels t;
+  set_single<S, COLL_SRT, false>(t, 0);
+  set_single<S, COLL_SRT, true>(t, 1);
+  set_single<S, COLL_MRT, false>(t, 2);
+  set_single<S, COLL_MRT, true>(t, 3);
   for (int m = 0; m < 4; ++m) {
     t.k[m][0][kModePull] = batch_kernel_of<S, 4, kModePull>(m);
     t.k[m][1][kModePull] = batch_kernel_of<S, 3, kModePull>(m);
     t.k[m][0][kModeAA] = batch_kernel_of<S, 4, kModeAA>(m);
     t.k[m][1][kModeAA] = batch_kernel_of<S, 3, kModeAA>(m);
+    t.flat[m][kModePull] = flat_kernel_of<S, kModePull>(m);
+    t.flat[m][kModeAA] = flat_kernel_of<S, kModeAA>(m);
     if constexpr (kDev<S>) {
       t.k[m][0][kModePaired] = batch_kernel_of<S, 4, kModePaired>(m);
       t.k[m][1][kModePaired] = batch_kernel_of<S, 3, kModePaired>(m);
+      t.flat[m][kModePaired] = flat_kernel_of<S, kModePaired>(m);
     } else {
       t.k[m][0][kModePaired] = t.k[m][1][kModePaired] = nullptr;
+      t.flat[m][kModePaired] = nullptr;
     }
   }
   return t;

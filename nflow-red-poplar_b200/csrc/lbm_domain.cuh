@@ -295,11 +295,13 @@ template <class S, int COLL, bool LES>
 void launch_step(const lbm_domain* d, const StepArgs<S>& a, cudaStream_t st) {
   if constexpr (kDev<S>) {
     if (d->g.paired) {
-      const dim3 gr((d->g.px / 2 + 127) / 128, d->g.nz, d->g.ny);
+      // one thread per word, CTAs no wider than a row's words (px / 2)
+      const dim3 bp = block_of(d->g.px / 2);
+      const dim3 gr((d->g.px / 2 + bp.x - 1) / bp.x, d->g.nz, d->g.ny);
       if (paired_kernel_applies(d->g) && a.sr)
-        k_step_paired<S, COLL, LES, true><<<gr, dim3(128), 0, st>>>(a);
+        k_step_paired<S, COLL, LES, true><<<gr, bp, 0, st>>>(a);
       else if (paired_kernel_applies(d->g))
-        k_step_paired<S, COLL, LES, false><<<gr, dim3(128), 0, st>>>(a);
+        k_step_paired<S, COLL, LES, false><<<gr, bp, 0, st>>>(a);
       else if (a.sr)
         k_step_rows<S, COLL, LES, true><<<grid_of(d->g, block_of(d->g.nx)), block_of(d->g.nx),
                                           0, st>>>(a);

@@ -1184,8 +1184,9 @@ __host__ __device__ __forceinline__ bool paired_kernel_applies(const Geometry& g
 #define LBM_PAIRED_THREADS_PER_SM 1024
 #endif
 
-// grid = (ceil(H / 128), nz, ny), 128 threads, one word (two nodes) per
-// thread; a.srcd[q] = plane q minus the donor offset 2 c_x + px (c_z + nz c_y)
+// grid = (ceil(H / b), nz, ny), b = H rounded up to a multiple of 32 and
+// at most 128 threads, one word (two nodes) per thread; a.srcd[q] = plane q
+// minus the donor offset 2 c_x + px (c_z + nz c_y)
 #ifndef LBM_PAIRED_SR_THREADS_PER_SM
 #define LBM_PAIRED_SR_THREADS_PER_SM 768
 #endif

@@ -47,12 +47,14 @@ def alone(iv, o, steps):
     return f, m
 
 
-# launch shapes: (schedule, register build, block, nodes per thread)
-SHAPES = [(0, 0, 256, 2), (1, 1, 128, 1), (0, 1, 256, 4), (1, 0, 128, 3), (1, 0, 256, 16)]
+# launch shapes: (schedule, register build, block, nodes per thread);
+# schedule 2 (flat grids, arguments as kernel parameters) has a fixed shape
+SHAPES = [(0, 0, 256, 2), (1, 1, 128, 1), (0, 1, 256, 4), (1, 0, 128, 3), (1, 0, 256, 16),
+          (2, 0, 128, 2)]
 
 
 @pytest.mark.parametrize("shape", SHAPES, ids=["s0r0b256n2", "s1r1b128n1", "s0r1b256n4",
-                                               "s1r0b128n3", "s1r0b256n16"])
+                                               "s1r0b128n3", "s1r0b256n16", "s2flat"])
 @pytest.mark.parametrize("steps", [1, 37, 100])
 def test_batch_matches_alone_bit_for_bit(steps, shape):
     sched, regs, block, npt = shape
@@ -92,7 +94,8 @@ def aa_opts(storage, kind, amp, mode):
                                stream_mode=mode)
 
 
-@pytest.mark.parametrize("shape", SHAPES[:2], ids=["s0r0b256n2", "s1r1b128n1"])
+@pytest.mark.parametrize("shape", SHAPES[:2] + SHAPES[-1:],
+                         ids=["s0r0b256n2", "s1r1b128n1", "s2flat"])
 @pytest.mark.parametrize("steps", [1, 2, 37, 100])
 def test_batch_aa_members_match_alone(steps, shape):
     """Pull members: bit for bit.  AA members: the batched AA kernel runs the
@@ -150,8 +153,9 @@ def test_batch_aa_member_takes_one_lattice():
     assert ab - aa >= 19 * 48 ** 3 * 4
 
 
-def test_continuous_batching_targets_and_late_admission():
-    b = pkg.Batch(hbm_budget=512 << 20, chunk_steps=8)
+@pytest.mark.parametrize("schedule", [0, 2])
+def test_continuous_batching_targets_and_late_admission(schedule):
+    b = pkg.Batch(hbm_budget=512 << 20, chunk_steps=8, schedule=schedule)
     iv0, st0, k0, a0 = CASES[0]
     iv1, st1, k1, a1 = CASES[2]
     iv2, st2, k2, a2 = CASES[3]
@@ -199,6 +203,7 @@ def test_autotune_keeps_results():
     ids = [b.add(iv, opts(st, k, a), 10 ** 6) for iv, st, k, a in CASES]
     cfg = b.autotune(trial_steps=8)
     assert cfg["block"] in (128, 256) and cfg["nodes_per_thread"] in (1, 2, 4, 8, 16)
+    assert cfg["schedule"] in (0, 1, 2)
     done = b.member(ids[0]).steps()
     b.step(8)
     b.sync()
@@ -219,7 +224,7 @@ def test_batch_rejects_fp64_and_bad_options():
     with pytest.raises(pkg.LbmError):
         pkg.Batch(hbm_budget=64 << 20, chunk_steps=7)
     with pytest.raises(pkg.LbmError):
-        pkg.Batch(hbm_budget=64 << 20, schedule=2)
+        pkg.Batch(hbm_budget=64 << 20, schedule=3)
     with pytest.raises(pkg.LbmError):
         pkg.Batch(hbm_budget=64 << 20, regs=2)
 
@@ -242,4 +247,32 @@ def test_fetch_returns_a_finished_members_fields_while_others_run():
     b.step(8)
     b.sync()
     assert b.member(long_).steps() == 24 + 64 + 8
+    b.close()
+
+
+@pytest.mark.parametrize("steps", [1, 37])
+def test_schedule2_large_members_take_the_single_domain_kernels(steps):
+    """Schedule 2: a member of at least 8192 CTAs of 128 items is a set of
+    its own and steps with its single-domain kernel (pull FP32, paired
+    FP16, AA FP32), next to small members packed into one flat launch; all
+    against each domain alone."""
+    cases = [(cavity(128), pkg.STORE_F32, 1, 1e-6, pkg.STREAM_AB),
+             (cavity(128, re=500.0), pkg.STORE_F16_SHIFT, 1, 1e-6, pkg.STREAM_AB),
+             (cavity(112, mrt=False, les=False), pkg.STORE_F32, 1, 1e-6, pkg.STREAM_AA),
+             (cavity(24, 20, 18), pkg.STORE_F32, 1, 1e-6, pkg.STREAM_AB),
+             (channel(48, 12, 14), pkg.STORE_F32, pkg.INIT_CHANNEL, 0.01, pkg.STREAM_AB)]
+    b = pkg.Batch(hbm_budget=2 << 30, chunk_steps=16, schedule=2)
+    ids = []
+    for iv, st, k, a, mode in cases:
+        ids.append(b.add(iv, pkg.default_options(storage=st, init_kind=k, noise_amp=a, seed=3,
+                                                 stream_mode=mode), steps))
+    b.step(steps)
+    b.sync()
+    for i, (iv, st, k, a, mode) in zip(ids, cases):
+        o = pkg.default_options(storage=st, init_kind=k, noise_amp=a, seed=3, stream_mode=mode)
+        f_a, m_a = alone(iv, o, steps)
+        m = b.member(i)
+        np.testing.assert_array_equal(m.export_arF(), f_a)
+        for x, y in zip(m.macroscopic(), m_a):
+            np.testing.assert_array_equal(x, y)
     b.close()

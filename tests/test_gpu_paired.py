@@ -235,7 +235,7 @@ def test_stochastic_rounding_rejected_where_not_built():
 
 @pytest.mark.parametrize("storage", STORES)
 @pytest.mark.parametrize("shape", [(0, 0, 256, 2), (1, 1, 128, 1), (0, 1, 128, 16),
-                                   (1, 0, 256, 3)])
+                                   (1, 0, 256, 3), (2, 0, 128, 2)])
 def test_batch_members_in_paired_rows_match_alone(storage, shape):
     """16-bit A/B batch members keep the paired rows (the batched kernel
     steps their words), except where the paired step does not apply (tiny
