@@ -494,7 +494,11 @@ typedef struct lbm_batch_options {
                              in the chunk graph (block, nodes_per_thread,
                              ctas_per_sm and regs do not apply); default 2   */
   int regs;               /* kernel build: 0 = 64 registers, 1 = 80           */
-  int reserved[6];
+  int own_set_ctas;       /* schedule 2: a member of at least this many CTAs
+                             (of 128 nodes or paired words) is a set of its
+                             own, stepped by its single-domain kernel;
+                             0 = 2048                                          */
+  int reserved[5];
 } lbm_batch_options;
 
 void lbm_batch_default_options(lbm_batch_options* bo);

@@ -78,7 +78,8 @@ class BatchOptions(C.Structure):
     _fields_ = [
         ("device", C.c_int), ("hbm_budget", C.c_size_t), ("chunk_steps", C.c_int),
         ("block", C.c_int), ("nodes_per_thread", C.c_int), ("ctas_per_sm", C.c_int),
-        ("schedule", C.c_int), ("regs", C.c_int), ("reserved", C.c_int * 6),
+        ("schedule", C.c_int), ("regs", C.c_int), ("own_set_ctas", C.c_int),
+        ("reserved", C.c_int * 5),
     ]
 
 
@@ -445,7 +446,7 @@ class Batch:
     """Many resident domains stepped together (continuous batching)."""
 
     def __init__(self, hbm_budget=1 << 30, device=0, chunk_steps=32, block=0,
-                 nodes_per_thread=0, ctas_per_sm=0, schedule=2, regs=0):
+                 nodes_per_thread=0, ctas_per_sm=0, schedule=2, regs=0, own_set_ctas=0):
         o = BatchOptions()
         lib().lbm_batch_default_options(C.byref(o))
         o.device, o.hbm_budget, o.chunk_steps = device, hbm_budget, chunk_steps
@@ -454,7 +455,7 @@ class Batch:
         if nodes_per_thread:
             o.nodes_per_thread = nodes_per_thread
         o.ctas_per_sm = ctas_per_sm
-        o.schedule, o.regs = schedule, regs
+        o.schedule, o.regs, o.own_set_ctas = schedule, regs, own_set_ctas
         h = C.c_void_p()
         check(lib().lbm_batch_create(C.byref(o), C.byref(h)))
         self.h = h
@@ -517,7 +518,7 @@ class Batch:
         o = BatchOptions()
         check(lib().lbm_batch_autotune(self.h, int(trial_steps), C.byref(o)))
         return dict(block=o.block, nodes_per_thread=o.nodes_per_thread, ctas_per_sm=o.ctas_per_sm,
-                    schedule=o.schedule, regs=o.regs)
+                    schedule=o.schedule, regs=o.regs, own_set_ctas=o.own_set_ctas)
 
     def last_step_ms(self):
         ms, lups = C.c_float(), C.c_longlong()
