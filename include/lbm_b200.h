@@ -407,11 +407,11 @@ int lbm_save_file(lbm_domain* d, int savetype, const char* dir, int index);
  * den_prev may be NULL (out[4] is then 0).  Work is ordered on `stream`
  * (a cudaStream_t, NULL = default stream); every call synchronises that
  * stream and copies the 8 results to the host before it returns.
- * The first call on a device also looks up the array's device address
- * (cudaGetSymbolAddress) and keeps it for later calls on that device; make
- * that first call before any stream capture begins, and do not use the
- * function across a cudaDeviceReset of the device (the kept address would
- * be stale).  All calls on a device share the array and it keeps the last
+ * Every call synchronises `stream`, so it cannot be made on a stream that
+ * is being captured into a graph.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) and keeps it for later calls
+ * on that device; do not use the function across a cudaDeviceReset of the
+ * device (the kept address would be stale).  All calls on a device share the array and it keeps the last
  * call's contents: calls that overlap on the GPU race and must be
  * serialised by the caller. */
 int lbm_field_diagnostics_static(const float* den, const float* den_prev, const float* velx,
