@@ -365,7 +365,12 @@ def pattern_ceilings(pkg, n=256, iters=20):
             ("aa_neighbor_f16", pkg.PATTERN_AA_NEIGHBOR, pkg.STORE_F16_SHIFT),
             ("aa_local_v8_f16", pkg.PATTERN_AA_LOCAL_V8, pkg.STORE_F16_SHIFT),
             ("aa_local_v16_f16", pkg.PATTERN_AA_LOCAL_V16, pkg.STORE_F16_SHIFT),
-            ("aa_local_v16_f32", pkg.PATTERN_AA_LOCAL_V16, pkg.STORE_F32)):
+            ("aa_local_v16_f32", pkg.PATTERN_AA_LOCAL_V16, pkg.STORE_F32),
+            ("aa_paired_local_f16", pkg.PATTERN_AA_PAIRED_LOCAL, pkg.STORE_F16_SHIFT),
+            ("aa_paired_neighbor_f16", pkg.PATTERN_AA_PAIRED_NEIGHBOR, pkg.STORE_F16_SHIFT),
+            ("pull_quad_f16", pkg.PATTERN_PULL_QUAD, pkg.STORE_F16_SHIFT),
+            ("aa_quad_local_f16", pkg.PATTERN_AA_QUAD_LOCAL, pkg.STORE_F16_SHIFT),
+            ("aa_quad_neighbor_f16", pkg.PATTERN_AA_QUAD_NEIGHBOR, pkg.STORE_F16_SHIFT)):
         m, g = pkg.pattern_ceiling(pat, st, n, iters)
         out[name] = {"MLUPS": round(m, 1), "GB_s": round(g, 1)}
     out["box"] = f"{n}^3, {iters} timed launches after 3, CUDA events"

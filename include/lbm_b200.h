@@ -168,10 +168,16 @@ enum {
   LBM_KERNEL_SCALAR = 1,  /* one node per thread                            */
   LBM_KERNEL_PACKED = 2,  /* two nodes per thread, packed FP32 arithmetic   */
   LBM_KERNEL_TMA = 3,     /* TMA-staged tiles, persistent producer/consumer */
-  LBM_KERNEL_PAIRED = 4   /* 16-bit pull form: rows stored as 32-bit words of
+  LBM_KERNEL_PAIRED = 4,  /* 16-bit pull form: rows stored as 32-bit words of
                              the node pairs (x, x + px/2), two nodes per thread
                              with packed FP32 arithmetic; the default (AUTO)
                              of FP16/BF16 shifted storage with LBM_STREAM_AB  */
+  LBM_KERNEL_QUAD = 5     /* 16-bit AA form: rows stored as 8-byte words of
+                             the nodes (w, w + nx/2, w + nx/4, w + 3nx/4), four
+                             nodes per thread, every access an aligned 8-byte
+                             word in both AA step kinds; the default (AUTO) of
+                             FP16/BF16 shifted storage with LBM_STREAM_AA when
+                             nx is a multiple of 8 and at least 16            */
 };
 
 typedef struct lbm_options {
@@ -198,9 +204,10 @@ typedef struct lbm_options {
  * from a hash of (node pair, step, seed), so runs are reproducible.  In a
  * steady flow round-to-nearest rounds the same value the same way every
  * step, a bias that accumulates; stochastic rounding turns it into noise.
- * STOCHASTIC needs FP16/BF16 shifted storage with LBM_STREAM_AB and kernel
- * AUTO, PAIRED or SCALAR (single domains; batch members round to nearest).
- * The initial state and imports round to nearest. */
+ * STOCHASTIC needs FP16/BF16 shifted storage, with LBM_STREAM_AB and kernel
+ * AUTO, PAIRED or SCALAR, or with LBM_STREAM_AA on quad rows (kernel AUTO or
+ * QUAD) (single domains; batch members round to nearest).  The initial
+ * state, imports and the first AA step after them round to nearest. */
 enum { LBM_ROUND_NEAREST = 0, LBM_ROUND_STOCHASTIC = 1 };
 
 /* Fill *opt with the defaults: FP32, reference init, A/B streaming. */
@@ -464,7 +471,14 @@ enum {
   LBM_PATTERN_AA_LOCAL = 3,     /* AA local step, one element per access       */
   LBM_PATTERN_AA_NEIGHBOR = 4,  /* AA neighbour step, one element per access   */
   LBM_PATTERN_AA_LOCAL_V8 = 5,  /* AA local step, 8-byte vectors per lane      */
-  LBM_PATTERN_AA_LOCAL_V16 = 6  /* AA local step, 16-byte vectors per lane     */
+  LBM_PATTERN_AA_LOCAL_V16 = 6, /* AA local step, 16-byte vectors per lane     */
+  /* 16-bit only: */
+  LBM_PATTERN_AA_PAIRED_LOCAL = 7,     /* AA steps over paired rows: 32-bit   */
+  LBM_PATTERN_AA_PAIRED_NEIGHBOR = 8,  /* words, two nodes per thread         */
+  LBM_PATTERN_PULL_QUAD = 9,           /* rows as 8-byte words of the nodes   */
+  LBM_PATTERN_AA_QUAD_LOCAL = 10,      /* (w, w+Q, w+2Q, w+3Q), Q = px/4:     */
+  LBM_PATTERN_AA_QUAD_NEIGHBOR = 11    /* four nodes per thread, x shifts are
+                                          whole-word shifts                   */
 };
 int lbm_pattern_ceiling(int pattern, int storage, int n, int iters, double* mlups,
                         double* gbs);

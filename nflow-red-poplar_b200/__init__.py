@@ -41,10 +41,11 @@ SAVE_VTU, SAVE_CSV = 0, 1
 STORE_F32, STORE_F16_SHIFT, STORE_BF16_SHIFT, STORE_F64 = 0, 1, 2, 3
 INIT_REFERENCE, INIT_DENSITY_NOISE, INIT_CHANNEL = 0, 1, 2
 STREAM_AB, STREAM_AA = 0, 1
-KERNEL_AUTO, KERNEL_SCALAR, KERNEL_PACKED, KERNEL_TMA, KERNEL_PAIRED = 0, 1, 2, 3, 4
+KERNEL_AUTO, KERNEL_SCALAR, KERNEL_PACKED, KERNEL_TMA, KERNEL_PAIRED, KERNEL_QUAD = 0, 1, 2, 3, 4, 5
 ROUND_NEAREST, ROUND_STOCHASTIC = 0, 1
 (PATTERN_COPY, PATTERN_PULL, PATTERN_PULL_PAIRED, PATTERN_AA_LOCAL, PATTERN_AA_NEIGHBOR,
- PATTERN_AA_LOCAL_V8, PATTERN_AA_LOCAL_V16) = range(7)
+ PATTERN_AA_LOCAL_V8, PATTERN_AA_LOCAL_V16, PATTERN_AA_PAIRED_LOCAL, PATTERN_AA_PAIRED_NEIGHBOR,
+ PATTERN_PULL_QUAD, PATTERN_AA_QUAD_LOCAL, PATTERN_AA_QUAD_NEIGHBOR) = range(12)
 SERVE_FIFO, SERVE_SHORTEST = 0, 1
 REQ_QUEUED, REQ_RESIDENT, REQ_DONE = 0, 1, 2
 

@@ -181,7 +181,7 @@ int launch_grid(lbm_batch* b, int variant, int block, int* grid) {
 
 int member_mode(const lbm_domain* d) {
   return d->opt.stream_mode == LBM_STREAM_AA ? kModeAA
-                                             : (d->g.paired ? kModePaired : kModePull);
+                                             : (d->g.rows == kRowsPaired ? kModePaired : kModePull);
 }
 
 int member_variant(const lbm_domain* d) {
@@ -387,7 +387,7 @@ int issue_chunk_flat(lbm_batch* b, int steps_offered, long long* lups) {
       it.active = (int)std::min<long long>(std::min(S, steps_offered), left);
       it.cur0 = d->cur;
       it.entry0 = d->aa_first ? kAAFromInit : (d->post_direct ? kAAComplete : kAAPending);
-      it.row_items = d->g.paired ? d->g.px / 2 : d->g.nx;
+      it.row_items = d->g.rows == kRowsPaired ? d->g.px / 2 : d->g.nx;
       const long long items = (long long)it.row_items * d->g.nz * d->g.ny;
       it.ctas = (unsigned)((items + kFlatBlock - 1) / kFlatBlock);
       if (it.ctas >= own) {
@@ -548,7 +548,7 @@ int issue_chunk(lbm_batch* b, int steps_offered, long long* lups) {
       const int active = (int)std::min<long long>(std::min(S, steps_offered), left);
       SlotMeta& sm = b->h_meta[n];
       // items of a row: its nodes, or the words of a paired row
-      const int row_items = d->g.paired ? d->g.px / 2 : d->g.nx;
+      const int row_items = d->g.rows == kRowsPaired ? d->g.px / 2 : d->g.nx;
       const long long items = (long long)row_items * d->g.nz * d->g.ny;
       sm.image_base = m.image_slot * kImages;
       sm.nx = row_items;
@@ -731,7 +731,8 @@ int lbm_batch_add(lbm_batch* b, const Inputval* pinput, const lbm_options* opt,
   if (target_steps < 0) return set_error(LBM_ERR_INVALID, "negative step target");
   if (opt && opt->storage == LBM_STORE_F64)
     return set_error(LBM_ERR_INVALID, "FP64 storage is not supported in batches");
-  if (opt && (opt->kernel == LBM_KERNEL_PACKED || opt->kernel == LBM_KERNEL_TMA))
+  if (opt && (opt->kernel == LBM_KERNEL_PACKED || opt->kernel == LBM_KERNEL_TMA ||
+              opt->kernel == LBM_KERNEL_QUAD))
     return set_error(LBM_ERR_INVALID,
                      "batches step one node (or one paired word) per thread: kernel AUTO, "
                      "SCALAR or PAIRED");
@@ -740,8 +741,11 @@ int lbm_batch_add(lbm_batch* b, const Inputval* pinput, const lbm_options* opt,
   lbm_domain* d = new lbm_domain();
   domain_prepare(d, pinput, opt);
   // 16-bit A/B members keep the paired rows of a single domain where the
-  // paired step applies (no STRUCT nodes, nx large enough), else plain rows
-  if (d->g.paired && !paired_kernel_applies(d->g)) d->g.paired = 0;
+  // paired step applies (no STRUCT nodes, nx large enough), else plain rows;
+  // AA members keep plain rows (the batched AA step is per node)
+  if (d->opt.stream_mode == LBM_STREAM_AA ||
+      (d->g.rows == kRowsPaired && !paired_kernel_applies(d->g)))
+    d->g.rows = kRowsPlain;
   d->opt.device = b->opt.device;
   d->pooled = true;
   d->stream = b->stream;

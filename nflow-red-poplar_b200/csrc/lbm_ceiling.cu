@@ -22,6 +22,14 @@
 //                   stores of plane q at x + c_q, one element per access
 //   AA_LOCAL_V8     AA local step with 8-byte vectors per lane
 //   AA_LOCAL_V16    AA local step with 16-byte vectors per lane
+//   AA_PAIRED_LOCAL, AA_PAIRED_NEIGHBOR
+//                   16-bit only: the AA steps over paired rows (32-bit words
+//                   of the nodes (w, w + px/2)), two nodes per thread
+//   PULL_QUAD, AA_QUAD_LOCAL, AA_QUAD_NEIGHBOR
+//                   16-bit only: rows stored as 8-byte words holding the
+//                   nodes (w, w + Q, w + 2Q, w + 3Q), Q = px/4, four nodes
+//                   per thread; an x shift is a whole-word shift, so every
+//                   access of both AA steps and of pull is an aligned vector
 //
 // Boxes of n^3 nodes, n a multiple of 32; shifted patterns visit the
 // interior nodes only (every donor and destination then lies inside).
@@ -29,6 +37,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <type_traits>
 
 #include "../../include/lbm_b200.h"
 #include "lbm_d3q19.cuh"
@@ -177,6 +186,62 @@ __global__ void __launch_bounds__(128) k_aa_local_vec(T* __restrict__ lat, Box b
   });
 }
 
+// 16-bit rows stored as words of NPW nodes (word w of a row holds the nodes
+// w + k n/NPW, k < NPW): MODE 0 pull, 1 AA local, 2 AA neighbour; shifted
+// modes visit the interior words 1 .. n/NPW - 2 of interior rows, so every
+// shifted word lies inside the row
+template <int NPW, int MODE>
+__global__ void __launch_bounds__(128) k_words(const void* __restrict__ src_, void* __restrict__ dst_,
+                                               Box b) {
+  using W = typename std::conditional<NPW == 2, uint32_t,
+                                      typename std::conditional<NPW == 4, uint2, uint4>::type>::type;
+  constexpr int P = NPW / 2;  // 32-bit pieces per word
+  const int NW = b.n / NPW;   // words per row
+  const int w = blockIdx.x * blockDim.x + threadIdx.x, z = blockIdx.y, y = blockIdx.z;
+  if (MODE == 1) {
+    if (w >= NW) return;
+  } else if (w < 1 || w > NW - 2 || z < 1 || z > b.n - 2 || y < 1 || y > b.n - 2) {
+    return;
+  }
+  const W* src = reinterpret_cast<const W*>(src_);
+  W* dst = reinterpret_cast<W*>(MODE == 0 ? dst_ : const_cast<void*>(src_));
+  const long long qw = b.qs / NPW;  // plane stride in words
+  const long long cell = w + (long long)NW * (z + (long long)b.n * y);
+  W v[Q];
+  float2 acc[P];
+#pragma unroll
+  for (int p = 0; p < P; ++p) acc[p] = make_float2(0.f, 0.f);
+  static_for<0, Q>([&](auto qc) {
+    constexpr int q = decltype(qc)::value;
+    const int off = cx(q) + NW * (cz(q) + b.n * cy(q));
+    if (MODE == 0) v[q] = src[q * qw + cell - off];
+    if (MODE == 1) v[q] = src[q * qw + cell];
+    if (MODE == 2) v[q] = src[opp(q) * qw + cell - off];
+    const __half2* h = reinterpret_cast<const __half2*>(&v[q]);
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      const float2 f = __half22float2(h[p]);
+      acc[p].x += f.x;
+      acc[p].y += f.y;
+    }
+  });
+  static_for<0, Q>([&](auto qc) {
+    constexpr int q = decltype(qc)::value;
+    const int off = cx(q) + NW * (cz(q) + b.n * cy(q));
+    W o;
+    __half2* oh = reinterpret_cast<__half2*>(&o);
+    const __half2* h = reinterpret_cast<const __half2*>(&v[q]);
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      const float2 f = __half22float2(h[p]);
+      oh[p] = __floats2half2_rn(fmaf(f.x, 0.5f, acc[p].x * 1e-7f), fmaf(f.y, 0.5f, acc[p].y * 1e-7f));
+    }
+    if (MODE == 0) dst[q * qw + cell] = o;
+    if (MODE == 1) dst[opp(q) * qw + cell] = o;
+    if (MODE == 2) dst[q * qw + cell + off] = o;
+  });
+}
+
 // plain copy of 19 planes with 16-byte vectors, each plane streamed
 // independently (the streaming bound of 19 + 19 planes)
 template <class T>
@@ -221,6 +286,20 @@ int launch(int pattern, void* a, void* b2, Box b, cudaStream_t st) {
       k_aa_local_vec<T, 16><<<dim3((b.n / per + 127) / 128, b.n, b.n), blk, 0, st>>>((T*)a, b);
       break;
     }
+    case LBM_PATTERN_AA_PAIRED_LOCAL:
+    case LBM_PATTERN_AA_PAIRED_NEIGHBOR:
+    case LBM_PATTERN_PULL_QUAD:
+    case LBM_PATTERN_AA_QUAD_LOCAL:
+    case LBM_PATTERN_AA_QUAD_NEIGHBOR: {
+      const int npw = pattern <= LBM_PATTERN_AA_PAIRED_NEIGHBOR ? 2 : 4;
+      const dim3 gw((b.n / npw + 127) / 128, b.n, b.n);
+      if (pattern == LBM_PATTERN_AA_PAIRED_LOCAL) k_words<2, 1><<<gw, blk, 0, st>>>(a, b2, b);
+      if (pattern == LBM_PATTERN_AA_PAIRED_NEIGHBOR) k_words<2, 2><<<gw, blk, 0, st>>>(a, b2, b);
+      if (pattern == LBM_PATTERN_PULL_QUAD) k_words<4, 0><<<gw, blk, 0, st>>>(a, b2, b);
+      if (pattern == LBM_PATTERN_AA_QUAD_LOCAL) k_words<4, 1><<<gw, blk, 0, st>>>(a, b2, b);
+      if (pattern == LBM_PATTERN_AA_QUAD_NEIGHBOR) k_words<4, 2><<<gw, blk, 0, st>>>(a, b2, b);
+      break;
+    }
   }
   return cudaGetLastError() == cudaSuccess ? LBM_OK : LBM_ERR_CUDA;
 }
@@ -231,7 +310,10 @@ long long nodes_of(int pattern, int n) {
   switch (pattern) {
     case LBM_PATTERN_PULL:
     case LBM_PATTERN_AA_NEIGHBOR: return i * i * i;
-    case LBM_PATTERN_PULL_PAIRED: return 2LL * (n / 2 - 2) * i * i;
+    case LBM_PATTERN_PULL_PAIRED:
+    case LBM_PATTERN_AA_PAIRED_NEIGHBOR: return 2LL * (n / 2 - 2) * i * i;
+    case LBM_PATTERN_PULL_QUAD:
+    case LBM_PATTERN_AA_QUAD_NEIGHBOR: return 4LL * (n / 4 - 2) * i * i;
     default: return (long long)n * n * n;
   }
 }
@@ -241,12 +323,13 @@ long long nodes_of(int pattern, int n) {
 extern "C" int lbm_pattern_ceiling(int pattern, int storage, int n, int iters, double* mlups,
                                    double* gbs) {
   if (!mlups || !gbs) return lbm::set_error(LBM_ERR_INVALID, "lbm_pattern_ceiling: NULL output");
-  if (pattern < LBM_PATTERN_COPY || pattern > LBM_PATTERN_AA_LOCAL_V16)
+  if (pattern < LBM_PATTERN_COPY || pattern > LBM_PATTERN_AA_QUAD_NEIGHBOR)
     return lbm::set_error(LBM_ERR_INVALID, "unknown pattern %d", pattern);
   if (storage != LBM_STORE_F32 && storage != LBM_STORE_F16_SHIFT)
     return lbm::set_error(LBM_ERR_INVALID, "patterns are timed for F32 and F16 storage only");
-  if (pattern == LBM_PATTERN_PULL_PAIRED && storage != LBM_STORE_F16_SHIFT)
-    return lbm::set_error(LBM_ERR_INVALID, "the paired pattern is a 16-bit layout");
+  if ((pattern == LBM_PATTERN_PULL_PAIRED || pattern >= LBM_PATTERN_AA_PAIRED_LOCAL) &&
+      storage != LBM_STORE_F16_SHIFT)
+    return lbm::set_error(LBM_ERR_INVALID, "the word patterns are 16-bit layouts");
   if (n < 32 || n > 512 || n % 32 || iters < 1 || iters > 100000)
     return lbm::set_error(LBM_ERR_INVALID, "n must be a multiple of 32 in [32, 512], iters >= 1");
   const size_t elem = storage == LBM_STORE_F32 ? 4 : 2;

@@ -110,6 +110,14 @@ inline size_t storage_bytes(int storage) {
 
 inline long long round_up(long long v, long long m) { return (v + m - 1) / m * m; }
 
+// A 16-bit AA domain can be stored in paired or quad rows (kRowsPaired,
+// kRowsQuad): the word AA step needs rows of whole words without padding
+// nodes (px == nx, a multiple of 8) and at least four words per row quarter.
+inline bool aa_word_rows_fit(const Inputval* in, const lbm_options* opt) {
+  return opt && (opt->storage == LBM_STORE_F16_SHIFT || opt->storage == LBM_STORE_BF16_SHIFT) &&
+         opt->stream_mode == LBM_STREAM_AA && in->nx % 8 == 0 && in->nx >= 16;
+}
+
 inline int validate(const Inputval* in, const lbm_options* opt) {
   if (!in) return set_error(LBM_ERR_INVALID, "NULL Inputval");
   if (in->nx < 3 || in->ny < 3 || in->nz < 3)
@@ -143,26 +151,35 @@ inline int validate(const Inputval* in, const lbm_options* opt) {
                        "AA streaming is implemented for the cavity (casetype %d) and the channel "
                        "(casetype %d) only",
                        CAVITY, CHANNEL);
-    if (opt->kernel < LBM_KERNEL_AUTO || opt->kernel > LBM_KERNEL_PAIRED)
+    if (opt->kernel < LBM_KERNEL_AUTO || opt->kernel > LBM_KERNEL_QUAD)
       return set_error(LBM_ERR_INVALID, "unknown kernel %d", opt->kernel);
+    if (opt->kernel == LBM_KERNEL_QUAD && !aa_word_rows_fit(in, opt))
+      return set_error(LBM_ERR_INVALID,
+                       "the quad kernel is the 16-bit AA form: FP16/BF16 shifted storage with "
+                       "LBM_STREAM_AA and nx a multiple of 8, at least 16 (nx = %d)",
+                       in->nx);
     if (opt->kernel == LBM_KERNEL_PAIRED &&
         ((opt->storage != LBM_STORE_F16_SHIFT && opt->storage != LBM_STORE_BF16_SHIFT) ||
-         opt->stream_mode != LBM_STREAM_AB))
+         (opt->stream_mode == LBM_STREAM_AA && !aa_word_rows_fit(in, opt))))
       return set_error(LBM_ERR_INVALID,
-                       "the paired kernel is the 16-bit pull (A/B) form: FP16/BF16 shifted "
-                       "storage with LBM_STREAM_AB");
+                       "the paired kernel is a 16-bit form: FP16/BF16 shifted storage, with "
+                       "LBM_STREAM_AB, or with LBM_STREAM_AA and nx a multiple of 8, at least 16");
     if (opt->wait_test < 0 || (opt->wait_test > 0 && opt->kernel != LBM_KERNEL_TMA))
       return set_error(LBM_ERR_INVALID, "wait_test applies to the TMA kernel only");
     if (opt->rounding != LBM_ROUND_NEAREST && opt->rounding != LBM_ROUND_STOCHASTIC)
       return set_error(LBM_ERR_INVALID, "unknown rounding %d", opt->rounding);
     if (opt->rounding == LBM_ROUND_STOCHASTIC &&
         ((opt->storage != LBM_STORE_F16_SHIFT && opt->storage != LBM_STORE_BF16_SHIFT) ||
-         opt->stream_mode != LBM_STREAM_AB ||
-         (opt->kernel != LBM_KERNEL_AUTO && opt->kernel != LBM_KERNEL_PAIRED &&
-          opt->kernel != LBM_KERNEL_SCALAR)))
+         (opt->stream_mode == LBM_STREAM_AB && opt->kernel != LBM_KERNEL_AUTO &&
+          opt->kernel != LBM_KERNEL_PAIRED && opt->kernel != LBM_KERNEL_SCALAR) ||
+         (opt->stream_mode == LBM_STREAM_AA &&
+          ((opt->kernel != LBM_KERNEL_AUTO && opt->kernel != LBM_KERNEL_QUAD &&
+            opt->kernel != LBM_KERNEL_PAIRED) ||
+           !aa_word_rows_fit(in, opt)))))
       return set_error(LBM_ERR_INVALID,
-                       "stochastic rounding needs FP16/BF16 shifted storage with LBM_STREAM_AB "
-                       "and kernel AUTO, PAIRED or SCALAR");
+                       "stochastic rounding needs FP16/BF16 shifted storage, with LBM_STREAM_AB "
+                       "and kernel AUTO, PAIRED or SCALAR, or with LBM_STREAM_AA on paired or "
+                       "quad rows (kernel AUTO, PAIRED or QUAD, nx a multiple of 8, at least 16)");
     if (!std::isfinite(opt->noise_amp) || !std::isfinite(opt->store_scale) ||
         opt->store_scale < 0.0f)
       return set_error(LBM_ERR_INVALID, "bad noise_amp/store_scale");
@@ -217,8 +234,8 @@ StepArgs<S> make_args(const lbm_domain* d, const void* src, void* dst, long long
   a.dst = (S*)dst;
   a.qs = d->qs;
   for (int q = 0; q < Q; ++q) {
-    // paired rows: a node one step away in x is two elements away
-    a.off[q] = (d->g.paired ? 2 : 1) * cx(q) + d->g.px * (cz(q) + d->g.nz * cy(q));
+    // paired / quad rows: a node one step away in x is two / four elements away
+    a.off[q] = row_step(d->g.rows) * cx(q) + d->g.px * (cz(q) + d->g.nz * cy(q));
     a.srcq[q] = src ? (const S*)src + q * d->qs : nullptr;
     a.srcd[q] = src ? (const S*)src + (q * d->qs - a.off[q]) : nullptr;
     a.dstq[q] = dst ? (S*)dst + q * d->qs : nullptr;
@@ -294,7 +311,7 @@ int with_model(const lbm_domain* d, F&& f) {
 template <class S, int COLL, bool LES>
 void launch_step(const lbm_domain* d, const StepArgs<S>& a, cudaStream_t st) {
   if constexpr (kDev<S>) {
-    if (d->g.paired) {
+    if (d->g.rows == kRowsPaired) {
       // one thread per word, CTAs no wider than a row's words (px / 2)
       const dim3 bp = block_of(d->g.px / 2);
       const dim3 gr((d->g.px / 2 + bp.x - 1) / bp.x, d->g.nz, d->g.ny);
@@ -365,7 +382,7 @@ inline TensorMapEncodeFn tensor_map_encoder() {
 // kernel option then falls back to the scalar kernel) for FP64 storage.
 template <class S>
 int domain_tensor_maps(lbm_domain* d, int sm_count) {
-  if (d->opt.stream_mode == LBM_STREAM_AA || d->g.paired) {
+  if (d->opt.stream_mode == LBM_STREAM_AA || d->g.rows != kRowsPlain) {
     // the TMA kernel is a pull (A/B) kernel over plain rows
     d->tmap_ok = false;
     return LBM_OK;
@@ -475,6 +492,11 @@ inline void free_all(lbm_domain* d) {
 }
 
 
+// Rows of a 16-bit AA domain with kernel AUTO where word rows fit.
+#ifndef LBM_AA_AUTO_ROWS
+#define LBM_AA_AUTO_ROWS kRowsQuad
+#endif
+
 // Fill the geometry, sizes and storage scale of d from the case.
 inline void domain_prepare(lbm_domain* d, const Inputval* pinput, const lbm_options* opt) {
   d->in = *pinput;
@@ -489,11 +511,19 @@ inline void domain_prepare(lbm_domain* d, const Inputval* pinput, const lbm_opti
   d->g.px = s.px;
   d->g.casetype = pinput->casetype;
   d->g.solid = nullptr;
-  // 16-bit pull (A/B) domains use paired rows unless another kernel is asked for
+  // 16-bit pull (A/B) domains use paired rows and 16-bit AA domains quad
+  // rows where they fit, unless another kernel is asked for
   const bool b16 =
       d->opt.storage == LBM_STORE_F16_SHIFT || d->opt.storage == LBM_STORE_BF16_SHIFT;
-  d->g.paired = b16 && d->opt.stream_mode == LBM_STREAM_AB &&
-                (d->opt.kernel == LBM_KERNEL_AUTO || d->opt.kernel == LBM_KERNEL_PAIRED);
+  d->g.rows = kRowsPlain;
+  if (b16 && d->opt.stream_mode == LBM_STREAM_AB &&
+      (d->opt.kernel == LBM_KERNEL_AUTO || d->opt.kernel == LBM_KERNEL_PAIRED))
+    d->g.rows = kRowsPaired;
+  if (aa_word_rows_fit(pinput, &d->opt)) {
+    if (d->opt.kernel == LBM_KERNEL_AUTO) d->g.rows = LBM_AA_AUTO_ROWS;
+    if (d->opt.kernel == LBM_KERNEL_PAIRED) d->g.rows = kRowsPaired;
+    if (d->opt.kernel == LBM_KERNEL_QUAD) d->g.rows = kRowsQuad;
+  }
   d->N = s.N;
   d->qs = s.qs;
   d->elem = storage_bytes(d->opt.storage);

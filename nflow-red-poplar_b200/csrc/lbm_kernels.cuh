@@ -66,26 +66,46 @@ __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(
 __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
 
+// Row layouts of the population planes (Geometry::rows).
+//   kRowsPlain:  element x of a row holds node x.
+//   kRowsPaired: 16-bit storage.  Element 2w of a row holds node w and
+//                element 2w + 1 node w + px/2, so that the 32-bit word w
+//                holds the node pair (w, w + px/2) and a donor one node away
+//                in x is one word away for both nodes of the pair
+//                (k_step_paired; AA form: k_aa_words).
+//   kRowsQuad:   16-bit storage, AA form (px == nx, a multiple of 8).  With
+//                D = px/4, the 8-byte word w of a row holds the nodes
+//                w, w + 2D, w + D, w + 3D in its four 16-bit slots, so that
+//                its low half is the paired word (w, w + px/2) and its high
+//                half the paired word (w + D, w + D + px/2); a node one step
+//                away in x is one word away for all four nodes (k_aa_words).
+enum { kRowsPlain = 0, kRowsPaired = 1, kRowsQuad = 2 };
+
 struct Geometry {
   int nx, ny, nz, px;
   int casetype;
-  // paired rows (16-bit storage, pull form): element 2w of a row holds node
-  // w and element 2w + 1 node w + px/2, so that the 32-bit word w holds the
-  // node pair (w, w + px/2) and a donor one node away in x is one word away
-  // for both nodes of the pair (k_step_paired)
-  int paired;
+  int rows;                    // kRows*
   const unsigned char* solid;  // [ny][nz][nx], nonzero = STRUCT; may be null
 };
 
-// element of node x within its row (plain or paired rows)
-__host__ __device__ __forceinline__ int row_slot(int x, int px, bool paired) {
-  if (!paired) return x;
-  const int h = px >> 1;
-  return x < h ? 2 * x : 2 * (x - h) + 1;
+// element of node x within its row (any row layout)
+__host__ __device__ __forceinline__ int row_slot(int x, int px, int rows) {
+  if (rows == kRowsPlain) return x;
+  if (rows == kRowsPaired) {
+    const int h = px >> 1;
+    return x < h ? 2 * x : 2 * (x - h) + 1;
+  }
+  const int d = px >> 2;
+  const int k = x / d, w = x - k * d;  // quarter k of the row, word w
+  return 4 * w + ((k & 1) << 1) + (k >> 1);
 }
 // in-plane element index of node (x, y, z)
 __host__ __device__ __forceinline__ int cell_of(const Geometry& g, int x, int y, int z) {
-  return row_slot(x, g.px, g.paired != 0) + g.px * (z + g.nz * y);
+  return row_slot(x, g.px, g.rows) + g.px * (z + g.nz * y);
+}
+// elements between x neighbours of a row layout
+__host__ __device__ __forceinline__ int row_step(int rows) {
+  return rows == kRowsPlain ? 1 : (rows == kRowsPaired ? 2 : 4);
 }
 
 // the geometry holds STRUCT nodes: POISEUILLE, or any case with a solid mask
@@ -196,7 +216,7 @@ struct PlaneAddr {
   __device__ __forceinline__ float scale() const { return a.scale; }
 };
 
-// The same per-node addressing for either row layout (a.g.paired): the
+// The same per-node addressing for any row layout (a.g.rows): the
 // donor x - c_q of population q is addressed through its own row slot.
 // Used by the per-node kernels of paired domains (edge words, initial
 // state, import, export); a donor outside the box is never formed.
@@ -693,12 +713,29 @@ __global__ void __launch_bounds__(128)
 // take make_args with k = s + 1.
 // ------------------------------------------------------------------ //
 
-// arF of node (x, y, z) from the swapped layout
+// arF of node (x, y, z) from the swapped layout (cell = cell_of the node)
 template <class S>
 __device__ __forceinline__ void aa_pull_swapped(RealOf<S> (&f)[Q], const StepArgs<S>& a, int x,
                                                 int y, int z, int cell) {
   const bool edge = (x == 0) | (x == a.g.nx - 1) | (y == 0) | (y == a.g.ny - 1) | (z == 0) |
                     (z == a.g.nz - 1);
+  if (a.g.rows != kRowsPlain) {
+    // quad rows: x neighbours are not a fixed element offset apart
+    const int t = edge ? node_type(a.g, x, y, z) : NODE_FLUID;
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      const int xs = x - cx(q), ys = y - cy(q), zs = z - cz(q);
+      const bool inside = (unsigned)xs < (unsigned)a.g.nx && (unsigned)ys < (unsigned)a.g.ny &&
+                          (unsigned)zs < (unsigned)a.g.nz;
+      if (inside) {
+        f[q] = ld(a.srcq[opp(q)] + cell_of(a.g, xs, ys, zs), q, a.inv_scale);
+      } else {
+        const RealOf<S> fo = ld(a.srcq[q] + cell, q, a.inv_scale);  // own f*_{opp q}
+        f[q] = boundary_value<S, q>(a, t, fo, y, z);
+      }
+    });
+    return;
+  }
   if (!edge) {
     static_for<0, Q>([&](auto qc) {
       constexpr int q = decltype(qc)::value;
@@ -826,7 +863,9 @@ template <class S, int COLL, bool LES, bool WARP_ROW = false>
 __device__ __forceinline__ void aa_step_node(const StepArgs<S>& a, int x, int y, int z,
                                              int neighbor, int entry) {
   using R = RealOf<S>;
-  const int cell = x + a.g.px * (z + a.g.nz * y);
+  // quad rows (16-bit storage) reach this per-node step only as a local
+  // step, whose slots are all at the node
+  const int cell = kDev<S> ? cell_of(a.g, x, y, z) : x + a.g.px * (z + a.g.nz * y);
   const bool face_row = (y == 0) | (y == a.g.ny - 1) | (z == 0) | (z == a.g.nz - 1);
   const bool xface = (x == 0) | (x == a.g.nx - 1);
   const bool edge = face_row | xface;
@@ -924,7 +963,7 @@ __global__ void __launch_bounds__(128) k_aa_macro(const __grid_constant__ StepAr
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int z = blockIdx.y, y = blockIdx.z;
   if (x >= a.g.nx) return;
-  const int cell = x + a.g.px * (z + a.g.nz * y);
+  const int cell = cell_of(a.g, x, y, z);
   R f[Q];
   if (layout == kAASwapped) {
     aa_pull_swapped<S>(f, a, x, y, z, cell);
@@ -972,7 +1011,7 @@ __global__ void __launch_bounds__(128)
     if (mode == kExportAANaturalPending) aa_open_face_rules<S>(f, a, x, y, z);
   } else if (mode == kExportAASwapped) {
     aa_pull_swapped<S>(f, a, x, y, z, (int)cell);
-  } else if (a.g.paired) {
+  } else if (a.g.rows != kRowsPlain) {
     pull<S>(f, a, RowAddr<S>(a, x, y, z), x, y, z);
   } else {
     pull<S>(f, a, PlaneAddr<S>(a, (int)cell), x, y, z);
@@ -1092,7 +1131,7 @@ __global__ void __launch_bounds__(64, LBM_PACKED_MIN_BLOCKS) k_step2(const __gri
 // Paired rows: the 16-bit pull step with two nodes per thread and 32-bit
 // accesses only.
 //
-// With Geometry::paired, word w of a row holds the nodes (w, w + H),
+// With paired rows (kRowsPaired), word w of a row holds the nodes (w, w + H),
 // H = px / 2.  The donors x - c_q of both nodes of a pair then lie in one
 // word of the donor row, shifted by c_x, so a thread loads one aligned
 // 32-bit word per population for two nodes (a warp reads 128 contiguous

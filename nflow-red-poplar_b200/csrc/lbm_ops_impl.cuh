@@ -5,6 +5,7 @@
 // the kernels of the four formats compile in parallel.
 #pragma once
 #include "lbm_domain.cuh"
+#include "lbm_quad.cuh"
 
 namespace lbm {
 
@@ -122,13 +123,57 @@ int ops_run_aa(lbm_domain* d, int nsteps) {
     auto args = [&](long long k, bool den, int neighbor) {
       return aa_args<S>(d, k, den, neighbor);
     };
+    // paired / quad rows (16-bit): k_aa_words, one word of two / four nodes
+    // per thread, except the first step after the initial state (a local
+    // step, whose slots are all at the node: the per-node step over the
+    // domain's rows)
+    int nh = 0;
+    dim3 bw(1, 1, 1), gw(1, 1, 1);
+    if constexpr (kDev<S>) {
+      if (d->g.rows != kRowsPlain) {
+        if (!aa_words_apply(d->g))
+          return set_error(LBM_ERR_INVALID, "AA domain rows without the word step");
+        nh = d->g.rows == kRowsQuad ? 2 : 1;
+        const int nw = d->g.px / (2 * nh);
+        bw = block_of(nw);
+        gw = dim3((nw + bw.x - 1) / bw.x, d->g.nz, d->g.ny);
+      }
+    }
+    auto launch = [&](cudaStream_t st, const StepArgs<S>& a, int nb, int entry) {
+      if constexpr (kDev<S>) {
+        if (nh && entry != kAAFromInit) {
+          auto go = [&](auto sr, auto nbc, auto nhc) {
+            k_aa_words<S, C, L, decltype(sr)::value, decltype(nbc)::value, decltype(nhc)::value>
+                <<<gw, bw, 0, st>>>(a, entry);
+          };
+          using T = std::true_type;
+          using F = std::false_type;
+          using I0 = std::integral_constant<int, 0>;
+          using I1 = std::integral_constant<int, 1>;
+          using I2 = std::integral_constant<int, 2>;
+          if (nh == 2) {
+            if (a.sr)
+              nb ? go(T{}, I1{}, I2{}) : go(T{}, I0{}, I2{});
+            else
+              nb ? go(F{}, I1{}, I2{}) : go(F{}, I0{}, I2{});
+          } else {
+            if (a.sr)
+              nb ? go(T{}, I1{}, I1{}) : go(T{}, I0{}, I1{});
+            else
+              nb ? go(F{}, I1{}, I1{}) : go(F{}, I0{}, I1{});
+          }
+          return;
+        }
+      }
+      if (nb)
+        k_aa_step<S, C, L, 1><<<gr, b, 0, st>>>(a, entry);
+      else
+        k_aa_step<S, C, L, 0><<<gr, b, 0, st>>>(a, entry);
+    };
     auto one = [&](bool den) {
       const long long k = d->step + 1;
       const int entry = d->aa_first ? kAAFromInit : (d->post_direct ? kAAComplete : kAAPending);
-      if (d->cur)
-        k_aa_step<S, C, L, 1><<<gr, b, 0, d->stream>>>(args(k, den, 1), entry);
-      else
-        k_aa_step<S, C, L, 0><<<gr, b, 0, d->stream>>>(args(k, den, 0), entry);
+      launch(d->stream, args(k, den, d->cur), d->cur, entry);
       d->aa_first = false;
       d->post_direct = false;
       d->cur ^= 1;
@@ -151,10 +196,7 @@ int ops_run_aa(lbm_domain* d, int nsteps) {
         long long k = d->step;
         for (int i = 0; i < kGraphSteps; ++i) {
           ++k;
-          if (cur)
-            k_aa_step<S, C, L, 1><<<gr, b, 0, d->capture>>>(args(k, false, 1), kAAPending);
-          else
-            k_aa_step<S, C, L, 0><<<gr, b, 0, d->capture>>>(args(k, false, 0), kAAPending);
+          launch(d->capture, args(k, false, cur), cur, kAAPending);
           cur ^= 1;
         }
         cudaGraph_t graph;

@@ -9,7 +9,7 @@ pytestmark = pytest.mark.gpu
 PATTERNS = [(p, pkg.STORE_F32) for p in (pkg.PATTERN_COPY, pkg.PATTERN_PULL, pkg.PATTERN_AA_LOCAL,
                                         pkg.PATTERN_AA_NEIGHBOR, pkg.PATTERN_AA_LOCAL_V8,
                                         pkg.PATTERN_AA_LOCAL_V16)] + \
-           [(p, pkg.STORE_F16_SHIFT) for p in range(7)]
+           [(p, pkg.STORE_F16_SHIFT) for p in range(12)]
 
 
 @pytest.mark.parametrize("pattern,storage", PATTERNS)

@@ -218,14 +218,20 @@ def test_stochastic_rounding_is_reproducible_and_seeded():
 def test_stochastic_rounding_rejected_where_not_built():
     iv = cavity(16, 12, 10)
     for o in (pkg.default_options(storage=pkg.STORE_F32, rounding=pkg.ROUND_STOCHASTIC),
+              # AA on plain rows (the per-node AA step has no stochastic rounding)
               pkg.default_options(storage=pkg.STORE_F16_SHIFT, rounding=pkg.ROUND_STOCHASTIC,
-                                  stream_mode=pkg.STREAM_AA),
+                                  stream_mode=pkg.STREAM_AA, kernel=pkg.KERNEL_SCALAR),
               pkg.default_options(storage=pkg.STORE_F16_SHIFT, rounding=pkg.ROUND_STOCHASTIC,
                                   kernel=pkg.KERNEL_TMA),
               pkg.default_options(storage=pkg.STORE_F16_SHIFT, rounding=5)):
         with pytest.raises(pkg.LbmError) as e:
             pkg.Domain(iv, o)
         assert e.value.code == pkg.LBM_ERR_INVALID
+    # AA rows that are not quad rows (nx not a multiple of 8)
+    with pytest.raises(pkg.LbmError):
+        pkg.Domain(cavity(20, 12, 10),
+                   pkg.default_options(storage=pkg.STORE_F16_SHIFT, rounding=pkg.ROUND_STOCHASTIC,
+                                       stream_mode=pkg.STREAM_AA))
     b = pkg.Batch(hbm_budget=64 << 20)
     with pytest.raises(pkg.LbmError):
         b.add(iv, pkg.default_options(storage=pkg.STORE_F16_SHIFT,

@@ -30,9 +30,9 @@ def channel():
                              mrt=True, les=True, cs=0.1)
 
 
-def run(storage, rounding=pkg.ROUND_NEAREST):
+def run(storage, rounding=pkg.ROUND_NEAREST, stream_mode=pkg.STREAM_AB):
     o = pkg.default_options(storage=storage, init_kind=pkg.INIT_CHANNEL, noise_amp=0.01, seed=1,
-                            rounding=rounding)
+                            rounding=rounding, stream_mode=stream_mode)
     d = pkg.Domain(channel(), o)
     d.run(STEPS)
     den, ux, uy, uz = d.macroscopic()
@@ -72,3 +72,11 @@ def test_bf16_stochastic_rounding_beats_nearest(ref):
     l2_sr, _ = errors(u_sr, ref[0])
     l2_rn, _ = errors(u_rn, ref[0])
     assert l2_sr < l2_rn / 2, (l2_sr, l2_rn)
+
+
+def test_fp16_aa_quad_stochastic_rounding_meets_the_target(ref):
+    """The 16-bit AA form on quad rows (the fastest 16-bit form) with
+    stochastic rounding holds the same bound."""
+    u_sr, _ = run(pkg.STORE_F16_SHIFT, pkg.ROUND_STOCHASTIC, pkg.STREAM_AA)
+    l2_sr, mx_sr = errors(u_sr, ref[0])
+    assert l2_sr <= 1e-3, (l2_sr, mx_sr)
