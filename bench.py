@@ -59,6 +59,11 @@ WORKLOADS = {
 }
 
 
+def KERNELS(pkg):
+    return {"auto": pkg.KERNEL_AUTO, "scalar": pkg.KERNEL_SCALAR, "packed": pkg.KERNEL_PACKED,
+            "tma": pkg.KERNEL_TMA, "paired": pkg.KERNEL_PAIRED, "quad": pkg.KERNEL_QUAD}
+
+
 def make_case(pkg, w, size=None):
     nx, ny, nz = w["nx"], w["ny"], w["nz"]
     if size:
@@ -291,9 +296,11 @@ def precision_c3(pkg, steps, kernel, size=None, warmup=0, re=None):
            "nx": iv.nx, "ny": iv.ny, "nz": iv.nz, "re": w["re_ch"], "tau": float(iv.m_dTau),
            "data": "synthetic", "forms": {}}
 
-    def run(storage, kern, rounding=0):
+    def run(storage, kern, rounding=0, streaming=None):
         o = pkg.default_options(storage=storage, init_kind=w["init"], noise_amp=w["amp"], seed=1,
-                                kernel=kern, rounding=rounding)
+                                kernel=kern, rounding=rounding,
+                                stream_mode=pkg.STREAM_AB if streaming == "ab" else
+                                pkg.STREAM_AA)
         d = pkg.Domain(iv, o)
         d.run(warmup)
         d.sync()
@@ -309,18 +316,26 @@ def precision_c3(pkg, steps, kernel, size=None, warmup=0, re=None):
                     mlups=iv.nx * iv.ny * iv.nz * (steps - warmup) / dt / 1e6,
                     nonfinite=int(diag[7]))
 
-    ref = run(pkg.STORE_F64, pkg.KERNEL_SCALAR)
+    ref = run(pkg.STORE_F64, pkg.KERNEL_SCALAR, streaming="ab")
     ens_ref = _enstrophy(ref["ux"], ref["uy"], ref["uz"])
     u2_ref = (ref["ux"].astype(np.float64) ** 2 + ref["uy"].astype(np.float64) ** 2 +
               ref["uz"].astype(np.float64) ** 2)
     umax = float(np.sqrt(u2_ref.max()))
     out["fp64"] = {"MLUPS": ref["mlups"], "kinetic_energy": ref["ke"], "enstrophy": ens_ref,
                    "max_u": umax}
-    for name, st, rnd in (("f32", pkg.STORE_F32, 0), ("f16_shift", pkg.STORE_F16_SHIFT, 0),
-                          ("bf16_shift", pkg.STORE_BF16_SHIFT, 0),
-                          ("f16_shift_sr", pkg.STORE_F16_SHIFT, pkg.ROUND_STOCHASTIC),
-                          ("bf16_shift_sr", pkg.STORE_BF16_SHIFT, pkg.ROUND_STOCHASTIC)):
-        r = run(st, kernel, rnd)
+    # every form in the AA scheme (FP32: one node per thread; 16-bit: quad
+    # rows), and the 16-bit stochastic-rounding forms also in the pull
+    # scheme (paired rows)
+    for name, st, rnd, sm in (("f32", pkg.STORE_F32, 0, "aa"),
+                              ("f16_shift", pkg.STORE_F16_SHIFT, 0, "aa"),
+                              ("bf16_shift", pkg.STORE_BF16_SHIFT, 0, "aa"),
+                              ("f16_shift_sr", pkg.STORE_F16_SHIFT, pkg.ROUND_STOCHASTIC, "aa"),
+                              ("bf16_shift_sr", pkg.STORE_BF16_SHIFT, pkg.ROUND_STOCHASTIC, "aa"),
+                              ("f16_shift_sr_ab", pkg.STORE_F16_SHIFT, pkg.ROUND_STOCHASTIC,
+                               "ab"),
+                              ("bf16_shift_sr_ab", pkg.STORE_BF16_SHIFT, pkg.ROUND_STOCHASTIC,
+                               "ab")):
+        r = run(st, kernel, rnd, sm)
         d2 = sum((r[k].astype(np.float64) - ref[k].astype(np.float64)) ** 2
                  for k in ("ux", "uy", "uz"))
         ens = _enstrophy(r["ux"], r["uy"], r["uz"])
@@ -332,17 +347,17 @@ def precision_c3(pkg, steps, kernel, size=None, warmup=0, re=None):
             "u_rel_l2_err": float(np.sqrt(d2.sum() / u2_ref.sum())),
             "kinetic_energy_rel_err": abs(r["ke"] - ref["ke"]) / abs(ref["ke"]),
             "enstrophy_rel_err": abs(ens - ens_ref) / abs(ens_ref),
-            "nonfinite_nodes": r["nonfinite"]}
+            "nonfinite_nodes": r["nonfinite"], "streaming": sm}
     f32 = out["forms"]["f32"]["MLUPS"]
-    for name in ("f16_shift", "bf16_shift", "f16_shift_sr", "bf16_shift_sr"):
-        out["forms"][name]["speedup_vs_f32"] = out["forms"][name]["MLUPS"] / f32
+    for name in out["forms"]:
+        if name != "f32":
+            out["forms"][name]["speedup_vs_f32"] = out["forms"][name]["MLUPS"] / f32
     return out
 
 
 def report_precision(args, pkg):
     """--report precision: precision_c3 with --steps steps as one JSON line."""
-    kern = {"auto": pkg.KERNEL_AUTO, "scalar": pkg.KERNEL_SCALAR, "packed": pkg.KERNEL_PACKED,
-            "tma": pkg.KERNEL_TMA}[args.kernel]
+    kern = KERNELS(pkg)[args.kernel]
     out = precision_c3(pkg, args.steps, kern, args.size or None, args.warmup, args.re or None)
     out["report"] = "precision"
     print(json.dumps(out), flush=True)
@@ -565,7 +580,8 @@ def main():
                     choices=["f32", "f16_shift", "bf16_shift", "f64", "f16_shift_sr",
                              "bf16_shift_sr"])
     ap.add_argument("--size", type=int, default=0, help="scale the workload to this nx (profiling)")
-    ap.add_argument("--kernel", default="auto", choices=["auto", "scalar", "packed", "tma"])
+    ap.add_argument("--kernel", default="auto",
+                    choices=["auto", "scalar", "packed", "tma", "paired", "quad"])
     ap.add_argument("--streaming", default=None, choices=["ab", "aa"],
                     help="ab: pull between two lattices; aa: AA pattern in one lattice "
                          "(default: aa for the step line, the 256^3 configuration's scheme; "
@@ -647,9 +663,7 @@ def main():
         streaming = streaming or args.streaming
         opt = pkg.default_options(storage=storage_id[storage], init_kind=w["init"],
                                   noise_amp=w["amp"], seed=1, device=local,
-                                  kernel={"auto": pkg.KERNEL_AUTO, "scalar": pkg.KERNEL_SCALAR,
-                                          "packed": pkg.KERNEL_PACKED,
-                                          "tma": pkg.KERNEL_TMA}[args.kernel],
+                                  kernel=KERNELS(pkg)[args.kernel],
                                   stream_mode=pkg.STREAM_AA if streaming == "aa"
                                   else pkg.STREAM_AB,
                                   rounding=pkg.ROUND_STOCHASTIC if storage.endswith("_sr")
@@ -740,12 +754,12 @@ def main():
                                "lbm_export_arF(padded host AoS), pinned host memory"}
         dom.close()
         # storage forms of the same workload (precision form: throughput),
-        # each with both streaming schemes where the form has them
-        # (stochastic rounding is built for the pull form only)
+        # each with both streaming schemes (16-bit: paired rows for pull,
+        # quad rows for AA)
         forms = {}
         for st in ("f32", "f16_shift", "bf16_shift", "f16_shift_sr", "bf16_shift_sr"):
             f = {}
-            for sm in (("ab",) if st.endswith("_sr") else ("ab", "aa")):
+            for sm in ("ab", "aa"):
                 d2, ms2 = timed_steps(st, args.steps, args.warmup, streaming=sm)
                 d2.close()
                 ms2 = allmax(ms2)

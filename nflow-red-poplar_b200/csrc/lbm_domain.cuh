@@ -110,9 +110,9 @@ inline size_t storage_bytes(int storage) {
 
 inline long long round_up(long long v, long long m) { return (v + m - 1) / m * m; }
 
-// A 16-bit AA domain can be stored in paired or quad rows (kRowsPaired,
-// kRowsQuad): the word AA step needs rows of whole words without padding
-// nodes (px == nx, a multiple of 8) and at least four words per row quarter.
+// A 16-bit AA domain can be stored in quad rows (kRowsQuad): the word AA
+// step needs rows of whole words without padding nodes (px == nx, a
+// multiple of 8) and at least four words per row quarter.
 inline bool aa_word_rows_fit(const Inputval* in, const lbm_options* opt) {
   return opt && (opt->storage == LBM_STORE_F16_SHIFT || opt->storage == LBM_STORE_BF16_SHIFT) &&
          opt->stream_mode == LBM_STREAM_AA && in->nx % 8 == 0 && in->nx >= 16;
@@ -160,10 +160,10 @@ inline int validate(const Inputval* in, const lbm_options* opt) {
                        in->nx);
     if (opt->kernel == LBM_KERNEL_PAIRED &&
         ((opt->storage != LBM_STORE_F16_SHIFT && opt->storage != LBM_STORE_BF16_SHIFT) ||
-         (opt->stream_mode == LBM_STREAM_AA && !aa_word_rows_fit(in, opt))))
+         opt->stream_mode != LBM_STREAM_AB))
       return set_error(LBM_ERR_INVALID,
-                       "the paired kernel is a 16-bit form: FP16/BF16 shifted storage, with "
-                       "LBM_STREAM_AB, or with LBM_STREAM_AA and nx a multiple of 8, at least 16");
+                       "the paired kernel is the 16-bit pull (A/B) form: FP16/BF16 shifted "
+                       "storage with LBM_STREAM_AB");
     if (opt->wait_test < 0 || (opt->wait_test > 0 && opt->kernel != LBM_KERNEL_TMA))
       return set_error(LBM_ERR_INVALID, "wait_test applies to the TMA kernel only");
     if (opt->rounding != LBM_ROUND_NEAREST && opt->rounding != LBM_ROUND_STOCHASTIC)
@@ -173,13 +173,12 @@ inline int validate(const Inputval* in, const lbm_options* opt) {
          (opt->stream_mode == LBM_STREAM_AB && opt->kernel != LBM_KERNEL_AUTO &&
           opt->kernel != LBM_KERNEL_PAIRED && opt->kernel != LBM_KERNEL_SCALAR) ||
          (opt->stream_mode == LBM_STREAM_AA &&
-          ((opt->kernel != LBM_KERNEL_AUTO && opt->kernel != LBM_KERNEL_QUAD &&
-            opt->kernel != LBM_KERNEL_PAIRED) ||
+          ((opt->kernel != LBM_KERNEL_AUTO && opt->kernel != LBM_KERNEL_QUAD) ||
            !aa_word_rows_fit(in, opt)))))
       return set_error(LBM_ERR_INVALID,
                        "stochastic rounding needs FP16/BF16 shifted storage, with LBM_STREAM_AB "
-                       "and kernel AUTO, PAIRED or SCALAR, or with LBM_STREAM_AA on paired or "
-                       "quad rows (kernel AUTO, PAIRED or QUAD, nx a multiple of 8, at least 16)");
+                       "and kernel AUTO, PAIRED or SCALAR, or with LBM_STREAM_AA on quad rows "
+                       "(kernel AUTO or QUAD, nx a multiple of 8, at least 16)");
     if (!std::isfinite(opt->noise_amp) || !std::isfinite(opt->store_scale) ||
         opt->store_scale < 0.0f)
       return set_error(LBM_ERR_INVALID, "bad noise_amp/store_scale");
@@ -492,11 +491,6 @@ inline void free_all(lbm_domain* d) {
 }
 
 
-// Rows of a 16-bit AA domain with kernel AUTO where word rows fit.
-#ifndef LBM_AA_AUTO_ROWS
-#define LBM_AA_AUTO_ROWS kRowsQuad
-#endif
-
 // Fill the geometry, sizes and storage scale of d from the case.
 inline void domain_prepare(lbm_domain* d, const Inputval* pinput, const lbm_options* opt) {
   d->in = *pinput;
@@ -519,11 +513,9 @@ inline void domain_prepare(lbm_domain* d, const Inputval* pinput, const lbm_opti
   if (b16 && d->opt.stream_mode == LBM_STREAM_AB &&
       (d->opt.kernel == LBM_KERNEL_AUTO || d->opt.kernel == LBM_KERNEL_PAIRED))
     d->g.rows = kRowsPaired;
-  if (aa_word_rows_fit(pinput, &d->opt)) {
-    if (d->opt.kernel == LBM_KERNEL_AUTO) d->g.rows = LBM_AA_AUTO_ROWS;
-    if (d->opt.kernel == LBM_KERNEL_PAIRED) d->g.rows = kRowsPaired;
-    if (d->opt.kernel == LBM_KERNEL_QUAD) d->g.rows = kRowsQuad;
-  }
+  if (aa_word_rows_fit(pinput, &d->opt) &&
+      (d->opt.kernel == LBM_KERNEL_AUTO || d->opt.kernel == LBM_KERNEL_QUAD))
+    d->g.rows = kRowsQuad;
   d->N = s.N;
   d->qs = s.qs;
   d->elem = storage_bytes(d->opt.storage);

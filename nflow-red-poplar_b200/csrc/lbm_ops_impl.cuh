@@ -127,40 +127,37 @@ int ops_run_aa(lbm_domain* d, int nsteps) {
     // per thread, except the first step after the initial state (a local
     // step, whose slots are all at the node: the per-node step over the
     // domain's rows)
-    int nh = 0;
-    dim3 bw(1, 1, 1), gw(1, 1, 1);
+    // quad rows (16-bit): k_aa_words, one word of four nodes per thread,
+    // except the first step after the initial state (a local step, whose
+    // slots are all at the node: the per-node step over quad rows)
+    bool words = false;
+    dim3 bw(1, 1, 1), gw(1, 1, 1), gn(1, 1, 1);
     if constexpr (kDev<S>) {
       if (d->g.rows != kRowsPlain) {
         if (!aa_words_apply(d->g))
           return set_error(LBM_ERR_INVALID, "AA domain rows without the word step");
-        nh = d->g.rows == kRowsQuad ? 2 : 1;
-        const int nw = d->g.px / (2 * nh);
+        words = true;
+        const int nw = d->g.px / 4;
         bw = block_of(nw);
-        gw = dim3((nw + bw.x - 1) / bw.x, d->g.nz, d->g.ny);
+        gw = dim3((nw + bw.x - 1) / bw.x, d->g.nz, d->g.ny);  // local step: every row
+        // neighbour step: rows off the faces, then the face rows
+        const int fz = (aa_face_rows(d->g) + d->g.nz - 3) / (d->g.nz - 2);
+        gn = dim3(gw.x, d->g.nz - 2, d->g.ny - 2 + fz);
       }
     }
     auto launch = [&](cudaStream_t st, const StepArgs<S>& a, int nb, int entry) {
       if constexpr (kDev<S>) {
-        if (nh && entry != kAAFromInit) {
-          auto go = [&](auto sr, auto nbc, auto nhc) {
-            k_aa_words<S, C, L, decltype(sr)::value, decltype(nbc)::value, decltype(nhc)::value>
-                <<<gw, bw, 0, st>>>(a, entry);
-          };
-          using T = std::true_type;
-          using F = std::false_type;
-          using I0 = std::integral_constant<int, 0>;
-          using I1 = std::integral_constant<int, 1>;
-          using I2 = std::integral_constant<int, 2>;
-          if (nh == 2) {
-            if (a.sr)
-              nb ? go(T{}, I1{}, I2{}) : go(T{}, I0{}, I2{});
+        if (words && entry != kAAFromInit) {
+          if (a.sr) {
+            if (nb)
+              k_aa_words<S, C, L, true, 1, 2><<<gn, bw, 0, st>>>(a, entry);
             else
-              nb ? go(F{}, I1{}, I2{}) : go(F{}, I0{}, I2{});
+              k_aa_words<S, C, L, true, 0, 2><<<gw, bw, 0, st>>>(a, entry);
           } else {
-            if (a.sr)
-              nb ? go(T{}, I1{}, I1{}) : go(T{}, I0{}, I1{});
+            if (nb)
+              k_aa_words<S, C, L, false, 1, 2><<<gn, bw, 0, st>>>(a, entry);
             else
-              nb ? go(F{}, I1{}, I1{}) : go(F{}, I0{}, I1{});
+              k_aa_words<S, C, L, false, 0, 2><<<gw, bw, 0, st>>>(a, entry);
           }
           return;
         }

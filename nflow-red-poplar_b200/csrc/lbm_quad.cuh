@@ -49,11 +49,10 @@
 
 namespace lbm {
 
-// the word AA step applies to the domain's geometry (paired or quad rows,
-// no STRUCT nodes, px == nx: no padding nodes)
+// the word AA step applies to the domain's geometry (quad rows, no STRUCT
+// nodes, px == nx: no padding nodes)
 __host__ __device__ __forceinline__ bool aa_words_apply(const Geometry& g) {
-  return (g.rows == kRowsQuad || g.rows == kRowsPaired) && !has_struct(g) && g.px == g.nx &&
-         g.nx >= 16;
+  return g.rows == kRowsQuad && !has_struct(g) && g.px == g.nx && g.nx >= 16;
 }
 
 __device__ __forceinline__ uint2 ld_w8(const void* p) {
@@ -125,20 +124,25 @@ __device__ __forceinline__ void st_word(void* p, uint2 v) { st_w8(p, v); }
 // per-node step's).  In paired rows the seams are those of the pull step:
 // node H - 1 (lo of word H - 1) and node H (hi of word 0) are x neighbours,
 // node 0 is the lo of word 0 and node nx - 1 the hi of word H - 1.
-template <class S, int COLL, bool LES, bool SR, int NB, int NH>
+// FACE (neighbour step): the row lies on a y or z face, so that some
+// populations' donor or destination rows are outside the box; the rows off
+// the faces are stepped by a launch without that code (FACE = false), the
+// face rows by their own launch (k_aa_face_rows), which keeps each kernel's
+// code short.
+template <class S, int COLL, bool LES, bool SR, int NB, int NH, bool FACE>
 __device__ __forceinline__ void aa_word(const StepArgs<S>& a, int w, int y, int z, int entry) {
   static_assert(kDev<S>, "paired and quad rows are 16-bit layouts");
+  static_assert(NB || !FACE, "face rows matter to the neighbour step only");
   using W = WordOf<NH>;
   const int H = a.g.px >> 1, D = a.g.px >> 2;
   const int NW = a.g.px / (2 * NH);                    // words per row
   const int e = 2 * NH * w + a.g.px * (z + a.g.nz * y);  // slot 0 of the word
-  const bool face_row = y == 0 || y == a.g.ny - 1 || z == 0 || z == a.g.nz - 1;
   const bool seam_lo = w == 0, seam_hi = w == NW - 1;
   // donor / destination row of population q inside the box (rows off a
   // face: always)
   auto row_in = [&](int dy, int dz) {
-    return !face_row || ((unsigned)(y + dy) < (unsigned)a.g.ny &&
-                         (unsigned)(z + dz) < (unsigned)a.g.nz);
+    if constexpr (!FACE) return true;
+    return (unsigned)(y + dy) < (unsigned)a.g.ny && (unsigned)(z + dz) < (unsigned)a.g.nz;
   };
   W v[Q];
   if constexpr (!NB) {
@@ -203,8 +207,8 @@ __device__ __forceinline__ void aa_word(const StepArgs<S>& a, int w, int y, int 
         // the word across the seam is the last one of the destination row
         S* wd = a.dstq[q] + (e + a.g.px);
         if constexpr (NH == 1) {
-          st_w2(wd, r >> 16);                                  // node H -> H - 1
-          st_w2(a.dst + (opp(q) * a.qs + e), r & 0xffffu);     // node 0: own slot
+          st_w2(wd, r >> 16);                               // node H -> H - 1
+          st_w2(a.dst + (opp(q) * a.qs + e), r & 0xffffu);  // node 0: own slot
         } else {
           // its slots k0 k2 k1 <- results k1 k3 k2; quarter 0 (x = 0) to
           // its own slot
@@ -216,8 +220,8 @@ __device__ __forceinline__ void aa_word(const StepArgs<S>& a, int w, int y, int 
         // the word across the seam is the first one of the destination row
         S* wd = a.dstq[q] + (e - a.g.px);
         if constexpr (NH == 1) {
-          st_w2(wd + 1, r & 0xffffu);                          // node H - 1 -> H
-          st_w2(a.dst + (opp(q) * a.qs + e + 1), r >> 16);     // node nx - 1: own slot
+          st_w2(wd + 1, r & 0xffffu);                           // node H - 1 -> H
+          st_w2(a.dst + (opp(q) * a.qs + e + 1), r >> 16);      // node nx - 1: own slot
         } else {
           // its slots k2 k1 k3 <- results k0 k1 k2; quarter 3 (x = nx - 1)
           // to its own slot
@@ -244,7 +248,11 @@ __device__ __forceinline__ void aa_word(const StepArgs<S>& a, int w, int y, int 
     });
     int tlo = NODE_FLUID, thi = NODE_FLUID;
     if constexpr (NB) {
-      if (face_row || ((seam_lo || seam_hi) && a.g.casetype != CAVITY)) {
+      // boundary rules of the donors outside the box: whole face rows (each
+      // node's wall rule) and the x faces (node 0, the lo lane of the first
+      // half of word 0; node nx - 1, the hi lane of the last half of the
+      // last word), whose rule is the value itself for the cavity's walls
+      if (FACE || ((seam_lo || seam_hi) && a.g.casetype != CAVITY)) {
         tlo = node_type(a.g, xlo, y, z);
         thi = node_type(a.g, xhi, y, z);
         static_for<0, Q>([&](auto qc) {
@@ -257,7 +265,8 @@ __device__ __forceinline__ void aa_word(const StepArgs<S>& a, int w, int y, int 
         });
       }
     } else {
-      if (entry == kAAPending && a.g.casetype == CHANNEL && !face_row) {
+      if (entry == kAAPending && a.g.casetype == CHANNEL && y > 0 && y < a.g.ny - 1 && z > 0 &&
+          z < a.g.nz - 1) {
         if (hb == 0 && seam_lo) quad_open_face_lane<S>(f, a, false, xlo, y, z);
         if (hb == NH - 1 && seam_hi) quad_open_face_lane<S>(f, a, true, xhi, y, z);
       }
@@ -274,8 +283,8 @@ __device__ __forceinline__ void aa_word(const StepArgs<S>& a, int w, int y, int 
     if constexpr (SR) h = sr_hash((uint32_t)(xlo + H * (z + a.g.nz * y)), kstep, a.sr_seed);
     collide_node<S, COLL, LES, true, F2>(f, ps, ux, uy, uz, inv_rho, a, [&](auto qc, F2 r) {
       constexpr int q = decltype(qc)::value;
-      if constexpr (NB) {
-        if (face_row && !row_in(cy(q), cz(q))) {
+      if constexpr (FACE) {
+        if (!row_in(cy(q), cz(q))) {
           // destination row outside: the wall value into the node's own slot
           r.v.x = aa_wall<S>(a, tlo, r.v.x, q);
           r.v.y = aa_wall<S>(a, thi, r.v.y, q);
@@ -299,17 +308,50 @@ __device__ __forceinline__ void aa_word(const StepArgs<S>& a, int w, int y, int 
   if constexpr (NH == 2) pass(std::integral_constant<int, 1>{});
 }
 
-// grid = (ceil(NW / b), nz, ny), NW = px / (2 NH) words per row, b = NW
-// rounded up to a multiple of 32 and at most 128 threads, one word per
-// thread
+// number of rows on a y or z face: 2 nz at y = 0 and y = ny - 1, then
+// 2 (ny - 2) at z = 0 and z = nz - 1
+__host__ __device__ __forceinline__ int aa_face_rows(const Geometry& g) {
+  return 2 * g.nz + 2 * (g.ny - 2);
+}
+
+// Local step: grid = (ceil(NW / b), nz, ny), every row.  Neighbour step:
+// grid = (ceil(NW / b), nz - 2, ny - 2 + FZ), FZ = ceil(aa_face_rows /
+// (nz - 2)): the rows off the y and z faces, then the face rows in the
+// trailing CTAs (a CTA-uniform branch into the code with the face rules,
+// so the hot code of the interior rows stays short and the face rows fill
+// the grid's tail).  NW = px / (2 NH) words per row, b = NW rounded up to a
+// multiple of 32 and at most 128 threads, one word per thread.  In the
+// neighbour step the two seam words of a row (0 and NW - 1) are taken by
+// the row's first two threads, so only the row's first warp diverges into
+// the seam code.
 template <class S, int COLL, bool LES, bool SR, int NB, int NH>
 __global__ void __launch_bounds__(128, (NH == 2 ? LBM_QUAD_THREADS_PER_SM
                                                 : LBM_AA_PAIRED_THREADS_PER_SM) / 128)
     k_aa_words(const __grid_constant__ StepArgs<S> a, int entry) {
-  const int w = (int)(blockIdx.x * blockDim.x + threadIdx.x);
-  const int z = blockIdx.y, y = blockIdx.z;
-  if (w >= a.g.px / (2 * NH)) return;
-  aa_word<S, COLL, LES, SR, NB, NH>(a, w, y, z, entry);
+  const int NW = a.g.px / (2 * NH);
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (t >= NW) return;
+  if constexpr (!NB) {
+    aa_word<S, COLL, LES, SR, 0, NH, false>(a, t, blockIdx.z, blockIdx.y, entry);  // y, z
+  } else {
+    const int w = t == 0 ? 0 : (t == 1 ? NW - 1 : t - 1);
+    if ((int)blockIdx.z < a.g.ny - 2) {
+      aa_word<S, COLL, LES, SR, 1, NH, false>(a, w, blockIdx.z + 1, blockIdx.y + 1, entry);
+    } else {
+      const int r = ((int)blockIdx.z - (a.g.ny - 2)) * (a.g.nz - 2) + (int)blockIdx.y;
+      if (r >= aa_face_rows(a.g)) return;
+      int y, z;
+      if (r < 2 * a.g.nz) {
+        y = r < a.g.nz ? 0 : a.g.ny - 1;
+        z = r % a.g.nz;
+      } else {
+        const int r2 = r - 2 * a.g.nz;
+        z = r2 < a.g.ny - 2 ? 0 : a.g.nz - 1;
+        y = 1 + r2 % (a.g.ny - 2);
+      }
+      aa_word<S, COLL, LES, SR, 1, NH, true>(a, w, y, z, entry);
+    }
+  }
 }
 
 }  // namespace lbm

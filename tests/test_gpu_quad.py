@@ -1,11 +1,10 @@
-"""The word AA step of the 16-bit forms over quad rows (LBM_KERNEL_QUAD) and
-paired rows (LBM_KERNEL_PAIRED with LBM_STREAM_AA).
+"""The word AA step of the 16-bit forms over quad rows (LBM_KERNEL_QUAD, the
+default of FP16/BF16 shifted storage with LBM_STREAM_AA).
 
 Quad rows store the 8-byte word w of every row as the nodes w, w + nx/2,
 w + nx/4, w + 3nx/4 and step four nodes per thread (two F2 halves of packed
-FP32 arithmetic); paired rows store the 4-byte word w as the nodes w,
-w + nx/2 and step two nodes per thread; the per-node AA step
-(LBM_KERNEL_SCALAR) steps plain rows one node per thread.  Both run the same node arithmetic without multiply-add
+FP32 arithmetic); the per-node AA step (LBM_KERNEL_SCALAR) steps plain rows
+one node per thread.  Both run the same node arithmetic without multiply-add
 contraction, so a domain must give the same bits either way: after any
 number of steps (ending on either AA layout, across CUDA-graph chunks) the
 exported arF, which undoes the layout, and the macroscopic fields are
@@ -49,7 +48,7 @@ def run(iv, o, steps):
     return out
 
 
-WORDS = [pkg.KERNEL_QUAD, pkg.KERNEL_PAIRED]
+WORDS = [pkg.KERNEL_QUAD]
 
 
 def both(iv, storage, steps, kind=pkg.INIT_DENSITY_NOISE, amp=1e-4, kernel=pkg.KERNEL_QUAD):
@@ -102,7 +101,7 @@ def test_quad_import_export_and_checkpoint(storage, tmp_path):
     arF = src.export_arF(padded=True)
     src.close()
     res = []
-    for kern in (pkg.KERNEL_QUAD, pkg.KERNEL_PAIRED, pkg.KERNEL_SCALAR):
+    for kern in (pkg.KERNEL_QUAD, pkg.KERNEL_SCALAR):
         d = pkg.Domain(iv, opts(storage, kern))
         d.import_arF(arF, padded=True)
         first = d.export_arF(padded=True)
@@ -137,7 +136,7 @@ def test_quad_is_the_16bit_aa_default_and_fallbacks():
     with pytest.raises(pkg.LbmError):
         pkg.Domain(iv2, opts(st, pkg.KERNEL_QUAD))
     with pytest.raises(pkg.LbmError):
-        pkg.Domain(iv2, opts(st, pkg.KERNEL_PAIRED))
+        pkg.Domain(iv, opts(st, pkg.KERNEL_PAIRED))  # paired rows: the pull form
     with pytest.raises(pkg.LbmError):
         pkg.Domain(iv, pkg.default_options(storage=st, kernel=pkg.KERNEL_QUAD))  # pull form
     with pytest.raises(pkg.LbmError):
