@@ -74,6 +74,9 @@ struct lbm_domain {
   // AA streaming: cur is the layout of lat[0] (0 natural, 1 swapped);
   // aa_first: the next step is the first after the initial state
   bool aa_first = false;
+  // channel on quad rows: the next AA step's inlet / outlet values
+  // [2][5][ny*nz] (k_aa_xface_rules)
+  float* xrule = nullptr;
 };
 
 // steps per captured graph chunk (even, so that a chunk returns the lattices
@@ -482,6 +485,7 @@ inline void free_all(lbm_domain* d) {
   if (d->flag && !d->pooled) cudaFree(d->flag);  // batch members: from the pool
   if (d->partial) cudaFree(d->partial);
   if (d->dout) cudaFree(d->dout);
+  if (d->xrule) cudaFree(d->xrule);
   for (int i = 0; i < 2; ++i)
     if (d->chunk[i]) cudaGraphExecDestroy(d->chunk[i]);
   if (d->capture) cudaStreamDestroy(d->capture);

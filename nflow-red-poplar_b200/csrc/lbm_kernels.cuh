@@ -189,6 +189,11 @@ struct StepArgs {
   int kpar;
   int sr;
   unsigned sr_seed;
+  // channel on quad rows: the inlet / outlet values this step takes for the
+  // populations whose donor lies outside the box at x = 0 (c_x = +1) and
+  // x = nx - 1 (c_x = -1), [2][5][ny*nz], computed after the step before
+  // (k_aa_xface_rules)
+  const float* xrule;
 };
 
 // internal value of a stored population

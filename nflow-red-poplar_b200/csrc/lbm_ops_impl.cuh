@@ -143,21 +143,38 @@ int ops_run_aa(lbm_domain* d, int nsteps) {
         // neighbour step: rows off the faces, then the face rows
         const int fz = (aa_face_rows(d->g) + d->g.nz - 3) / (d->g.nz - 2);
         gn = dim3(gw.x, d->g.nz - 2, d->g.ny - 2 + fz);
+        // channels: the buffer of the x-face values (k_aa_xface_rules)
+        if (d->g.casetype == CHANNEL && !d->xrule)
+          CK(cudaMalloc(&d->xrule, (size_t)10 * d->g.ny * d->g.nz * sizeof(float)));
       }
     }
+    const unsigned gx = (unsigned)((2 * (d->g.ny - 2) * (d->g.nz - 2) + 127) / 128);
     auto launch = [&](cudaStream_t st, const StepArgs<S>& a, int nb, int entry) {
       if constexpr (kDev<S>) {
-        if (words && entry != kAAFromInit) {
-          if (a.sr) {
-            if (nb)
-              k_aa_words<S, C, L, true, 1, 2><<<gn, bw, 0, st>>>(a, entry);
-            else
-              k_aa_words<S, C, L, true, 0, 2><<<gw, bw, 0, st>>>(a, entry);
+        if (words) {
+          if (entry != kAAFromInit) {
+            StepArgs<S> aw = a;
+            aw.xrule = d->xrule;
+            if (aw.sr) {
+              if (nb)
+                k_aa_words<S, C, L, true, 1, 2><<<gn, bw, 0, st>>>(aw, entry);
+              else
+                k_aa_words<S, C, L, true, 0, 2><<<gw, bw, 0, st>>>(aw, entry);
+            } else {
+              if (nb)
+                k_aa_words<S, C, L, false, 1, 2><<<gn, bw, 0, st>>>(aw, entry);
+              else
+                k_aa_words<S, C, L, false, 0, 2><<<gw, bw, 0, st>>>(aw, entry);
+            }
           } else {
-            if (nb)
-              k_aa_words<S, C, L, false, 1, 2><<<gn, bw, 0, st>>>(a, entry);
-            else
-              k_aa_words<S, C, L, false, 0, 2><<<gw, bw, 0, st>>>(a, entry);
+            k_aa_step<S, C, L, 0><<<gr, b, 0, st>>>(a, entry);
+          }
+          if (d->xrule) {
+            // the next step's x-face values, from the face planes this step wrote
+            StepArgs<S> fa = a;
+            fa.prho_in = a.prho_out;
+            fa.pu_in = a.pu_out;
+            k_aa_xface_rules<S><<<gx, 128, 0, st>>>(fa, d->xrule);
           }
           return;
         }

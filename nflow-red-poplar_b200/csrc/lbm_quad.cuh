@@ -96,6 +96,47 @@ __device__ __forceinline__ void quad_open_face_lane(F2 (&f)[Q], const StepArgs<S
 #define LBM_AA_PAIRED_THREADS_PER_SM 1024
 #endif
 
+// index of population q (c_x = +-1) among the five with its c_x
+__host__ __device__ constexpr int xface_index(int q) {
+  int j = 0;
+  for (int p = 1; p < q; ++p) j += cx(p) == cx(q);
+  return j;
+}
+
+// Channels on quad rows: after every AA step, the inlet / outlet values
+// that the next step takes for the populations whose donor lies outside the
+// box at the x faces of the interior rows: at x = 0 (inlet) the five with
+// c_x = +1, at x = nx - 1 (outlet) the five with c_x = -1.  In both AA
+// layouts the node's own slot (x, q) then holds f*_{opp q} (a pending
+// natural slot after a neighbour step, the own slot after a local step), and
+// the value is boundary_value of the node with the face planes the step
+// just wrote: a = the next step's arguments.  The step kernels read the
+// five values instead of evaluating the rule (FP64 arithmetic that only
+// two threads of a row would run): the same FP32 values, so the same bits.
+// grid = ceil(2 (ny - 2)(nz - 2) / 128) blocks of 128.
+template <class S>
+__global__ void __launch_bounds__(128) k_aa_xface_rules(const __grid_constant__ StepArgs<S> a,
+                                                        float* __restrict__ out) {
+  const int ni = (a.g.ny - 2) * (a.g.nz - 2);
+  const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (i >= 2 * ni) return;
+  const int face = i >= ni, r = face ? i - ni : i;
+  const int y = 1 + r / (a.g.nz - 2), z = 1 + r % (a.g.nz - 2);
+  const int x = face ? a.g.nx - 1 : 0;
+  const int P = a.g.ny * a.g.nz, yz = y * a.g.nz + z;
+  const int t = node_type(a.g, x, y, z);
+  const int cell = cell_of(a.g, x, y, z);
+  static_for<1, Q>([&](auto qc) {
+    constexpr int q = decltype(qc)::value;
+    if constexpr (cx(q) != 0) {
+      if ((cx(q) == 1) == (face == 0)) {
+        const RealOf<S> fo = ld(a.srcq[q] + cell, q, a.inv_scale);
+        out[(face * 5 + xface_index(q)) * P + yz] = (float)boundary_value<S, q>(a, t, fo, y, z);
+      }
+    }
+  });
+}
+
 // a word of NH 32-bit halves (NH = 1: paired rows, 2: quad rows)
 template <int NH>
 using WordOf = typename std::conditional<NH == 1, uint32_t, uint2>::type;
@@ -252,7 +293,18 @@ __device__ __forceinline__ void aa_word(const StepArgs<S>& a, int w, int y, int 
       // node's wall rule) and the x faces (node 0, the lo lane of the first
       // half of word 0; node nx - 1, the hi lane of the last half of the
       // last word), whose rule is the value itself for the cavity's walls
-      if (FACE || ((seam_lo || seam_hi) && a.g.casetype != CAVITY)) {
+      if (!FACE && a.xrule && (seam_lo || seam_hi)) {
+        // channel x faces: the values k_aa_xface_rules left for this step
+        const int P = a.g.ny * a.g.nz, yz = y * a.g.nz + z;
+        static_for<0, Q>([&](auto qc) {
+          constexpr int q = decltype(qc)::value;
+          if constexpr (cx(q) == 1) {
+            if (hb == 0 && seam_lo) f[q].v.x = a.xrule[xface_index(q) * P + yz];
+          } else if constexpr (cx(q) == -1) {
+            if (hb == NH - 1 && seam_hi) f[q].v.y = a.xrule[(5 + xface_index(q)) * P + yz];
+          }
+        });
+      } else if (FACE || ((seam_lo || seam_hi) && a.g.casetype != CAVITY)) {
         tlo = node_type(a.g, xlo, y, z);
         thi = node_type(a.g, xhi, y, z);
         static_for<0, Q>([&](auto qc) {
@@ -266,9 +318,22 @@ __device__ __forceinline__ void aa_word(const StepArgs<S>& a, int w, int y, int 
       }
     } else {
       if (entry == kAAPending && a.g.casetype == CHANNEL && y > 0 && y < a.g.ny - 1 && z > 0 &&
-          z < a.g.nz - 1) {
-        if (hb == 0 && seam_lo) quad_open_face_lane<S>(f, a, false, xlo, y, z);
-        if (hb == NH - 1 && seam_hi) quad_open_face_lane<S>(f, a, true, xhi, y, z);
+          z < a.g.nz - 1 && (seam_lo || seam_hi)) {
+        if (a.xrule) {
+          // the values k_aa_xface_rules left for this step
+          const int P = a.g.ny * a.g.nz, yz = y * a.g.nz + z;
+          static_for<0, Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            if constexpr (cx(q) == 1) {
+              if (hb == 0 && seam_lo) f[q].v.x = a.xrule[xface_index(q) * P + yz];
+            } else if constexpr (cx(q) == -1) {
+              if (hb == NH - 1 && seam_hi) f[q].v.y = a.xrule[(5 + xface_index(q)) * P + yz];
+            }
+          });
+        } else {
+          if (hb == 0 && seam_lo) quad_open_face_lane<S>(f, a, false, xlo, y, z);
+          if (hb == NH - 1 && seam_hi) quad_open_face_lane<S>(f, a, true, xhi, y, z);
+        }
       }
     }
     PairState<F2> ps;
