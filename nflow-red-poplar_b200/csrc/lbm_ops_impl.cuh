@@ -130,8 +130,8 @@ int ops_run_aa(lbm_domain* d, int nsteps) {
     // quad rows (16-bit): k_aa_words, one word of four nodes per thread,
     // except the first step after the initial state (a local step, whose
     // slots are all at the node: the per-node step over quad rows)
-    bool words = false;
-    dim3 bw(1, 1, 1), gw(1, 1, 1), gn(1, 1, 1);
+    [[maybe_unused]] bool words = false;
+    [[maybe_unused]] dim3 bw(1, 1, 1), gw(1, 1, 1), gn(1, 1, 1);
     if constexpr (kDev<S>) {
       if (d->g.rows != kRowsPlain) {
         if (!aa_words_apply(d->g))
@@ -148,7 +148,8 @@ int ops_run_aa(lbm_domain* d, int nsteps) {
           CK(cudaMalloc(&d->xrule, (size_t)10 * d->g.ny * d->g.nz * sizeof(float)));
       }
     }
-    const unsigned gx = (unsigned)((2 * (d->g.ny - 2) * (d->g.nz - 2) + 127) / 128);
+    [[maybe_unused]] const unsigned gx =
+        (unsigned)((2 * (d->g.ny - 2) * (d->g.nz - 2) + 127) / 128);
     auto launch = [&](cudaStream_t st, const StepArgs<S>& a, int nb, int entry) {
       if constexpr (kDev<S>) {
         if (words) {

@@ -287,7 +287,7 @@ __device__ __forceinline__ void aa_word(const StepArgs<S>& a, int w, int y, int 
       constexpr int q = decltype(qc)::value;
       f[q] = unpack_pair<S>(half_of<hb>(v[q]), a.inv_scale);
     });
-    int tlo = NODE_FLUID, thi = NODE_FLUID;
+    [[maybe_unused]] int tlo = NODE_FLUID, thi = NODE_FLUID;
     if constexpr (NB) {
       // boundary rules of the donors outside the box: whole face rows (each
       // node's wall rule) and the x faces (node 0, the lo lane of the first
@@ -344,7 +344,7 @@ __device__ __forceinline__ void aa_word(const StepArgs<S>& a, int w, int y, int 
       write_macro<S>(a, xlo, y, z, ps.rho_full.v.x, ux.v.x, uy.v.x, uz.v.x);
       write_macro<S>(a, xhi, y, z, ps.rho_full.v.y, ux.v.y, uy.v.y, uz.v.y);
     }
-    uint32_t h = 0u;
+    [[maybe_unused]] uint32_t h = 0u;
     if constexpr (SR) h = sr_hash((uint32_t)(xlo + H * (z + a.g.nz * y)), kstep, a.sr_seed);
     collide_node<S, COLL, LES, true, F2>(f, ps, ux, uy, uz, inv_rho, a, [&](auto qc, F2 r) {
       constexpr int q = decltype(qc)::value;
