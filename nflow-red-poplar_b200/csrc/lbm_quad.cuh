@@ -66,26 +66,6 @@ __device__ __forceinline__ void st_w2(void* p, uint32_t v) {
   *reinterpret_cast<unsigned short*>(p) = (unsigned short)v;
 }
 
-// open-face rules (inlet / outlet) of one F2 lane whose node has pending
-// natural slots (the per-node aa_open_face_rules on that lane)
-template <class S>
-__device__ __forceinline__ void quad_open_face_lane(F2 (&f)[Q], const StepArgs<S>& a, bool hi,
-                                                    int x, int y, int z) {
-  float g[Q];
-  static_for<0, Q>([&](auto qc) {
-    constexpr int q = decltype(qc)::value;
-    g[q] = hi ? f[q].v.y : f[q].v.x;
-  });
-  aa_open_face_rules<S>(g, a, x, y, z);
-  static_for<0, Q>([&](auto qc) {
-    constexpr int q = decltype(qc)::value;
-    if (hi)
-      f[q].v.y = g[q];
-    else
-      f[q].v.x = g[q];
-  });
-}
-
 // Resident threads per SM the register budgets are sized for: the quad step
 // (two F2 halves per thread, 128 registers) and the paired AA step (one F2
 // half, 64 registers).
@@ -135,6 +115,18 @@ __global__ void __launch_bounds__(128) k_aa_xface_rules(const __grid_constant__ 
       }
     }
   });
+}
+
+// The wall rule of boundary_value (fixed wall: the value itself; moving
+// wall: minus the lid term) for population q at a wall node of type t.
+template <class S, int q>
+__device__ __forceinline__ RealOf<S> wall_value(const StepArgs<S>& a, int t, RealOf<S> fo) {
+  using R = RealOf<S>;
+  if (t != NODE_MOVINGWALL) return fo;
+  constexpr int d = opp(q);
+  R eu = add_rn(add_rn(mul_rn(R(cx(d)), a.ulx), mul_rn(R(cy(d)), a.uly)), mul_rn(R(cz(d)), a.ulz));
+  R term = mul_rn(mul_rn(mul_rn(R(6), weight<R>(d)), a.rho0), eu);
+  return sub_rn(fo, term);
 }
 
 // a word of NH 32-bit halves (NH = 1: paired rows, 2: quad rows)
@@ -275,6 +267,21 @@ __device__ __forceinline__ void aa_word(const StepArgs<S>& a, int w, int y, int 
       }
     }
   };
+  // channels: the x-face lanes of this word take the values of
+  // k_aa_xface_rules (node 0: lo lane of half 0 of word 0, c_x = +1
+  // populations; node nx - 1: hi lane of the last half of the last word,
+  // c_x = -1 populations)
+  auto xface_lanes = [&](F2 (&f)[Q], int hb) {
+    const int P = a.g.ny * a.g.nz, yz = y * a.g.nz + z;
+    static_for<0, Q>([&](auto qc) {
+      constexpr int q = decltype(qc)::value;
+      if constexpr (cx(q) == 1) {
+        if (hb == 0 && seam_lo) f[q].v.x = a.xrule[xface_index(q) * P + yz];
+      } else if constexpr (cx(q) == -1) {
+        if (hb == NH - 1 && seam_hi) f[q].v.y = a.xrule[(5 + xface_index(q)) * P + yz];
+      }
+    });
+  };
   // the halves, each a compile-time pass: half hb holds the nodes
   // (w + hb D, w + hb D + H); every pass but the last leaves its packed
   // results in its half of v[q], the last stores each population's word as
@@ -289,52 +296,34 @@ __device__ __forceinline__ void aa_word(const StepArgs<S>& a, int w, int y, int 
     });
     [[maybe_unused]] int tlo = NODE_FLUID, thi = NODE_FLUID;
     if constexpr (NB) {
-      // boundary rules of the donors outside the box: whole face rows (each
-      // node's wall rule) and the x faces (node 0, the lo lane of the first
-      // half of word 0; node nx - 1, the hi lane of the last half of the
-      // last word), whose rule is the value itself for the cavity's walls
-      if (!FACE && a.xrule && (seam_lo || seam_hi)) {
-        // channel x faces: the values k_aa_xface_rules left for this step
-        const int P = a.g.ny * a.g.nz, yz = y * a.g.nz + z;
-        static_for<0, Q>([&](auto qc) {
-          constexpr int q = decltype(qc)::value;
-          if constexpr (cx(q) == 1) {
-            if (hb == 0 && seam_lo) f[q].v.x = a.xrule[xface_index(q) * P + yz];
-          } else if constexpr (cx(q) == -1) {
-            if (hb == NH - 1 && seam_hi) f[q].v.y = a.xrule[(5 + xface_index(q)) * P + yz];
-          }
-        });
-      } else if (FACE || ((seam_lo || seam_hi) && a.g.casetype != CAVITY)) {
+      // boundary rules of the donors outside the box.  Face rows: each
+      // node's wall rule (rows on a y or z face hold walls only: the lid,
+      // and fixed walls, which a channel's side faces keep over its inlet
+      // and outlet; their x faces are fixed walls, whose rule is the value
+      // itself).  Rows off the faces: the x faces (node 0, the lo lane of
+      // the first half of word 0; node nx - 1, the hi lane of the last half
+      // of the last word), whose rule is the value itself for the cavity's
+      // fixed walls and, for the channel's inlet and outlet, the value
+      // k_aa_xface_rules left for this step.
+      if constexpr (FACE) {
         tlo = node_type(a.g, xlo, y, z);
         thi = node_type(a.g, xhi, y, z);
         static_for<0, Q>([&](auto qc) {
           constexpr int q = decltype(qc)::value;
-          const bool rout = !row_in(-cy(q), -cz(q));
-          if (rout || (cx(q) == 1 && hb == 0 && seam_lo))
-            f[q].v.x = boundary_value<S, q>(a, tlo, f[q].v.x, y, z);
-          if (rout || (cx(q) == -1 && hb == NH - 1 && seam_hi))
-            f[q].v.y = boundary_value<S, q>(a, thi, f[q].v.y, y, z);
+          if (!row_in(-cy(q), -cz(q))) {
+            f[q].v.x = wall_value<S, q>(a, tlo, f[q].v.x);
+            f[q].v.y = wall_value<S, q>(a, thi, f[q].v.y);
+          }
         });
+      } else if (a.xrule && (seam_lo || seam_hi)) {
+        xface_lanes(f, hb);
       }
     } else {
-      if (entry == kAAPending && a.g.casetype == CHANNEL && y > 0 && y < a.g.ny - 1 && z > 0 &&
-          z < a.g.nz - 1 && (seam_lo || seam_hi)) {
-        if (a.xrule) {
-          // the values k_aa_xface_rules left for this step
-          const int P = a.g.ny * a.g.nz, yz = y * a.g.nz + z;
-          static_for<0, Q>([&](auto qc) {
-            constexpr int q = decltype(qc)::value;
-            if constexpr (cx(q) == 1) {
-              if (hb == 0 && seam_lo) f[q].v.x = a.xrule[xface_index(q) * P + yz];
-            } else if constexpr (cx(q) == -1) {
-              if (hb == NH - 1 && seam_hi) f[q].v.y = a.xrule[(5 + xface_index(q)) * P + yz];
-            }
-          });
-        } else {
-          if (hb == 0 && seam_lo) quad_open_face_lane<S>(f, a, false, xlo, y, z);
-          if (hb == NH - 1 && seam_hi) quad_open_face_lane<S>(f, a, true, xhi, y, z);
-        }
-      }
+      // pending natural slots of the channel's inlet and outlet nodes: the
+      // values k_aa_xface_rules left for this step
+      if (entry == kAAPending && a.xrule && y > 0 && y < a.g.ny - 1 && z > 0 &&
+          z < a.g.nz - 1 && (seam_lo || seam_hi))
+        xface_lanes(f, hb);
     }
     PairState<F2> ps;
     make_pairs<F2, true>(f, ps);
