@@ -207,7 +207,8 @@ typedef struct lbm_options {
  * STOCHASTIC needs FP16/BF16 shifted storage, with LBM_STREAM_AB and kernel
  * AUTO, PAIRED or SCALAR, or with LBM_STREAM_AA on quad rows (kernel AUTO or
  * QUAD) (single domains; batch members round to nearest).  The initial
- * state, imports and the first AA step after them round to nearest. */
+ * state, imports and the first AA step after the initial state round to
+ * nearest. */
 enum { LBM_ROUND_NEAREST = 0, LBM_ROUND_STOCHASTIC = 1 };
 
 /* Fill *opt with the defaults: FP32, reference init, A/B streaming. */
